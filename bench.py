@@ -1,0 +1,378 @@
+"""Benchmark of the dense-reconstruction path: PatchMatch px-iters/s and TSDF voxel-updates/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form plain|fast]
+
+Workload (the scan-scale configuration): 48 synthetic views of 640x480 (sphere-on-plane scene,
+3-octave value noise, helical camera path, 2 mm / 0.1 deg pose noise, pixel noise 0.01), 8
+sources, 5 red/black iterations, 11x11 window dilated by 2 (6 x 6 samples); consistency filter of
+every view; TSDF 512^3 at 4 mm, truncation 2 cm, f32 tsdf + uint16 Q8.8 weights.
+
+One step = the photometric PatchMatch stage over all 48 views + the consistency filter of all
+views + TSDF integration of all 48 filtered maps.  `value` is the PatchMatch px-iters/s of the
+step (px-iter = one pixel updated in one red/black iteration: 48 * 307200 * 5 per step) timed on
+the PatchMatch stage; the TSDF stage gives voxel-updates/s (134M voxels * 48 views per step).
+Inputs are resident in HBM for `value`; `e2e` repeats the step through the C ABI with the images
+copied from pinned host memory every step and the filtered maps and the TSDF volume read back.
+L2 is flushed (a 256 MB write) before every timed step.
+
+Multi-GPU: the path shards by reference view with no data-path collective in the photometric
+stage; each rank runs an independent replica of the workload ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "luvas.io-3d_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "PatchMatch px-iters/s, TSDF voxel-upd/s: chosen vs plain FP32 form, 1×B200"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(args):
+    from luvas3d import scenes
+
+    return scenes.scan(n_views=args.views, width=args.width, height=args.height,
+                       tsdf_dim=args.tsdf_dim)
+
+
+def cpu_baseline(w, threads: int, budget_s: float = 20.0) -> dict:
+    """The FP32 oracle on the host cores: one reference view's init + 1 red/black iteration at
+    full resolution with the workload's sources, and one TSDF view integration of the full
+    volume.  px-iters/s and voxel-updates/s of that bounded sample."""
+    import oracle
+
+    o = oracle.Stereo(w.width, w.height, w.views, w.images, 32, threads=threads)
+    t0 = time.perf_counter()
+    o.kernel(oracle.INIT, 0, w.sources[0], min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
+    t_init = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for phase in (0, 1):
+        o.kernel(oracle.PROPAGATE, 0, w.sources[0], iteration=0, phase=phase,
+                 min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
+    t_prop = time.perf_counter() - t0
+    pm = w.pixels / (t_init / 2 + t_prop) if False else w.pixels / t_prop
+    # TSDF: one view into the full volume
+    o.kernel(oracle.PACK, 0, w.sources[0], min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
+    v = w.views[0]
+    k = v.intrinsics
+    ot = oracle.Tsdf(w.width, w.height, w.tsdf_voxel, w.tsdf_origin, w.tsdf_truncation,
+                     dense=w.tsdf_dims, weight_q8=True, threads=threads)
+    t0 = time.perf_counter()
+    ot.integrate(dict(k=(k.fx, k.fy, k.cx, k.cy), R=v.pose.R, t=v.pose.t,
+                      max_depth=w.ranges[0][1]), o.depths[0])
+    t_tsdf = time.perf_counter() - t0
+    vox = int(np.prod(w.tsdf_dims))
+    return {"value": pm, "unit": "px-iters/s", "cores": threads, "kind": "port",
+            "sample": (f"FP32 oracle: 1 reference view x 1 red/black iteration at "
+                       f"{w.width}x{w.height}, {len(w.sources[0])} sources "
+                       f"({t_prop:.2f} s); TSDF 1 view into {w.tsdf_dims[0]}^3 ({t_tsdf:.2f} s)"),
+            "tsdf_voxel_updates_per_s": vox / t_tsdf, "seconds": t_prop + t_tsdf}
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    """--impl reference: the CPU restatement of the path on the host cores (the reference has no
+    CPU implementation of these stages; its WGSL needs WebGPU, unavailable on this box)."""
+    if rank != 0:
+        return
+    w = build_workload(args)
+    threads = os.cpu_count() or 1
+    vals, tv = [], []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(w, threads)
+        if i >= args.warmup:
+            vals.append(r["value"])
+            tv.append(r["tsdf_voxel_updates_per_s"])
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "px-iters/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * w.pixels / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "scan: 48 views 640x480, 8 sources, 5 iterations, TSDF 512^3",
+                   "sample": r["sample"]},
+        "tsdf_voxel_updates_per_s": statistics.median(tv),
+        "cpu_baseline": {"value": v, "unit": "px-iters/s", "cores": threads, "kind": "port",
+                         "sample": r["sample"]},
+        "e2e": {"value": v, "unit": "px-iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="auto", choices=["auto", "plain", "fast"])
+    ap.add_argument("--views", type=int, default=48)
+    ap.add_argument("--width", type=int, default=640)
+    ap.add_argument("--height", type=int, default=480)
+    ap.add_argument("--tsdf-dim", type=int, default=512)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    from luvas3d import (DTYPE_F32, FORM_PLAIN, DenseStereo, IntegrationView, SolveOptions,
+                         StereoOptions, TsdfVolume)
+
+    w = build_workload(args)
+    V, P = len(w.views), w.pixels
+    form = FORM_PLAIN
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    stereo = DenseStereo(w.width, w.height, w.views,
+                         StereoOptions(storage=DTYPE_F32, form=form, stream=sptr))
+    tsdf = TsdfVolume(w.width, w.height, w.tsdf_voxel, w.tsdf_origin, dense=w.tsdf_dims,
+                      truncation=w.tsdf_truncation, weight_q8=True, stream=sptr)
+    for i, im in enumerate(w.images):
+        stereo.set_image(i, im)
+    refs = list(range(V))
+    opts = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=w.iterations)
+            for r in refs]
+    iviews = [IntegrationView(v.intrinsics, v.pose, w.ranges[i][1]) for i, v in enumerate(w.views)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step(evs):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            evs[0].record(stream)
+        stereo.solve_all(refs, opts)
+        with torch.cuda.stream(stream):
+            evs[1].record(stream)
+        tsdf.reset()  # a fresh volume per scan (tsdf 1, weight 0), outside the timed TSDF stage
+        stereo.filter_all(refs, w.sources, w.needed)
+        with torch.cuda.stream(stream):
+            evs[2].record(stream)
+        tsdf.integrate_many(iviews, stereo=stereo, layers=refs)
+        with torch.cuda.stream(stream):
+            evs[3].record(stream)
+
+    mk = lambda: [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for _ in range(args.warmup):
+        step(mk())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = stereo.launches + tsdf.launches
+    clocks = ClockSampler(local)
+    clocks.start()
+    all_evs = []
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        evs = mk()
+        step(evs)
+        all_evs.append(evs)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    launches = stereo.launches + tsdf.launches - launches0
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    pm_ms = [e[0].elapsed_time(e[1]) for e in all_evs]
+    filt_ms = [e[1].elapsed_time(e[2]) for e in all_evs]
+    ts_ms = [e[2].elapsed_time(e[3]) for e in all_evs]
+    step_ms = [e[0].elapsed_time(e[3]) for e in all_evs]
+    tot = torch.tensor([sum(pm_ms), sum(ts_ms), sum(step_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    pm_s, ts_s, st_s = (float(x) / 1e3 for x in tot.tolist())
+    px_iters = V * P * w.iterations * args.steps * world
+    vox = int(np.prod(w.tsdf_dims))
+    voxel_updates = vox * V * args.steps * world
+    value = px_iters / pm_s
+
+    # ---- roofline of the dominant kernel (red/black propagate), timed alone -------------------
+    peaks, peak_kind = _peaks()
+    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    from luvas3d import KERNEL_PROPAGATE
+    reps = 10
+    with torch.cuda.stream(stream):
+        ev_a.record(stream)
+    for i in range(reps):
+        stereo.dispatch(KERNEL_PROPAGATE, 0, opts[0], iteration=1, phase=i & 1)
+    with torch.cuda.stream(stream):
+        ev_b.record(stream)
+    torch.cuda.synchronize()
+    prop_ms = ev_a.elapsed_time(ev_b) / reps
+    S = len(w.sources[0])
+    flop_per_px_phase = 14 * S * (18 + 36 * 37 + 15) + 36 * 26
+    prop_flops = flop_per_px_phase * (P / 2)
+    achieved = prop_flops / (prop_ms / 1e3) / 1e12
+    fp32_peak = 148 * 128 * 2 * (clk.get("sm_mhz") or 1965.0) * 1e6 / 1e12
+    tsdf_bytes = vox * 12
+    tsdf_gbs = tsdf_bytes / (sum(ts_ms) / len(ts_ms) / 1e3) / 1e9
+
+    # ---- end to end through the C ABI with pinned host buffers ------------------------------
+    e2e = None
+    if not args.no_e2e:
+        pinned = [torch.from_numpy(np.ascontiguousarray(im)).pin_memory() for im in w.images]
+        out_f = torch.empty((V, w.height, w.width), dtype=torch.int32).pin_memory()
+        out_t = torch.empty(vox, dtype=torch.float32).pin_memory()
+        out_w = torch.empty(vox, dtype=torch.int16).pin_memory()
+        import ctypes as C
+        from luvas3d import _lib
+        lib = _lib.load()
+
+        def e2e_step():
+            for i, im in enumerate(pinned):
+                stereo.set_image_device(i, im.data_ptr(), DTYPE_F32)
+            stereo.solve_all(refs, opts)
+            stereo.filter_all(refs, w.sources, w.needed)
+            tsdf.reset()
+            tsdf.integrate_many(iviews, stereo=stereo, layers=refs)
+            for r in refs:
+                _lib.check(lib.l3d_stereo_read_filtered_layer(
+                    stereo._h(), r, C.c_void_p(out_f[r].data_ptr())))
+            _lib.check(lib.l3d_tsdf_read(tsdf._h(), C.c_void_p(out_t.data_ptr()),
+                                         C.c_void_p(out_w.data_ptr())))
+
+        e2e_step()
+        torch.cuda.synchronize()
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            ea.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        with torch.cuda.stream(stream):
+            eb.record(stream)
+        torch.cuda.synchronize()
+        e2e_s = torch.tensor([ea.elapsed_time(eb) / 1e3], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+        e2e = {"value": px_iters / float(e2e_s.item()), "unit": "px-iters/s",
+               "h2d_bytes_per_step": V * P * 4,
+               "d2h_bytes_per_step": V * P * 4 + vox * 6,
+               "ms_per_step": float(e2e_s.item()) * 1e3 / args.steps,
+               "includes": "image upload from pinned host memory, PatchMatch, filter, TSDF, "
+                           "read-back of the filtered maps and the TSDF volume"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, os.cpu_count() or 1)
+        cpu.pop("seconds", None)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "px-iters/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": st_s * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded sphere-on-plane scene, value-noise texture)",
+        "config": {"workload": "scan: 48 views 640x480, 8 sources, 5 iterations, window 11x11 "
+                               "dilated by 2, TSDF 512^3 at 4 mm, trunc 2 cm, Q8.8 weights",
+                   "form": "plain", "l2": "flushed (256 MB write) before every step",
+                   "parallelism": f"replica x{world}"},
+        "tsdf_voxel_updates_per_s": voxel_updates / ts_s,
+        "stage_ms": {"patchmatch": sum(pm_ms) / len(pm_ms), "filter": sum(filt_ms) / len(filt_ms),
+                     "tsdf": sum(ts_ms) / len(ts_ms)},
+        "roofline": {"kernel": "k_propagate (plain FP32, one colour of one view)",
+                     "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2) at the "
+                                    "sampled median SM clock",
+                     "launch_ms": prop_ms, "flop_per_launch": prop_flops},
+        "roofline_tsdf": {"kernel": "k_integrate_many", "bound": "hbm", "achieved": tsdf_gbs,
+                          "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                          "frac": tsdf_gbs / peaks.get("hbm_gbs", 6650.0),
+                          "peak_source": peak_kind, "bytes_per_launch": tsdf_bytes},
+        "clocks": clk,
+        "gpu_launches": launches,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "wall_s_timed": t_wall,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    stereo.destroy()
+    tsdf.destroy()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,265 @@
+/*
+ * luvas3d - B200-native dense reconstruction (PatchMatch multi-view stereo + TSDF integration).
+ *
+ * Plain C ABI of libluvas3d.so.  It replaces the WebGPU plumbing behind the scanner's stereo
+ * and fusion stage API; every entry point names the reference interface it stands in for
+ * (paths inside the reference project, frontend/src/app/vision/...).
+ *
+ * Conventions
+ *   - Every call returns an int status (L3D_OK = 0).  On failure l3d_last_error() gives a
+ *     message for the calling thread.  No C++ exception crosses the ABI.
+ *   - Handles are opaque.  A handle owns its device memory and one CUDA stream; calls on one
+ *     handle are serialised on that stream and must not be made concurrently from two threads.
+ *     Different handles may be used from different threads.
+ *   - Host buffers are owned by the caller.  Input buffers in pageable memory may be reused as
+ *     soon as the call returns.  Input buffers in pinned (page-locked) memory are copied
+ *     asynchronously and must stay unchanged until the next synchronising call on the handle
+ *     (any l3d_*_read_*, l3d_*_synchronize or destroy).
+ *   - solve/filter/integrate enqueue device work and return without waiting (the reference's
+ *     Promises resolve when the GPU finishes; here l3d_*_synchronize or a read waits).
+ *   - Poses map world to camera in computer-vision axes (x right, y down, z forward):
+ *     x_cam = R X + t, R row-major (frontend/src/app/vision/geometry/camera.ts:19-26).
+ *   - There is no CPU fallback: when no CUDA device is usable, create calls fail with
+ *     L3D_ECUDA.
+ */
+#ifndef LUVAS3D_H
+#define LUVAS3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define L3D_ABI_VERSION 1
+
+/* Status codes. */
+#define L3D_OK 0
+#define L3D_EINVAL 1     /* bad argument: null pointer, shape, index or option */
+#define L3D_ECUDA 2      /* CUDA runtime error (message carries the CUDA error string) */
+#define L3D_ENOMEM 3     /* device or pinned-host allocation failed */
+#define L3D_ESTATE 4     /* not valid in the handle's current state */
+#define L3D_ETIMEOUT 5   /* a bounded device-side wait gave up */
+
+/* Element types of host images and device image storage. */
+#define L3D_DTYPE_U8 0   /* r8unorm: value / 255 (the reference's texture format) */
+#define L3D_DTYPE_F32 1
+#define L3D_DTYPE_F16 2
+#define L3D_DTYPE_BF16 3
+
+/* Kernel forms. */
+#define L3D_FORM_PLAIN 0 /* FP32, one reference view per launch, the oracle's operation order */
+#define L3D_FORM_FAST 1  /* FP16/BF16 image storage, batched views, compensated FP32 sums */
+
+/* TSDF weight storage. */
+#define L3D_WEIGHT_F32 0 /* f32 weights in [0, max_weight] (the reference's storage) */
+#define L3D_WEIGHT_Q8 1  /* uint16 weights in Q8.8 fixed point: weight = value / 256 */
+
+/* Single-kernel dispatch ids for l3d_stereo_dispatch (the units DenseStereo.sliced submits). */
+#define L3D_KERNEL_INIT 0
+#define L3D_KERNEL_INIT_COARSE 1
+#define L3D_KERNEL_PROPAGATE 2
+#define L3D_KERNEL_PACK 3
+#define L3D_KERNEL_CONSISTENCY 4
+
+typedef struct l3d_stereo l3d_stereo;
+typedef struct l3d_tsdf l3d_tsdf;
+
+/* Intrinsics (geometry/camera.ts:12-17). */
+typedef struct {
+    double fx, fy, cx, cy;
+} l3d_intrinsics;
+
+/* Pose, world -> camera (geometry/camera.ts:23-26). */
+typedef struct {
+    double R[9];
+    double t[3];
+} l3d_pose;
+
+/* StereoView (mvs/dense-stereo.ts:57-60). */
+typedef struct {
+    l3d_intrinsics intrinsics;
+    l3d_pose pose;
+} l3d_view;
+
+/* StereoOptions (mvs/dense-stereo.ts:84-88) plus the device layout choices. */
+typedef struct {
+    const l3d_stereo* coarse; /* CoarseLevel (dense-stereo.ts:78-82): its planes seed from_coarse
+                                 solves; it must outlive this handle.  NULL = none */
+    int32_t depth_maps;       /* 1: a packed depth map per view (default); 0: one map */
+    int32_t storage;          /* device image storage: F32 (plain form), F16 or BF16 */
+    int32_t form;             /* L3D_FORM_PLAIN or L3D_FORM_FAST */
+    int32_t window;           /* samples per window side: 6 (reference, offsets +-1,3,5) or 11 */
+    int32_t dilation;         /* spacing of window samples: 2 (reference) or 1 */
+    void* stream;             /* cudaStream_t to run on, or NULL to create one */
+} l3d_stereo_opts;
+
+/* SolveOptions (mvs/dense-stereo.ts:62-75). */
+typedef struct {
+    const int32_t* sources;   /* source layers; the first 8 are used (MAX_SOURCES) */
+    int32_t n_sources;
+    double min_depth, max_depth;
+    const float* prior;       /* host, width * height metres (0 = no prior), or NULL */
+    int32_t geometric;        /* ACMM pass: start from the packed map, add reprojection error */
+    int32_t iterations;
+    int32_t from_coarse;      /* start from the coarse level's planes */
+    int32_t pack;             /* store the packed depth map (reference default: 1) */
+} l3d_solve_opts;
+
+/* Device pointers of a stereo handle, for zero-copy interop (e.g. DLPack / torch). */
+typedef struct {
+    void* images;             /* n_views * height * width of the storage type */
+    uint32_t* depths;         /* depth_maps ? n_views : 1  maps of width * height */
+    float* hyp;               /* width * height * 4: normal xyz, depth */
+    float* cost;              /* width * height */
+    uint32_t* filtered;       /* width * height */
+    uint32_t* filtered_all;   /* n_views * width * height, NULL until l3d_stereo_filter_all */
+    float* hyp_all;           /* n_views * width * height * 4, NULL until l3d_stereo_solve_all */
+    float* cost_all;          /* n_views * width * height, NULL until l3d_stereo_solve_all */
+} l3d_stereo_buffers;
+
+/* Brick-sparse or dense TSDF volume: BrickGrid / TsdfVolume (fusion/tsdf-volume.ts:13-65,
+ * 158-188).  tsdf starts at 1 and weight at 0 (tsdf-volume.ts:188). */
+typedef struct {
+    double origin[3];         /* world position of voxel (0,0,0)'s corner */
+    double voxel;             /* voxel edge (m) */
+    double truncation;        /* mu (m); the reference uses 4 voxels (tsdf-volume.ts:179) */
+    double max_weight;        /* MAX_WEIGHT = 96 (tsdf-volume.ts:7) */
+    double prior_weight;      /* PRIOR_WEIGHT = 0.12 (tsdf-volume.ts:8) */
+    int32_t dense;            /* 1: dense dims[0] x dims[1] x dims[2], x fastest;
+                                 0: brick pool, voxel (brick, x, y, z) at brick*512 + x + 8y + 64z */
+    int32_t dims[3];
+    const int32_t* coords;    /* brick pool: count * 4 int32 (bx, by, bz, pad) (BrickGrid.build) */
+    int32_t count;            /* number of bricks in the pool */
+    int32_t weight_type;      /* L3D_WEIGHT_F32 or L3D_WEIGHT_Q8 */
+    int32_t width, height;    /* size of the depth maps that will be integrated */
+    void* stream;             /* cudaStream_t to run on, or NULL to create one */
+} l3d_tsdf_desc;
+
+/* IntegrationView (fusion/tsdf-volume.ts:67-79). */
+typedef struct {
+    l3d_intrinsics intrinsics;
+    l3d_pose pose;
+    double max_depth;         /* farthest depth worth integrating (m) */
+    const float* prior;       /* host, width * height (0 = none), or NULL */
+    double confidence;        /* typical scene depth for confidence weighting, 0 = off */
+} l3d_integration_view;
+
+/* ---- errors ---- */
+
+/* Copies the calling thread's last error message into buf (always NUL-terminated); returns the
+ * message length.  No reference counterpart: the reference throws JS Errors
+ * (pipeline/stages/stage-runner.ts:40-49, gpu/gpu-device.ts:92-100). */
+size_t l3d_last_error(char* buf, size_t size);
+
+/* ---- stereo: DenseStereo (mvs/dense-stereo.ts:107-416) ---- */
+
+/* Fills the reference defaults: depth_maps 1, storage F32, form PLAIN, window 6, dilation 2. */
+void l3d_stereo_opts_default(l3d_stereo_opts* opts);
+
+/* new DenseStereo(device, width, height, views, options) (dense-stereo.ts:126-218). */
+int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_view* views,
+                      const l3d_stereo_opts* opts, l3d_stereo** out);
+
+/* DenseStereo.setImage(layer, gray) (dense-stereo.ts:221-228).  dtype is the host element type;
+ * row_stride_bytes = 0 means tightly packed rows. */
+int l3d_stereo_set_image(l3d_stereo* s, int32_t layer, int32_t dtype, const void* pixels,
+                         int64_t row_stride_bytes);
+
+/* DenseStereo.solve(ref, options) (dense-stereo.ts:231-285): init (or init_coarse), iterations
+ * x red/black propagate, pack. */
+int l3d_stereo_solve(l3d_stereo* s, int32_t ref, const l3d_solve_opts* opts);
+
+/* The photometric stage for many reference views at once (reconstructor.ts:88-94 loops
+ * StereoRun.solve over layers).  opts[i] belongs to refs[i].  Each view's hypotheses live in
+ * hyp_all/cost_all; packed maps land in depths[ref] exactly as a sequence of solve() calls
+ * would leave them.  Geometric passes read the maps as they were when the call started
+ * (Jacobi order), a documented difference from per-view solve() calls (Gauss-Seidel). */
+int l3d_stereo_solve_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
+                         const l3d_solve_opts* opts);
+
+/* One kernel of the schedule over the whole image of view ref, with the dispatch state of
+ * (iteration, phase): the unit DenseStereo.sliced submits (dense-stereo.ts:315-335). */
+int l3d_stereo_dispatch(l3d_stereo* s, int32_t kernel, int32_t ref, const l3d_solve_opts* opts,
+                        int32_t iteration, int32_t phase);
+
+/* DenseStereo.filter(ref, sources, needed) (dense-stereo.ts:296-309): consistency filter of
+ * depths[ref] into the filtered map. */
+int l3d_stereo_filter(l3d_stereo* s, int32_t ref, const int32_t* checks, int32_t n_checks,
+                      int32_t needed);
+
+/* filter() for many views into filtered_all[layer] (the loop of fusion/tsdf-meshing.ts:72-83
+ * and depth-fusion.ts:34).  checks: n_refs * 8 layers, -1 padded; needed: n_refs values. */
+int l3d_stereo_filter_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
+                          const int32_t* checks, const int32_t* needed);
+
+/* Reads (block until the handle's queued work is done). */
+/* DenseStereo.filteredMap readback (dense-stereo.ts:347-352) of the filtered map. */
+int l3d_stereo_read_filtered(l3d_stereo* s, uint32_t* out);
+/* filtered_all[layer]. */
+int l3d_stereo_read_filtered_layer(l3d_stereo* s, int32_t layer, uint32_t* out);
+/* DenseStereo.depthMap(ref) (dense-stereo.ts:355-358). */
+int l3d_stereo_read_depth(l3d_stereo* s, int32_t ref, uint32_t* out);
+/* DenseStereo.hypotheses (dense-stereo.ts:288-290) and the cost buffer; hyp4 is
+ * width * height * 4 floats (normal xyz, depth).  Either pointer may be NULL. */
+int l3d_stereo_read_hyp(l3d_stereo* s, float* hyp4, float* cost);
+/* hyp_all/cost_all of one layer after solve_all. */
+int l3d_stereo_read_hyp_layer(l3d_stereo* s, int32_t layer, float* hyp4, float* cost);
+
+/* State uploads (no reference counterpart; they restore a saved state, e.g. to run one kernel
+ * from a known state, like the session snapshot of pipeline/reconstructor.ts:49-51). */
+int l3d_stereo_write_hyp(l3d_stereo* s, const float* hyp4, const float* cost);
+int l3d_stereo_write_depth(l3d_stereo* s, int32_t ref, const uint32_t* packed);
+
+/* hypothesis_cost of given planes at every pixel of view ref (patchmatch.wgsl.ts:192-233):
+ * planes is width * height * 4 floats (normal, depth); view_costs (NULL or width*height*8)
+ * receives the per-source costs. */
+int l3d_stereo_plane_cost(l3d_stereo* s, int32_t ref, const l3d_solve_opts* opts,
+                          const float* planes, float* cost, float* view_costs);
+
+int l3d_stereo_buffers_get(const l3d_stereo* s, l3d_stereo_buffers* out);
+/* The handle's cudaStream_t (as void*). */
+int l3d_stereo_stream(const l3d_stereo* s, void** stream);
+int l3d_stereo_synchronize(l3d_stereo* s);
+/* Device kernels launched by this handle since creation (for launch accounting). */
+int64_t l3d_stereo_launches(const l3d_stereo* s);
+/* DenseStereo.destroy() (dense-stereo.ts:403-416). */
+void l3d_stereo_destroy(l3d_stereo* s);
+
+/* ---- TSDF: TsdfVolume (fusion/tsdf-volume.ts:158-291) ---- */
+
+/* new TsdfVolume(device, grid, layout, depthBuffer, width, height) (tsdf-volume.ts:171-222). */
+int l3d_tsdf_create(const l3d_tsdf_desc* desc, l3d_tsdf** out);
+
+/* TsdfVolume.integrate(view) (tsdf-volume.ts:445-473): integrates one packed depth map, either
+ * the filtered map of stereo (src != NULL, the buffer shared at tsdf-meshing.ts:71) or a host
+ * map (packed, width * height u32).  Brick culling (visibleBricks, tsdf-volume.ts:425-439) runs
+ * on the device. */
+int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packed,
+                       const l3d_integration_view* view);
+
+/* Integrates n depth maps in one sweep over the volume (each voxel read and written once);
+ * equal, bit for bit, to n integrate() calls in order.  Maps come from src's filtered_all
+ * (src != NULL, layers[i]) or from packed (host, n * width * height). */
+int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                            const uint32_t* packed, int32_t n, const l3d_integration_view* views);
+
+/* TsdfVolume.read() (tsdf-volume.ts:475-482).  weight is float* (F32) or uint16_t* (Q8).
+ * Either pointer may be NULL. */
+int l3d_tsdf_read(l3d_tsdf* t, float* tsdf, void* weight);
+/* Back to the initial state (tsdf 1, weight 0). */
+int l3d_tsdf_reset(l3d_tsdf* t);
+/* Voxel count (dense: product of dims; pool: count * 512). */
+int64_t l3d_tsdf_voxels(const l3d_tsdf* t);
+int l3d_tsdf_device_buffers(const l3d_tsdf* t, float** tsdf, void** weight);
+int l3d_tsdf_stream(const l3d_tsdf* t, void** stream);
+int l3d_tsdf_synchronize(l3d_tsdf* t);
+int64_t l3d_tsdf_launches(const l3d_tsdf* t);
+/* TsdfVolume.destroy() (tsdf-volume.ts:484-495). */
+void l3d_tsdf_destroy(l3d_tsdf* t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

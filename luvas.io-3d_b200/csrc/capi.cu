@@ -1,0 +1,986 @@
+/*
+ * C ABI of libluvas3d.so (declared in include/luvas3d.h): handle management, argument checks,
+ * dispatch parameters and the solve / filter / integrate schedules.
+ *
+ * The host side replaces DenseStereo and TsdfVolume (frontend/src/app/vision/mvs/dense-stereo.ts,
+ * frontend/src/app/vision/fusion/tsdf-volume.ts).  Differences from the WebGPU host, by design:
+ * whole-image launches instead of 20 ms row bands with a host wait per band
+ * (dense-stereo.ts:315-344), brick culling on the device instead of a CPU loop
+ * (tsdf-volume.ts:425-439), and stream-ordered asynchronous calls instead of awaits.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/luvas3d.h"
+#include "l3d_internal.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? L3D_ENOMEM : L3D_ECUDA, "%s: %s (%s)", what,
+                cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+#define L3D_CUDA(call, what)                          \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+size_t dtype_size(int dtype) {
+    switch (dtype) {
+        case L3D_DTYPE_U8: return 1;
+        case L3D_DTYPE_F32: return 4;
+        case L3D_DTYPE_F16:
+        case L3D_DTYPE_BF16: return 2;
+        default: return 0;
+    }
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+}  // namespace
+
+/* ------------------------------------------------------------------ stereo handle ---------- */
+
+struct l3d_stereo {
+    int W = 0, H = 0, V = 0;
+    long long P = 0;
+    std::vector<l3d_view> views;
+    l3d_stereo_opts opts{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t done = nullptr;        /* recorded after work other handles consume */
+    int n_maps = 0;
+    void* images = nullptr;            /* V * P of the storage type */
+    uint32_t* depths = nullptr;        /* n_maps * P */
+    float4* hyp = nullptr;
+    float* cost = nullptr;
+    float* prior = nullptr;
+    uint32_t* filtered = nullptr;
+    uint32_t* filtered_all = nullptr;  /* lazily: V * P */
+    float4* hyp_all = nullptr;         /* lazily: V * P */
+    float* cost_all = nullptr;
+    float* prior_all = nullptr;
+    void* staging = nullptr;           /* host image upload staging */
+    size_t staging_bytes = 0;
+    float4* planes = nullptr;          /* plane_cost scratch */
+    float* plane_out = nullptr;
+    long long launches = 0;
+};
+
+namespace {
+
+/* DenseStereo.params (dense-stereo.ts:360-401) for one dispatch, FP64 -> f32.  The homography
+ * base B = K_s R K_r^-1 and kt = K_s t are composed in FP64 here. */
+void relative_pose(const l3d_pose& a, const l3d_pose& b, double* R, double* t) {
+    /* relativePose (geometry/camera.ts:73-77), reference summation order */
+    const double* Ra = a.R;
+    const double* Rb = b.R;
+    double At[9] = {Ra[0], Ra[3], Ra[6], Ra[1], Ra[4], Ra[7], Ra[2], Ra[5], Ra[8]};
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++)
+            R[r * 3 + c] = Rb[r * 3] * At[c] + Rb[r * 3 + 1] * At[3 + c] + Rb[r * 3 + 2] * At[6 + c];
+    for (int r = 0; r < 3; r++) {
+        double rt = R[r * 3] * a.t[0] + R[r * 3 + 1] * a.t[1] + R[r * 3 + 2] * a.t[2];
+        t[r] = b.t[r] - rt;
+    }
+}
+
+uint32_t seed_of(int ref, int iteration, int phase, int flags) {
+    uint32_t s = (uint32_t)(ref + 1) * 0x9e3779b1u;
+    return s + (uint32_t)iteration * 97u + (uint32_t)phase * 13u + (uint32_t)flags * 7u;
+}
+
+L3dParams build_params(const l3d_stereo* s, int ref, const int32_t* sources, int n, double min_depth,
+                       double max_depth, int iteration, int phase, double step, int flags,
+                       int needed, int coarse_w, int coarse_h) {
+    L3dParams p;
+    std::memset(&p, 0, sizeof(p));
+    const l3d_view& rv = s->views[ref];
+    const double kr[4] = {rv.intrinsics.fx, rv.intrinsics.fy, rv.intrinsics.cx, rv.intrinsics.cy};
+    for (int i = 0; i < 4; i++) p.k[i] = (float)kr[i];
+    p.kinv[0] = 1.0f / p.k[0];
+    p.kinv[1] = 1.0f / p.k[1];
+    p.kinv[2] = (-p.k[2]) / p.k[0];
+    p.kinv[3] = (-p.k[3]) / p.k[1];
+    p.W = s->W;
+    p.H = s->H;
+    p.ref = ref;
+    p.n = std::min(n, L3D_MAX_SOURCES);
+    p.range[0] = (float)(1.0 / min_depth);
+    p.range[1] = (float)(1.0 / max_depth);
+    p.range[2] = (float)step;
+    p.range[3] = (float)0.2;                 /* GEOMETRIC_WEIGHT, dense-stereo.ts:92 */
+    p.iter = (unsigned)iteration;
+    p.phase = (unsigned)phase;
+    p.seed = seed_of(ref, iteration, phase, flags);
+    p.flags = (unsigned)flags;
+    p.needed = (unsigned)needed;
+    if (coarse_w > 0 && coarse_h > 0) {
+        /* scaleIntrinsics (geometry/camera.ts:28-36) */
+        double sx = (double)coarse_w / s->W, sy = (double)coarse_h / s->H;
+        p.ck[0] = (float)(kr[0] * sx);
+        p.ck[1] = (float)(kr[1] * sy);
+        p.ck[2] = (float)((kr[2] + 0.5) * sx - 0.5);
+        p.ck[3] = (float)((kr[3] + 0.5) * sy - 0.5);
+        p.cW = coarse_w;
+        p.cH = coarse_h;
+    }
+    p.ref_off = (long long)ref * s->P;
+    p.ref_dep_off = s->n_maps > 1 ? (long long)ref * s->P : 0;
+    for (int k = 0; k < p.n; k++) {
+        const l3d_view& v = s->views[sources[k]];
+        const double kv[4] = {v.intrinsics.fx, v.intrinsics.fy, v.intrinsics.cx, v.intrinsics.cy};
+        double R[9], t[3];
+        relative_pose(rv.pose, v.pose, R, t);
+        L3dSrc& o = p.src[k];
+        for (int i = 0; i < 4; i++) o.k[i] = (float)kv[i];
+        for (int i = 0; i < 9; i++) o.R[i] = (float)R[i];
+        for (int i = 0; i < 3; i++) o.t[i] = (float)t[i];
+        double A[9];
+        for (int c = 0; c < 3; c++) {
+            A[0 * 3 + c] = kv[0] * R[0 * 3 + c] + kv[2] * R[2 * 3 + c];
+            A[1 * 3 + c] = kv[1] * R[1 * 3 + c] + kv[3] * R[2 * 3 + c];
+            A[2 * 3 + c] = R[2 * 3 + c];
+        }
+        for (int r = 0; r < 3; r++) {
+            o.B[r * 3 + 0] = (float)(A[r * 3 + 0] / kr[0]);
+            o.B[r * 3 + 1] = (float)(A[r * 3 + 1] / kr[1]);
+            o.B[r * 3 + 2] =
+                (float)(A[r * 3 + 2] - A[r * 3 + 0] * kr[2] / kr[0] - A[r * 3 + 1] * kr[3] / kr[1]);
+        }
+        o.kt[0] = (float)(kv[0] * t[0] + kv[2] * t[2]);
+        o.kt[1] = (float)(kv[1] * t[1] + kv[3] * t[2]);
+        o.kt[2] = (float)t[2];
+        o.layer = sources[k];
+        o.W = s->W;
+        o.H = s->H;
+        o.img_off = (long long)sources[k] * s->P;
+        o.dep_off = s->n_maps > 1 ? (long long)sources[k] * s->P : 0;
+    }
+    return p;
+}
+
+L3dStereoDev dev_of(const l3d_stereo* s) {
+    L3dStereoDev d;
+    d.images = (const float*)s->images;
+    d.images_lp = s->images;
+    d.hyp = s->hyp;
+    d.cost = s->cost;
+    d.prior = nullptr;
+    d.depths = s->depths;
+    d.filtered = s->filtered;
+    d.coarse = s->opts.coarse ? s->opts.coarse->hyp : nullptr;
+    return d;
+}
+
+int check_sources(const l3d_stereo* s, const int32_t* src, int n) {
+    if (n < 0) return fail(L3D_EINVAL, "negative source count");
+    if (n > 0 && !src) return fail(L3D_EINVAL, "sources is NULL");
+    for (int k = 0; k < std::min(n, L3D_MAX_SOURCES); k++)
+        if (src[k] < 0 || src[k] >= s->V)
+            return fail(L3D_EINVAL, "source layer %d out of range [0, %d)", src[k], s->V);
+    return L3D_OK;
+}
+
+int check_solve(const l3d_stereo* s, int ref, const l3d_solve_opts* o) {
+    if (!s) return fail(L3D_EINVAL, "stereo handle is NULL");
+    if (!o) return fail(L3D_EINVAL, "solve options are NULL");
+    if (ref < 0 || ref >= s->V) return fail(L3D_EINVAL, "reference layer %d out of range [0, %d)", ref, s->V);
+    int rc = check_sources(s, o->sources, o->n_sources);
+    if (rc) return rc;
+    if (!(o->min_depth > 0.0) || !(o->max_depth > o->min_depth))
+        return fail(L3D_EINVAL, "depth range must satisfy 0 < min_depth < max_depth");
+    if (o->iterations < 0) return fail(L3D_EINVAL, "negative iteration count");
+    if ((o->geometric || o->pack) && s->n_maps == 1 && s->V > 1)
+        return fail(L3D_ESTATE, "handle was created without per-view depth maps");
+    if (o->from_coarse && !s->opts.coarse)
+        return fail(L3D_ESTATE, "from_coarse needs a coarse level");
+    return L3D_OK;
+}
+
+int upload_prior(l3d_stereo* s, const float* prior, float* dst) {
+    L3D_CUDA(cudaMemcpyAsync(dst, prior, s->P * sizeof(float), cudaMemcpyHostToDevice, s->stream),
+             "prior upload");
+    return L3D_OK;
+}
+
+int launch(l3d_stereo* s, int kernel, const L3dParams& p, const L3dStereoDev& d) {
+    cudaError_t e = l3d_launch_plain(kernel, p, d, s->opts.window, s->opts.dilation, s->stream);
+    s->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return L3D_OK;
+}
+
+/* One reference view through the schedule of DenseStereo.solve (dense-stereo.ts:231-285),
+ * on hypothesis buffers hyp/cost. */
+int solve_one(l3d_stereo* s, int ref, const l3d_solve_opts* o, float4* hyp, float* cost,
+              float* prior_dev) {
+    int n = std::min(o->n_sources, L3D_MAX_SOURCES);
+    if (n == 0) return L3D_OK;                            /* dense-stereo.ts:233 */
+    const int flags = o->geometric ? 1 : 0;
+    L3dStereoDev d = dev_of(s);
+    d.hyp = hyp;
+    d.cost = cost;
+    if (o->prior && !o->geometric) {
+        int rc = upload_prior(s, o->prior, prior_dev);
+        if (rc) return rc;
+        d.prior = prior_dev;
+    }
+    int cw = 0, ch = 0;
+    if (s->opts.coarse) {
+        cw = s->opts.coarse->W;
+        ch = s->opts.coarse->H;
+    }
+    const bool coarse = o->from_coarse && s->opts.coarse;
+    L3dParams p = build_params(s, ref, o->sources, n, o->min_depth, o->max_depth, 0, 0, 1.0, flags,
+                               0, cw, ch);
+    int rc = launch(s, coarse ? L3D_K_INIT_COARSE : L3D_K_INIT, p, d);
+    if (rc) return rc;
+    for (int it = 0; it < o->iterations; it++) {
+        double step = std::pow(0.5, it);
+        for (int phase = 0; phase < 2; phase++) {
+            p = build_params(s, ref, o->sources, n, o->min_depth, o->max_depth, it, phase, step,
+                             flags, 0, cw, ch);
+            rc = launch(s, L3D_K_PROPAGATE, p, d);
+            if (rc) return rc;
+        }
+    }
+    if (o->pack) {
+        p = build_params(s, ref, o->sources, n, o->min_depth, o->max_depth, 0, 0, 0.0, flags, 0,
+                         cw, ch);
+        rc = launch(s, L3D_K_PACK, p, d);
+        if (rc) return rc;
+    }
+    return L3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t l3d_last_error(char* buf, size_t size) {
+    if (buf && size) {
+        size_t n = std::min(size - 1, g_error.size());
+        std::memcpy(buf, g_error.data(), n);
+        buf[n] = 0;
+    }
+    return g_error.size();
+}
+
+void l3d_stereo_opts_default(l3d_stereo_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->depth_maps = 1;
+    o->storage = L3D_DTYPE_F32;
+    o->form = L3D_FORM_PLAIN;
+    o->window = 6;
+    o->dilation = 2;
+}
+
+int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_view* views,
+                      const l3d_stereo_opts* opts, l3d_stereo** out) {
+    if (!out) return fail(L3D_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (width <= 0 || height <= 0) return fail(L3D_EINVAL, "image size must be positive");
+    if ((long long)width * height >= (1ll << 31)) return fail(L3D_EINVAL, "image too large");
+    if (n_views <= 0 || !views) return fail(L3D_EINVAL, "need at least one view");
+    l3d_stereo_opts o;
+    if (opts) o = *opts;
+    else l3d_stereo_opts_default(&o);
+    if (!((o.window == 6 && o.dilation == 2) || (o.window == 11 && o.dilation == 1)))
+        return fail(L3D_EINVAL, "window %d / dilation %d not supported (6/2 or 11/1)", o.window, o.dilation);
+    if (o.form != L3D_FORM_PLAIN && o.form != L3D_FORM_FAST)
+        return fail(L3D_EINVAL, "unknown form %d", o.form);
+    if (o.form == L3D_FORM_PLAIN && o.storage != L3D_DTYPE_F32)
+        return fail(L3D_EINVAL, "the plain form stores images as F32");
+    if (o.storage != L3D_DTYPE_F32 && o.storage != L3D_DTYPE_F16 && o.storage != L3D_DTYPE_BF16)
+        return fail(L3D_EINVAL, "image storage must be F32, F16 or BF16");
+    if (o.form == L3D_FORM_FAST)
+        return fail(L3D_EINVAL, "the fast form is not available in this build");
+    for (int i = 0; i < n_views; i++) {
+        const l3d_intrinsics& k = views[i].intrinsics;
+        if (!(k.fx != 0.0) || !(k.fy != 0.0) || !std::isfinite(k.fx) || !std::isfinite(k.fy))
+            return fail(L3D_EINVAL, "view %d has a zero or non-finite focal length", i);
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "no CUDA device");
+    l3d_stereo* s = new (std::nothrow) l3d_stereo();
+    if (!s) return fail(L3D_ENOMEM, "host allocation failed");
+    s->W = width;
+    s->H = height;
+    s->V = n_views;
+    s->P = (long long)width * height;
+    s->views.assign(views, views + n_views);
+    s->opts = o;
+    s->n_maps = o.depth_maps ? n_views : 1;
+    auto cleanup = [&](int rc) {
+        l3d_stereo_destroy(s);
+        return rc;
+    };
+    if (o.stream) {
+        s->stream = (cudaStream_t)o.stream;
+    } else {
+        e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "stream creation"));
+        s->own_stream = true;
+    }
+    e = cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "event creation"));
+    size_t esize = dtype_size(o.storage);
+    if ((e = cudaMalloc(&s->images, (size_t)n_views * s->P * esize)) != cudaSuccess ||
+        (e = dalloc(&s->depths, (size_t)s->n_maps * s->P)) != cudaSuccess ||
+        (e = dalloc(&s->hyp, (size_t)s->P)) != cudaSuccess ||
+        (e = dalloc(&s->cost, (size_t)s->P)) != cudaSuccess ||
+        (e = dalloc(&s->prior, (size_t)s->P)) != cudaSuccess ||
+        (e = dalloc(&s->filtered, (size_t)s->P)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "device allocation"));
+    /* zero-initialised like WebGPU buffers */
+    if ((e = cudaMemsetAsync(s->images, 0, (size_t)n_views * s->P * esize, s->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(s->depths, 0, (size_t)s->n_maps * s->P * 4, s->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(s->hyp, 0, (size_t)s->P * 16, s->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(s->cost, 0, (size_t)s->P * 4, s->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(s->prior, 0, (size_t)s->P * 4, s->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(s->filtered, 0, (size_t)s->P * 4, s->stream)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "device clear"));
+    *out = s;
+    return L3D_OK;
+}
+
+int l3d_stereo_set_image(l3d_stereo* s, int32_t layer, int32_t dtype, const void* pixels,
+                         int64_t row_stride_bytes) {
+    if (!s || !pixels) return fail(L3D_EINVAL, "NULL handle or pixels");
+    if (layer < 0 || layer >= s->V) return fail(L3D_EINVAL, "layer %d out of range [0, %d)", layer, s->V);
+    size_t es = dtype_size(dtype);
+    if (!es) return fail(L3D_EINVAL, "unknown dtype %d", dtype);
+    size_t row = (size_t)s->W * es;
+    size_t stride = row_stride_bytes ? (size_t)row_stride_bytes : row;
+    if (stride < row) return fail(L3D_EINVAL, "row stride smaller than a row");
+    size_t need = row * s->H;
+    if (s->staging_bytes < need) {
+        if (s->staging) {
+            cudaStreamSynchronize(s->stream);
+            cudaFree(s->staging);
+            s->staging = nullptr;
+            s->staging_bytes = 0;
+        }
+        L3D_CUDA(cudaMalloc(&s->staging, need), "staging allocation");
+        s->staging_bytes = need;
+    }
+    L3D_CUDA(cudaMemcpy2DAsync(s->staging, row, pixels, stride, row, s->H, cudaMemcpyHostToDevice,
+                               s->stream),
+             "image upload");
+    size_t out_es = dtype_size(s->opts.storage);
+    void* dst = (char*)s->images + (size_t)layer * s->P * out_es;
+    cudaError_t e = l3d_launch_convert(s->staging, dtype, (int64_t)row, s->W, s->H, dst,
+                                       s->opts.storage, s->stream);
+    s->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "image conversion");
+    return L3D_OK;
+}
+
+int l3d_stereo_solve(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o) {
+    int rc = check_solve(s, ref, o);
+    if (rc) return rc;
+    return solve_one(s, ref, o, s->hyp, s->cost, s->prior);
+}
+
+int l3d_stereo_solve_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
+                         const l3d_solve_opts* opts) {
+    if (!s || n_refs < 0 || (n_refs > 0 && (!refs || !opts)))
+        return fail(L3D_EINVAL, "bad arguments to solve_all");
+    for (int i = 0; i < n_refs; i++) {
+        int rc = check_solve(s, refs[i], &opts[i]);
+        if (rc) return rc;
+    }
+    if (!s->hyp_all) {
+        L3D_CUDA(dalloc(&s->hyp_all, (size_t)s->V * s->P), "hyp_all allocation");
+        L3D_CUDA(dalloc(&s->cost_all, (size_t)s->V * s->P), "cost_all allocation");
+        L3D_CUDA(dalloc(&s->prior_all, (size_t)s->V * s->P), "prior_all allocation");
+    }
+    for (int i = 0; i < n_refs; i++) {
+        int r = refs[i];
+        int rc = solve_one(s, r, &opts[i], s->hyp_all + (size_t)r * s->P, s->cost_all + (size_t)r * s->P,
+                           s->prior_all + (size_t)r * s->P);
+        if (rc) return rc;
+    }
+    return L3D_OK;
+}
+
+int l3d_stereo_dispatch(l3d_stereo* s, int32_t kernel, int32_t ref, const l3d_solve_opts* o,
+                        int32_t iteration, int32_t phase) {
+    if (kernel == L3D_KERNEL_CONSISTENCY) return fail(L3D_EINVAL, "use l3d_stereo_filter");
+    int rc = check_solve(s, ref, o);
+    if (rc) return rc;
+    if (kernel < L3D_KERNEL_INIT || kernel > L3D_KERNEL_PACK)
+        return fail(L3D_EINVAL, "unknown kernel %d", kernel);
+    if (kernel == L3D_KERNEL_INIT_COARSE && !s->opts.coarse)
+        return fail(L3D_ESTATE, "init_coarse needs a coarse level");
+    if (phase != 0 && phase != 1) return fail(L3D_EINVAL, "phase must be 0 or 1");
+    int n = std::min(o->n_sources, L3D_MAX_SOURCES);
+    L3dStereoDev d = dev_of(s);
+    if (kernel == L3D_KERNEL_INIT && o->prior && !o->geometric) {
+        rc = upload_prior(s, o->prior, s->prior);
+        if (rc) return rc;
+        d.prior = s->prior;
+    }
+    int cw = s->opts.coarse ? s->opts.coarse->W : 0, ch = s->opts.coarse ? s->opts.coarse->H : 0;
+    double step = kernel == L3D_KERNEL_PACK ? 0.0 : std::pow(0.5, iteration);
+    L3dParams p = build_params(s, ref, o->sources, n, o->min_depth, o->max_depth, iteration, phase,
+                               step, o->geometric ? 1 : 0, 0, cw, ch);
+    return launch(s, kernel, p, d);
+}
+
+int l3d_stereo_filter(l3d_stereo* s, int32_t ref, const int32_t* checks, int32_t n, int32_t needed) {
+    if (!s) return fail(L3D_EINVAL, "stereo handle is NULL");
+    if (ref < 0 || ref >= s->V) return fail(L3D_EINVAL, "reference layer %d out of range", ref);
+    int rc = check_sources(s, checks, n);
+    if (rc) return rc;
+    if (s->n_maps == 1 && s->V > 1) return fail(L3D_ESTATE, "handle was created without per-view depth maps");
+    /* DenseStereo.filter (dense-stereo.ts:296-309): range 0.01 - 100 m, no flags */
+    L3dParams p = build_params(s, ref, checks, std::min(n, L3D_MAX_SOURCES), 0.01, 100.0, 0, 0, 0.0,
+                               0, needed, 0, 0);
+    return launch(s, L3D_K_CONSISTENCY, p, dev_of(s));
+}
+
+int l3d_stereo_filter_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs, const int32_t* checks,
+                          const int32_t* needed) {
+    if (!s || n_refs < 0 || (n_refs > 0 && (!refs || !checks || !needed)))
+        return fail(L3D_EINVAL, "bad arguments to filter_all");
+    if (s->n_maps == 1 && s->V > 1) return fail(L3D_ESTATE, "handle was created without per-view depth maps");
+    if (!s->filtered_all) L3D_CUDA(dalloc(&s->filtered_all, (size_t)s->V * s->P), "filtered_all allocation");
+    for (int i = 0; i < n_refs; i++) {
+        int r = refs[i];
+        if (r < 0 || r >= s->V) return fail(L3D_EINVAL, "reference layer %d out of range", r);
+        int32_t src[L3D_MAX_SOURCES];
+        int n = 0;
+        for (int k = 0; k < L3D_MAX_SOURCES; k++)
+            if (checks[i * L3D_MAX_SOURCES + k] >= 0) src[n++] = checks[i * L3D_MAX_SOURCES + k];
+        int rc = check_sources(s, src, n);
+        if (rc) return rc;
+        L3dParams p = build_params(s, r, src, n, 0.01, 100.0, 0, 0, 0.0, 0, needed[i], 0, 0);
+        L3dStereoDev d = dev_of(s);
+        d.filtered = s->filtered_all + (size_t)r * s->P;
+        rc = launch(s, L3D_K_CONSISTENCY, p, d);
+        if (rc) return rc;
+    }
+    return L3D_OK;
+}
+
+static int read_dev(l3d_stereo* s, void* dst, const void* src, size_t bytes, const char* what) {
+    L3D_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->stream), what);
+    L3D_CUDA(cudaStreamSynchronize(s->stream), what);
+    return L3D_OK;
+}
+
+int l3d_stereo_read_filtered(l3d_stereo* s, uint32_t* out) {
+    if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
+    return read_dev(s, out, s->filtered, s->P * 4, "read filtered");
+}
+
+int l3d_stereo_read_filtered_layer(l3d_stereo* s, int32_t layer, uint32_t* out) {
+    if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
+    if (layer < 0 || layer >= s->V) return fail(L3D_EINVAL, "layer out of range");
+    if (!s->filtered_all) return fail(L3D_ESTATE, "no filter_all has run");
+    return read_dev(s, out, s->filtered_all + (size_t)layer * s->P, s->P * 4, "read filtered layer");
+}
+
+int l3d_stereo_read_depth(l3d_stereo* s, int32_t ref, uint32_t* out) {
+    if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
+    if (ref < 0 || ref >= s->n_maps) return fail(L3D_EINVAL, "depth map %d out of range", ref);
+    return read_dev(s, out, s->depths + (size_t)ref * s->P, s->P * 4, "read depth");
+}
+
+int l3d_stereo_read_hyp(l3d_stereo* s, float* hyp4, float* cost) {
+    if (!s) return fail(L3D_EINVAL, "NULL handle");
+    if (hyp4) {
+        int rc = read_dev(s, hyp4, s->hyp, s->P * 16, "read hypotheses");
+        if (rc) return rc;
+    }
+    if (cost) return read_dev(s, cost, s->cost, s->P * 4, "read costs");
+    return L3D_OK;
+}
+
+int l3d_stereo_read_hyp_layer(l3d_stereo* s, int32_t layer, float* hyp4, float* cost) {
+    if (!s) return fail(L3D_EINVAL, "NULL handle");
+    if (layer < 0 || layer >= s->V) return fail(L3D_EINVAL, "layer out of range");
+    if (!s->hyp_all) return fail(L3D_ESTATE, "no solve_all has run");
+    if (hyp4) {
+        int rc = read_dev(s, hyp4, s->hyp_all + (size_t)layer * s->P, s->P * 16, "read hypotheses");
+        if (rc) return rc;
+    }
+    if (cost) return read_dev(s, cost, s->cost_all + (size_t)layer * s->P, s->P * 4, "read costs");
+    return L3D_OK;
+}
+
+int l3d_stereo_write_hyp(l3d_stereo* s, const float* hyp4, const float* cost) {
+    if (!s) return fail(L3D_EINVAL, "NULL handle");
+    if (hyp4) L3D_CUDA(cudaMemcpyAsync(s->hyp, hyp4, s->P * 16, cudaMemcpyHostToDevice, s->stream), "write hypotheses");
+    if (cost) L3D_CUDA(cudaMemcpyAsync(s->cost, cost, s->P * 4, cudaMemcpyHostToDevice, s->stream), "write costs");
+    return L3D_OK;
+}
+
+int l3d_stereo_write_depth(l3d_stereo* s, int32_t ref, const uint32_t* packed) {
+    if (!s || !packed) return fail(L3D_EINVAL, "NULL argument");
+    if (ref < 0 || ref >= s->n_maps) return fail(L3D_EINVAL, "depth map %d out of range", ref);
+    L3D_CUDA(cudaMemcpyAsync(s->depths + (size_t)ref * s->P, packed, s->P * 4, cudaMemcpyHostToDevice,
+                             s->stream),
+             "write depth");
+    return L3D_OK;
+}
+
+int l3d_stereo_plane_cost(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o, const float* planes,
+                          float* cost, float* view_costs) {
+    int rc = check_solve(s, ref, o);
+    if (rc) return rc;
+    if (!planes || !cost) return fail(L3D_EINVAL, "NULL planes or cost");
+    if (!s->planes) {
+        L3D_CUDA(dalloc(&s->planes, (size_t)s->P), "plane scratch");
+        L3D_CUDA(dalloc(&s->plane_out, (size_t)s->P * (1 + L3D_MAX_SOURCES)), "plane scratch");
+    }
+    L3D_CUDA(cudaMemcpyAsync(s->planes, planes, s->P * 16, cudaMemcpyHostToDevice, s->stream), "planes upload");
+    int n = std::min(o->n_sources, L3D_MAX_SOURCES);
+    L3dParams p = build_params(s, ref, o->sources, n, o->min_depth, o->max_depth, 0, 0, 1.0,
+                               o->geometric ? 1 : 0, 0, 0, 0);
+    cudaError_t e = l3d_launch_plane_cost(p, dev_of(s), s->planes, s->plane_out, s->plane_out + s->P,
+                                          s->opts.window, s->opts.dilation, s->stream);
+    s->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "plane cost launch");
+    rc = read_dev(s, cost, s->plane_out, s->P * 4, "read plane cost");
+    if (rc) return rc;
+    if (view_costs) return read_dev(s, view_costs, s->plane_out + s->P, s->P * 4 * L3D_MAX_SOURCES, "read view costs");
+    return L3D_OK;
+}
+
+int l3d_stereo_buffers_get(const l3d_stereo* s, l3d_stereo_buffers* out) {
+    if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
+    out->images = s->images;
+    out->depths = s->depths;
+    out->hyp = (float*)s->hyp;
+    out->cost = s->cost;
+    out->filtered = s->filtered;
+    out->filtered_all = s->filtered_all;
+    out->hyp_all = (float*)s->hyp_all;
+    out->cost_all = s->cost_all;
+    return L3D_OK;
+}
+
+int l3d_stereo_stream(const l3d_stereo* s, void** stream) {
+    if (!s || !stream) return fail(L3D_EINVAL, "NULL argument");
+    *stream = (void*)s->stream;
+    return L3D_OK;
+}
+
+int l3d_stereo_synchronize(l3d_stereo* s) {
+    if (!s) return fail(L3D_EINVAL, "NULL handle");
+    L3D_CUDA(cudaStreamSynchronize(s->stream), "synchronize");
+    return L3D_OK;
+}
+
+int64_t l3d_stereo_launches(const l3d_stereo* s) { return s ? s->launches : -1; }
+
+void l3d_stereo_destroy(l3d_stereo* s) {
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    cudaFree(s->images);
+    cudaFree(s->depths);
+    cudaFree(s->hyp);
+    cudaFree(s->cost);
+    cudaFree(s->prior);
+    cudaFree(s->filtered);
+    cudaFree(s->filtered_all);
+    cudaFree(s->hyp_all);
+    cudaFree(s->cost_all);
+    cudaFree(s->prior_all);
+    cudaFree(s->staging);
+    cudaFree(s->planes);
+    cudaFree(s->plane_out);
+    if (s->done) cudaEventDestroy(s->done);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+}  // extern "C"
+
+/* ------------------------------------------------------------------ TSDF handle ------------ */
+
+struct l3d_tsdf {
+    L3dTsdfGrid g{};
+    int q8 = 0;
+    long long voxels = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t done = nullptr;
+    cudaEvent_t staged = nullptr;     /* after the last copy out of the pinned staging tables */
+    float* tsdf = nullptr;
+    void* weight = nullptr;
+    int32_t* coords = nullptr;
+    uint8_t* mask = nullptr;          /* bricks * mask_views */
+    int mask_views = 0;
+    L3dTsdfView* views = nullptr;     /* device, capacity view_cap */
+    int view_cap = 0;
+    const uint32_t** depth_ptrs = nullptr;  /* device, capacity view_cap */
+    uint32_t* maps = nullptr;         /* uploaded host maps, map_cap * P */
+    int map_cap = 0;
+    float* priors = nullptr;          /* uploaded priors, prior_cap * P */
+    int prior_cap = 0;
+    L3dTsdfView* views_host = nullptr;      /* pinned staging for views */
+    const uint32_t** ptrs_host = nullptr;   /* pinned staging for depth pointers */
+    long long launches = 0;
+};
+
+namespace {
+
+L3dTsdfView make_view(const l3d_integration_view& v) {
+    L3dTsdfView o;
+    std::memset(&o, 0, sizeof(o));
+    const double k[4] = {v.intrinsics.fx, v.intrinsics.fy, v.intrinsics.cx, v.intrinsics.cy};
+    for (int i = 0; i < 4; i++) {
+        o.k[i] = (float)k[i];
+        o.kd[i] = k[i];
+    }
+    for (int i = 0; i < 9; i++) {
+        o.R[i] = (float)v.pose.R[i];
+        o.Rd[i] = v.pose.R[i];
+    }
+    for (int i = 0; i < 3; i++) {
+        o.t[i] = (float)v.pose.t[i];
+        o.td[i] = v.pose.t[i];
+    }
+    o.conf = (float)v.confidence;
+    o.has_prior = v.prior != nullptr;
+    o.max_depth = v.max_depth;
+    return o;
+}
+
+int ensure_views(l3d_tsdf* t, int n) {
+    if (t->view_cap >= n) return L3D_OK;
+    cudaStreamSynchronize(t->stream);
+    cudaFree(t->views);
+    cudaFree(t->depth_ptrs);
+    cudaFreeHost(t->views_host);
+    cudaFreeHost(t->ptrs_host);
+    t->views = nullptr;
+    t->depth_ptrs = nullptr;
+    t->views_host = nullptr;
+    t->ptrs_host = nullptr;
+    t->view_cap = 0;
+    L3D_CUDA(cudaMalloc(&t->views, (size_t)n * sizeof(L3dTsdfView)), "view table");
+    L3D_CUDA(cudaMalloc(&t->depth_ptrs, (size_t)n * sizeof(void*)), "view table");
+    L3D_CUDA(cudaMallocHost(&t->views_host, (size_t)n * sizeof(L3dTsdfView)), "view staging");
+    L3D_CUDA(cudaMallocHost(&t->ptrs_host, (size_t)n * sizeof(void*)), "view staging");
+    t->view_cap = n;
+    return L3D_OK;
+}
+
+int ensure_mask(l3d_tsdf* t, int n) {
+    if (t->mask_views >= n) return L3D_OK;
+    cudaStreamSynchronize(t->stream);
+    cudaFree(t->mask);
+    t->mask = nullptr;
+    t->mask_views = 0;
+    L3D_CUDA(cudaMalloc(&t->mask, (size_t)t->g.bricks * n), "brick mask");
+    t->mask_views = n;
+    return L3D_OK;
+}
+
+int ensure_maps(l3d_tsdf* t, int n) {
+    if (t->map_cap >= n) return L3D_OK;
+    cudaStreamSynchronize(t->stream);
+    cudaFree(t->maps);
+    t->maps = nullptr;
+    t->map_cap = 0;
+    L3D_CUDA(cudaMalloc(&t->maps, (size_t)n * t->g.W * t->g.H * 4), "depth map upload buffer");
+    t->map_cap = n;
+    return L3D_OK;
+}
+
+int ensure_priors(l3d_tsdf* t, int n) {
+    if (t->prior_cap >= n) return L3D_OK;
+    cudaStreamSynchronize(t->stream);
+    cudaFree(t->priors);
+    t->priors = nullptr;
+    t->prior_cap = 0;
+    L3D_CUDA(cudaMalloc(&t->priors, (size_t)n * t->g.W * t->g.H * 4), "prior upload buffer");
+    t->prior_cap = n;
+    return L3D_OK;
+}
+
+int check_view(const l3d_integration_view* v) {
+    if (!v) return fail(L3D_EINVAL, "integration view is NULL");
+    if (!(v->intrinsics.fx != 0.0) || !(v->intrinsics.fy != 0.0))
+        return fail(L3D_EINVAL, "zero focal length");
+    return L3D_OK;
+}
+
+/* Orders the TSDF stream after the stereo handle's queued work (the filtered maps). */
+int after_stereo(l3d_tsdf* t, const l3d_stereo* s) {
+    L3D_CUDA(cudaEventRecord(s->done, s->stream), "event record");
+    L3D_CUDA(cudaStreamWaitEvent(t->stream, s->done, 0), "stream wait");
+    return L3D_OK;
+}
+/* Orders the stereo stream after the TSDF kernels that read its maps. */
+int before_stereo(l3d_tsdf* t, const l3d_stereo* s) {
+    L3D_CUDA(cudaEventRecord(t->done, t->stream), "event record");
+    L3D_CUDA(cudaStreamWaitEvent(s->stream, t->done, 0), "stream wait");
+    return L3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int l3d_tsdf_create(const l3d_tsdf_desc* d, l3d_tsdf** out) {
+    if (!out) return fail(L3D_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!d) return fail(L3D_EINVAL, "descriptor is NULL");
+    if (!(d->voxel > 0.0) || !(d->truncation > 0.0) || !(d->max_weight > 0.0))
+        return fail(L3D_EINVAL, "voxel, truncation and max_weight must be positive");
+    if (d->width <= 0 || d->height <= 0) return fail(L3D_EINVAL, "depth map size must be positive");
+    if (d->weight_type != L3D_WEIGHT_F32 && d->weight_type != L3D_WEIGHT_Q8)
+        return fail(L3D_EINVAL, "unknown weight type %d", d->weight_type);
+    if (d->weight_type == L3D_WEIGHT_Q8 && !(d->max_weight * 256.0 <= 65535.0))
+        return fail(L3D_EINVAL, "Q8.8 weights need max_weight <= 255.99");
+    L3dTsdfGrid g;
+    std::memset(&g, 0, sizeof(g));
+    if (d->dense) {
+        for (int i = 0; i < 3; i++) {
+            if (d->dims[i] <= 0) return fail(L3D_EINVAL, "dense dims must be positive");
+            g.dims[i] = d->dims[i];
+            g.nb[i] = (d->dims[i] + 7) / 8;
+        }
+        g.bricks = (long long)g.nb[0] * g.nb[1] * g.nb[2];
+    } else {
+        if (d->count <= 0 || !d->coords) return fail(L3D_EINVAL, "brick pool needs coords and count > 0");
+        g.bricks = d->count;
+    }
+    for (int i = 0; i < 3; i++) {
+        g.origin[i] = (float)d->origin[i];
+        g.origin_d[i] = d->origin[i];
+    }
+    g.voxel = (float)d->voxel;
+    g.mu = (float)d->truncation;
+    g.prior_weight = (float)d->prior_weight;
+    g.max_weight = (float)d->max_weight;
+    g.max_q = (unsigned)rintf(g.max_weight * 256.0f);
+    g.voxel_d = d->voxel;
+    g.trunc_d = d->truncation;
+    g.dense = d->dense ? 1 : 0;
+    g.W = d->width;
+    g.H = d->height;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "no CUDA device");
+    l3d_tsdf* t = new (std::nothrow) l3d_tsdf();
+    if (!t) return fail(L3D_ENOMEM, "host allocation failed");
+    t->g = g;
+    t->q8 = d->weight_type == L3D_WEIGHT_Q8;
+    t->voxels = g.dense ? (long long)g.dims[0] * g.dims[1] * g.dims[2] : g.bricks * 512;
+    auto cleanup = [&](int rc) {
+        l3d_tsdf_destroy(t);
+        return rc;
+    };
+    if (d->stream) {
+        t->stream = (cudaStream_t)d->stream;
+    } else {
+        e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "stream creation"));
+        t->own_stream = true;
+    }
+    if ((e = cudaEventCreateWithFlags(&t->done, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&t->staged, cudaEventDisableTiming)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "event creation"));
+    if ((e = cudaMalloc(&t->tsdf, (size_t)t->voxels * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&t->weight, (size_t)t->voxels * (t->q8 ? 2 : 4))) != cudaSuccess)
+        return cleanup(cuda_fail(e, "volume allocation"));
+    if (!g.dense) {
+        if ((e = cudaMalloc(&t->coords, (size_t)g.bricks * 16)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "coords allocation"));
+        if ((e = cudaMemcpyAsync(t->coords, d->coords, (size_t)g.bricks * 16, cudaMemcpyHostToDevice,
+                                 t->stream)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "coords upload"));
+        if ((e = cudaStreamSynchronize(t->stream)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "coords upload"));
+    }
+    int rc = l3d_tsdf_reset(t);
+    if (rc) return cleanup(rc);
+    *out = t;
+    return L3D_OK;
+}
+
+int l3d_tsdf_reset(l3d_tsdf* t) {
+    if (!t) return fail(L3D_EINVAL, "NULL handle");
+    cudaError_t e = l3d_launch_tsdf_fill(t->tsdf, t->weight, t->voxels, t->q8, t->stream);
+    t->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "volume fill");
+    return L3D_OK;
+}
+
+int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packed,
+                       const l3d_integration_view* view) {
+    if (!t) return fail(L3D_EINVAL, "NULL handle");
+    int rc = check_view(view);
+    if (rc) return rc;
+    if ((src == nullptr) == (packed == nullptr))
+        return fail(L3D_EINVAL, "give exactly one of a stereo handle or a packed map");
+    const long long P = (long long)t->g.W * t->g.H;
+    if (src && (src->W != t->g.W || src->H != t->g.H))
+        return fail(L3D_EINVAL, "stereo size %dx%d differs from the volume's %dx%d", src->W, src->H, t->g.W, t->g.H);
+    if ((rc = ensure_mask(t, 1))) return rc;
+    L3dTsdfView v = make_view(*view);
+    const uint32_t* depth;
+    if (src) {
+        if ((rc = after_stereo(t, src))) return rc;
+        depth = src->filtered;
+    } else {
+        if ((rc = ensure_maps(t, 1))) return rc;
+        L3D_CUDA(cudaMemcpyAsync(t->maps, packed, P * 4, cudaMemcpyHostToDevice, t->stream), "map upload");
+        depth = t->maps;
+    }
+    const float* prior = nullptr;
+    if (view->prior) {
+        if ((rc = ensure_priors(t, 1))) return rc;
+        L3D_CUDA(cudaMemcpyAsync(t->priors, view->prior, P * 4, cudaMemcpyHostToDevice, t->stream), "prior upload");
+        prior = t->priors;
+    }
+    /* visibility of this view's bricks, then the integration: two launches */
+    cudaError_t e = l3d_launch_tsdf_view(t->g, v, t->coords, t->mask, depth, prior, t->tsdf, t->weight,
+                                         t->q8, t->stream);
+    t->launches += 2;
+    if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
+    if (src && (rc = before_stereo(t, src))) return rc;
+    return L3D_OK;
+}
+
+int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                            const uint32_t* packed, int32_t n, const l3d_integration_view* views) {
+    if (!t) return fail(L3D_EINVAL, "NULL handle");
+    if (n < 0 || (n > 0 && !views)) return fail(L3D_EINVAL, "bad view list");
+    if (n == 0) return L3D_OK;
+    if ((src == nullptr) == (packed == nullptr))
+        return fail(L3D_EINVAL, "give exactly one of a stereo handle or packed maps");
+    const long long P = (long long)t->g.W * t->g.H;
+    if (src) {
+        if (!layers) return fail(L3D_EINVAL, "layers is NULL");
+        if (!src->filtered_all) return fail(L3D_ESTATE, "stereo handle has no filter_all output");
+        if (src->W != t->g.W || src->H != t->g.H) return fail(L3D_EINVAL, "stereo size differs from the volume's");
+        for (int i = 0; i < n; i++)
+            if (layers[i] < 0 || layers[i] >= src->V) return fail(L3D_EINVAL, "layer %d out of range", layers[i]);
+    }
+    int rc;
+    for (int i = 0; i < n; i++)
+        if ((rc = check_view(&views[i]))) return rc;
+    if ((rc = ensure_views(t, n)) || (rc = ensure_mask(t, n))) return rc;
+    bool any_prior = false;
+    for (int i = 0; i < n; i++) any_prior |= views[i].prior != nullptr;
+    if (src) {
+        if ((rc = after_stereo(t, src))) return rc;
+    } else {
+        if ((rc = ensure_maps(t, n))) return rc;
+        L3D_CUDA(cudaMemcpyAsync(t->maps, packed, (size_t)n * P * 4, cudaMemcpyHostToDevice, t->stream), "map upload");
+    }
+    if (any_prior) {
+        if ((rc = ensure_priors(t, n))) return rc;
+        for (int i = 0; i < n; i++)
+            if (views[i].prior)
+                L3D_CUDA(cudaMemcpyAsync(t->priors + (size_t)i * P, views[i].prior, P * 4, cudaMemcpyHostToDevice, t->stream), "prior upload");
+    }
+    /* the pinned staging tables are reused: wait until the previous call's copies have run */
+    L3D_CUDA(cudaEventSynchronize(t->staged), "staging wait");
+    for (int i = 0; i < n; i++) {
+        t->views_host[i] = make_view(views[i]);
+        t->ptrs_host[i] = src ? src->filtered_all + (size_t)layers[i] * P : t->maps + (size_t)i * P;
+    }
+    L3D_CUDA(cudaMemcpyAsync(t->views, t->views_host, (size_t)n * sizeof(L3dTsdfView), cudaMemcpyHostToDevice, t->stream), "view upload");
+    L3D_CUDA(cudaMemcpyAsync(t->depth_ptrs, t->ptrs_host, (size_t)n * sizeof(void*), cudaMemcpyHostToDevice, t->stream), "view upload");
+    L3D_CUDA(cudaEventRecord(t->staged, t->stream), "event record");
+    cudaError_t e = l3d_launch_tsdf_visible(t->g, t->views, n, t->coords, t->mask, t->stream);
+    t->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "visibility launch");
+    e = l3d_launch_tsdf_many(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors, t->tsdf,
+                             t->weight, t->q8, t->stream);
+    t->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
+    if (src && (rc = before_stereo(t, src))) return rc;
+    return L3D_OK;
+}
+
+int l3d_tsdf_read(l3d_tsdf* t, float* tsdf, void* weight) {
+    if (!t) return fail(L3D_EINVAL, "NULL handle");
+    if (tsdf) L3D_CUDA(cudaMemcpyAsync(tsdf, t->tsdf, (size_t)t->voxels * 4, cudaMemcpyDeviceToHost, t->stream), "read tsdf");
+    if (weight)
+        L3D_CUDA(cudaMemcpyAsync(weight, t->weight, (size_t)t->voxels * (t->q8 ? 2 : 4), cudaMemcpyDeviceToHost, t->stream), "read weight");
+    L3D_CUDA(cudaStreamSynchronize(t->stream), "read");
+    return L3D_OK;
+}
+
+int64_t l3d_tsdf_voxels(const l3d_tsdf* t) { return t ? t->voxels : -1; }
+
+int l3d_tsdf_device_buffers(const l3d_tsdf* t, float** tsdf, void** weight) {
+    if (!t) return fail(L3D_EINVAL, "NULL handle");
+    if (tsdf) *tsdf = t->tsdf;
+    if (weight) *weight = t->weight;
+    return L3D_OK;
+}
+
+int l3d_tsdf_stream(const l3d_tsdf* t, void** stream) {
+    if (!t || !stream) return fail(L3D_EINVAL, "NULL argument");
+    *stream = (void*)t->stream;
+    return L3D_OK;
+}
+
+int l3d_tsdf_synchronize(l3d_tsdf* t) {
+    if (!t) return fail(L3D_EINVAL, "NULL handle");
+    L3D_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+    return L3D_OK;
+}
+
+int64_t l3d_tsdf_launches(const l3d_tsdf* t) { return t ? t->launches : -1; }
+
+void l3d_tsdf_destroy(l3d_tsdf* t) {
+    if (!t) return;
+    if (t->stream) cudaStreamSynchronize(t->stream);
+    cudaFree(t->tsdf);
+    cudaFree(t->weight);
+    cudaFree(t->coords);
+    cudaFree(t->mask);
+    cudaFree(t->views);
+    cudaFree(t->depth_ptrs);
+    cudaFree(t->maps);
+    cudaFree(t->priors);
+    cudaFreeHost(t->views_host);
+    cudaFreeHost(t->ptrs_host);
+    if (t->done) cudaEventDestroy(t->done);
+    if (t->staged) cudaEventDestroy(t->staged);
+    if (t->own_stream && t->stream) cudaStreamDestroy(t->stream);
+    delete t;
+}
+
+}  // extern "C"

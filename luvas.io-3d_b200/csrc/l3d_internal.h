@@ -1,0 +1,111 @@
+/*
+ * Internal types shared by the C-ABI layer and the CUDA kernels of libluvas3d.so.
+ */
+#ifndef L3D_INTERNAL_H
+#define L3D_INTERNAL_H
+
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#define L3D_MAX_SOURCES 8      /* MAX_SOURCES, mvs/dense-stereo.ts:90 */
+#define L3D_FILTER_COST 7u     /* FILTER_COST, mvs/patchmatch.wgsl.ts:43 */
+
+/* One source view of a dispatch: the View block of patchmatch.wgsl.ts:4-10 (k, R rows, t,
+ * layer) plus the homography base B = K_s R K_r^-1 and kt = K_s t composed in FP64 on the host
+ * and rounded to f32. */
+struct L3dSrc {
+    float k[4];
+    float R[9];
+    float t[3];
+    float B[9];
+    float kt[3];
+    int layer;
+    int W, H;                  /* source image size */
+    long long img_off;         /* element offset of the source image in the image array */
+    long long dep_off;         /* element offset of the source's packed depth map */
+};
+
+/* The Params block of patchmatch.wgsl.ts:12-26 as DenseStereo.params fills it
+ * (dense-stereo.ts:360-401); the band rows are gone (whole-image launches). */
+struct L3dParams {
+    float k[4];
+    float kinv[4];             /* 1/fx, 1/fy, -cx/fx, -cy/fy in f32 */
+    int W, H, ref, n;
+    float range[4];            /* 1/min depth, 1/max depth, step, geometric weight */
+    unsigned iter, phase, seed, flags, needed;
+    float ck[4];               /* coarse-level intrinsics */
+    int cW, cH;
+    long long ref_off;         /* element offset of the reference image */
+    long long ref_dep_off;     /* element offset of the reference's packed depth map */
+    L3dSrc src[L3D_MAX_SOURCES];
+};
+
+/* Per-view constants of the TSDF integrate uniform (tsdf-volume.ts:286-296), in f32, plus the
+ * FP64 pose for brick culling. */
+struct L3dTsdfView {
+    float k[4];
+    float R[9];
+    float t[3];
+    float conf;
+    int has_prior;
+    double kd[4];
+    double Rd[9];
+    double td[3];
+    double max_depth;
+};
+
+struct L3dTsdfGrid {
+    float origin[3];
+    float voxel;
+    float mu;
+    float prior_weight;
+    float max_weight;
+    unsigned max_q;            /* rint(max_weight * 256) for Q8.8 weights */
+    double origin_d[3];
+    double voxel_d;
+    double trunc_d;
+    int dense;
+    int dims[3];
+    int nb[3];                 /* bricks per axis (dense) */
+    long long bricks;          /* dense: nb product; pool: count */
+    int W, H;                  /* depth map size */
+};
+
+/* ---- launchers (stereo.cu / stereo_fast.cu / tsdf.cu); each returns cudaGetLastError() ---- */
+
+enum { L3D_K_INIT = 0, L3D_K_INIT_COARSE = 1, L3D_K_PROPAGATE = 2, L3D_K_PACK = 3,
+       L3D_K_CONSISTENCY = 4 };
+
+struct L3dStereoDev {
+    const float* images;       /* f32 storage (plain form) */
+    const void* images_lp;     /* f16/bf16 storage (fast form) */
+    float4* hyp;
+    float* cost;
+    const float* prior;        /* may be NULL */
+    uint32_t* depths;
+    uint32_t* filtered;
+    const float4* coarse;      /* may be NULL */
+};
+
+cudaError_t l3d_launch_plain(int kernel, const L3dParams& p, const L3dStereoDev& d, int win,
+                             int dil, cudaStream_t stream);
+cudaError_t l3d_launch_plane_cost(const L3dParams& p, const L3dStereoDev& d, const float4* planes,
+                                  float* cost, float* view_costs, int win, int dil,
+                                  cudaStream_t stream);
+cudaError_t l3d_launch_convert(const void* src, int dtype, int64_t row_stride, int W, int H,
+                               void* dst, int storage, cudaStream_t stream);
+
+cudaError_t l3d_launch_tsdf_visible(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
+                                    const int32_t* coords, uint8_t* mask, cudaStream_t stream);
+/* visibility of one view (into mask) followed by its integration: two launches */
+cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,
+                                 uint8_t* mask, const uint32_t* depth, const float* prior,
+                                 float* tsdf, void* weight, int q8, cudaStream_t stream);
+cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
+                                 const int32_t* coords, const uint8_t* mask,
+                                 const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                 float* tsdf, void* weight, int q8, cudaStream_t stream);
+cudaError_t l3d_launch_tsdf_fill(float* tsdf, void* weight, long long voxels, int q8,
+                                 cudaStream_t stream);
+
+#endif

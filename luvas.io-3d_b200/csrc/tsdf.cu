@@ -1,0 +1,371 @@
+/*
+ * TSDF integration of packed depth maps (frontend/src/app/vision/fusion/tsdf-volume.ts).
+ *
+ *   k_visible      visibleBricks (tsdf-volume.ts:425-439) on the device: one thread per
+ *                  (brick, view) evaluates the reference's FP64 frustum test, in the reference's
+ *                  operation order (built with --fmad=false, so no FP64 contraction).
+ *   k_integrate    one view per launch (TsdfVolume.integrate, tsdf-volume.ts:445-473).  A thread
+ *                  owns four consecutive voxels along x (inside one 8^3 brick): it computes the
+ *                  four observations from the L2-resident depth map first and touches the volume
+ *                  only when one of them updates, with one 128-bit tsdf access and one 64-bit
+ *                  (Q8.8) or 128-bit (f32) weight access.  HBM-bound.
+ *   k_integrate_many
+ *                  many views per sweep: the same thread keeps its four voxels in registers,
+ *                  applies every view in order and writes back once; per-voxel results equal the
+ *                  per-view launches bit for bit (the per-voxel update order is unchanged).
+ *
+ * Per-voxel arithmetic (tsdf-volume.ts:316-358), fixed order shared with the FP32 restatement:
+ *   world = fma(i + 0.5, voxel, origin); cam = R world + t (fma chain); pixel =
+ *   rint(fma(f * cam, 1 / cam.z, c)); weight w = max(0.2, |n . normalize(cam)|) x confidence
+ *   factor, or the prior weight; tsdf <- fma(tsdf, w0, obs * w) / (w0 + w);
+ *   weight <- min(w0 + w, max).  Q8.8 weights: w is rounded to a multiple of 1/256 first, so
+ *   weights stay exact integers.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "l3d_fmath.h"
+#include "l3d_internal.h"
+
+namespace {
+
+__device__ __forceinline__ float dot3f(float3 a, float3 b) {
+    return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x));
+}
+__device__ __forceinline__ float3 normalize3f(float3 v) {
+    float il = 1.0f / sqrtf(dot3f(v, v));
+    return make_float3(v.x * il, v.y * il, v.z * il);
+}
+__device__ __forceinline__ float maxw(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float minw(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float clampw(float v, float lo, float hi) { return minw(maxw(v, lo), hi); }
+
+__device__ __forceinline__ float3 unpack_normal(uint32_t packed) {
+    float ex = ((float)((packed >> 16) & 63u) / 63.0f) * 2.0f - 1.0f;
+    float ey = ((float)((packed >> 22) & 63u) / 63.0f) * 2.0f - 1.0f;
+    float3 n = make_float3(ex, ey, (1.0f - fabsf(ex)) - fabsf(ey));
+    if (n.z < 0.0f) {
+        float sx = n.x >= 0.0f ? 1.0f : -1.0f;
+        float sy = n.y >= 0.0f ? 1.0f : -1.0f;
+        float nx = (1.0f - fabsf(n.y)) * sx;
+        float ny = (1.0f - fabsf(n.x)) * sy;
+        n.x = nx;
+        n.y = ny;
+    }
+    return normalize3f(n);
+}
+
+/* Observation of one voxel in one view; false when the voxel is not updated. */
+__device__ __forceinline__ bool observe(const L3dTsdfGrid& g, const L3dTsdfView& v,
+                                        const uint32_t* __restrict__ depth,
+                                        const float* __restrict__ prior, int gx, int gy, int gz,
+                                        float* obs, float* wout) {
+    float wx = fmaf((float)gx + 0.5f, g.voxel, g.origin[0]);
+    float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
+    float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
+    const float* R = v.R;
+    float3 cam = make_float3(fmaf(R[2], wz, fmaf(R[1], wy, fmaf(R[0], wx, v.t[0]))),
+                             fmaf(R[5], wz, fmaf(R[4], wy, fmaf(R[3], wx, v.t[1]))),
+                             fmaf(R[8], wz, fmaf(R[7], wy, fmaf(R[6], wx, v.t[2]))));
+    if (!(cam.z > 0.01f)) return false;
+    float iz = 1.0f / cam.z;
+    float rx = rintf(fmaf(v.k[0] * cam.x, iz, v.k[2]));
+    float ry = rintf(fmaf(v.k[1] * cam.y, iz, v.k[3]));
+    if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)g.W && ry < (float)g.H)) return false;
+    long long i = (long long)(int)ry * g.W + (int)rx;
+    uint32_t packed = __ldg(depth + i);
+    float d = l3d_f16_to_f32(packed & 0xffffu);
+    float w;
+    if (d > 0.0f) {
+        float3 n = unpack_normal(packed);
+        float3 cn = normalize3f(cam);
+        w = maxw(0.2f, fabsf(dot3f(n, cn)));
+        if (v.conf > 0.0f) {
+            float c = (float)(packed >> 28) / 8.0f;
+            float r = clampw(v.conf / d, 0.5f, 2.0f);
+            w = w * ((maxw(0.15f, (1.0f - c) * (1.0f - c)) * r) * r);
+        }
+    } else {
+        d = prior ? __ldg(prior + i) : 0.0f;
+        w = g.prior_weight;
+    }
+    if (!(d > 0.0f)) return false;
+    float sdf = d - cam.z;
+    if (sdf < -g.mu) return false;
+    *obs = minw(1.0f, sdf / g.mu);
+    *wout = w;
+    return true;
+}
+
+__device__ __forceinline__ void apply_f32(float& t, float& w0, float obs, float w, float maxw_) {
+    t = fmaf(t, w0, obs * w) / (w0 + w);
+    w0 = minw(w0 + w, maxw_);
+}
+
+__device__ __forceinline__ void apply_q8(float& t, uint32_t& w0i, float obs, float w, unsigned maxq) {
+    uint32_t wi = (uint32_t)rintf(w * 256.0f);
+    if (wi == 0u) return;
+    float w0 = (float)w0i * 0.00390625f;
+    float wf = (float)wi * 0.00390625f;
+    t = fmaf(t, w0, obs * wf) / (w0 + wf);
+    w0i = min(w0i + wi, maxq);
+}
+
+/* Voxel coordinates and storage index of the first voxel of quad q (VEC consecutive x). */
+template <int VEC>
+__device__ __forceinline__ bool quad_coords(const L3dTsdfGrid& g, const int32_t* coords,
+                                            long long q, int* gx, int* gy, int* gz,
+                                            long long* idx, long long* brick) {
+    if (g.dense) {
+        long long qx = g.dims[0] / VEC;
+        long long rest = q / qx;
+        *gx = (int)(q - rest * qx) * VEC;
+        *gy = (int)(rest % g.dims[1]);
+        *gz = (int)(rest / g.dims[1]);
+        if (*gz >= g.dims[2]) return false;
+        *idx = ((long long)*gz * g.dims[1] + *gy) * g.dims[0] + *gx;
+        *brick = ((long long)(*gz >> 3) * g.nb[1] + (*gy >> 3)) * g.nb[0] + (*gx >> 3);
+    } else {
+        long long b = q / (512 / VEC);
+        if (b >= g.bricks) return false;
+        int local = (int)(q - b * (512 / VEC)) * VEC;
+        const int32_t* c = coords + b * 4;
+        *gx = c[0] * 8 + (local & 7);
+        *gy = c[1] * 8 + ((local >> 3) & 7);
+        *gz = c[2] * 8 + (local >> 6);
+        *idx = b * 512 + local;
+        *brick = b;
+    }
+    return true;
+}
+
+/* visibleBricks (tsdf-volume.ts:425-439) for brick b of view v, FP64, reference order. */
+__device__ __forceinline__ uint8_t brick_visible(const L3dTsdfGrid& g, const L3dTsdfView& v,
+                                                 const int32_t* __restrict__ coords, long long b) {
+    int bx, by, bz;
+    if (g.dense) {
+        bx = (int)(b % g.nb[0]);
+        by = (int)((b / g.nb[0]) % g.nb[1]);
+        bz = (int)(b / ((long long)g.nb[0] * g.nb[1]));
+    } else {
+        bx = coords[b * 4];
+        by = coords[b * 4 + 1];
+        bz = coords[b * 4 + 2];
+    }
+    double side = g.voxel_d * 8.0;
+    double c0 = g.origin_d[0] + (bx + 0.5) * side;
+    double c1 = g.origin_d[1] + (by + 0.5) * side;
+    double c2 = g.origin_d[2] + (bz + 0.5) * side;
+    double radius = g.voxel_d * 8.0 * 0.87 + g.trunc_d;
+    const double* R = v.Rd;
+    double p0 = R[0] * c0 + R[1] * c1 + R[2] * c2 + v.td[0];
+    double p1 = R[3] * c0 + R[4] * c1 + R[5] * c2 + v.td[1];
+    double p2 = R[6] * c0 + R[7] * c1 + R[8] * c2 + v.td[2];
+    double u = (v.kd[0] * p0) / p2 + v.kd[2];
+    double w = (v.kd[1] * p1) / p2 + v.kd[3];
+    double z = p2;
+    if (z < 0.02 - radius || z > v.max_depth + radius) return 0;
+    double margin = (v.kd[0] * radius) / fmax(0.02, z);
+    if (u < -margin || w < -margin || u > g.W + margin || w > g.H + margin) return 0;
+    return 1;
+}
+
+__global__ void k_visible(const L3dTsdfGrid g, const L3dTsdfView* __restrict__ views, int n_views,
+                          const int32_t* __restrict__ coords, uint8_t* __restrict__ mask) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.bricks * n_views) return;
+    int vi = (int)(t / g.bricks);
+    long long b = t - (long long)vi * g.bricks;
+    mask[t] = brick_visible(g, views[vi], coords, b);
+}
+
+__global__ void k_visible_one(const L3dTsdfGrid g, const L3dTsdfView v,
+                              const int32_t* __restrict__ coords, uint8_t* __restrict__ mask) {
+    long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= g.bricks) return;
+    mask[b] = brick_visible(g, v, coords, b);
+}
+
+template <int VEC, bool Q8>
+__global__ void __launch_bounds__(256) k_integrate(const L3dTsdfGrid g, const L3dTsdfView v,
+                                                   const int32_t* __restrict__ coords,
+                                                   const uint8_t* __restrict__ mask,
+                                                   const uint32_t* __restrict__ depth,
+                                                   const float* __restrict__ prior,
+                                                   float* __restrict__ tsdf, void* __restrict__ weight,
+                                                   long long quads) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= quads) return;
+    int gx, gy, gz;
+    long long idx, brick;
+    if (!quad_coords<VEC>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
+    if (!mask[brick]) return;
+    float obs[VEC], w[VEC];
+    bool ok[VEC];
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < VEC; j++) {
+        ok[j] = observe(g, v, depth, v.has_prior ? prior : nullptr, gx + j, gy, gz, &obs[j], &w[j]);
+        any |= ok[j];
+    }
+    if (!any) return;
+    if (VEC == 4) {
+        float4 t4 = *(const float4*)(tsdf + idx);
+        float t[4] = {t4.x, t4.y, t4.z, t4.w};
+        if (Q8) {
+            ushort4 w4 = *(const ushort4*)((const uint16_t*)weight + idx);
+            uint32_t wq[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (ok[j]) apply_q8(t[j], wq[j], obs[j], w[j], g.max_q);
+            *(ushort4*)((uint16_t*)weight + idx) =
+                make_ushort4((uint16_t)wq[0], (uint16_t)wq[1], (uint16_t)wq[2], (uint16_t)wq[3]);
+        } else {
+            float4 w4 = *(const float4*)((const float*)weight + idx);
+            float ww[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (ok[j]) apply_f32(t[j], ww[j], obs[j], w[j], g.max_weight);
+            *(float4*)((float*)weight + idx) = make_float4(ww[0], ww[1], ww[2], ww[3]);
+        }
+        *(float4*)(tsdf + idx) = make_float4(t[0], t[1], t[2], t[3]);
+    } else {
+        float t = tsdf[idx];
+        if (Q8) {
+            uint32_t wq = ((const uint16_t*)weight)[idx];
+            apply_q8(t, wq, obs[0], w[0], g.max_q);
+            ((uint16_t*)weight)[idx] = (uint16_t)wq;
+        } else {
+            float ww = ((const float*)weight)[idx];
+            apply_f32(t, ww, obs[0], w[0], g.max_weight);
+            ((float*)weight)[idx] = ww;
+        }
+        tsdf[idx] = t;
+    }
+}
+
+template <int VEC, bool Q8>
+__global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
+                                                        const L3dTsdfView* __restrict__ views,
+                                                        int n_views,
+                                                        const int32_t* __restrict__ coords,
+                                                        const uint8_t* __restrict__ mask,
+                                                        const uint32_t* const* __restrict__ depths,
+                                                        const float* __restrict__ priors,
+                                                        float* __restrict__ tsdf,
+                                                        void* __restrict__ weight, long long quads) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= quads) return;
+    int gx, gy, gz;
+    long long idx, brick;
+    if (!quad_coords<VEC>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
+    const long long P = (long long)g.W * g.H;
+    float t[VEC];
+    float wf[VEC];
+    uint32_t wq[VEC];
+    bool loaded = false;
+    for (int vi = 0; vi < n_views; vi++) {
+        if (!mask[(long long)vi * g.bricks + brick]) continue;
+        const L3dTsdfView& v = views[vi];
+        const uint32_t* depth = depths[vi];
+        const float* prior = v.has_prior ? priors + (long long)vi * P : nullptr;
+#pragma unroll
+        for (int j = 0; j < VEC; j++) {
+            float obs, w;
+            if (!observe(g, v, depth, prior, gx + j, gy, gz, &obs, &w)) continue;
+            if (!loaded) {
+                loaded = true;
+#pragma unroll
+                for (int k = 0; k < VEC; k++) {
+                    t[k] = tsdf[idx + k];
+                    if (Q8) wq[k] = ((const uint16_t*)weight)[idx + k];
+                    else wf[k] = ((const float*)weight)[idx + k];
+                }
+            }
+            if (Q8) apply_q8(t[j], wq[j], obs, w, g.max_q);
+            else apply_f32(t[j], wf[j], obs, w, g.max_weight);
+        }
+    }
+    if (!loaded) return;
+    if (VEC == 4) {
+        *(float4*)(tsdf + idx) = make_float4(t[0], t[1], t[2], t[3]);
+        if (Q8)
+            *(ushort4*)((uint16_t*)weight + idx) =
+                make_ushort4((uint16_t)wq[0], (uint16_t)wq[1], (uint16_t)wq[2], (uint16_t)wq[3]);
+        else
+            *(float4*)((float*)weight + idx) = make_float4(wf[0], wf[1], wf[2], wf[3]);
+    } else {
+        tsdf[idx] = t[0];
+        if (Q8) ((uint16_t*)weight)[idx] = (uint16_t)wq[0];
+        else ((float*)weight)[idx] = wf[0];
+    }
+}
+
+__global__ void k_fill(float* tsdf, void* weight, long long voxels, int q8) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= voxels) return;
+    tsdf[i] = 1.0f;
+    if (q8) ((uint16_t*)weight)[i] = 0;
+    else ((float*)weight)[i] = 0.0f;
+}
+
+inline bool vec4_ok(const L3dTsdfGrid& g) { return !g.dense || (g.dims[0] % 4 == 0); }
+
+inline long long quad_count(const L3dTsdfGrid& g, int vec) {
+    if (g.dense) return (long long)(g.dims[0] / vec) * g.dims[1] * g.dims[2];
+    return g.bricks * (512 / vec);
+}
+
+}  // namespace
+
+cudaError_t l3d_launch_tsdf_visible(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
+                                    const int32_t* coords, uint8_t* mask, cudaStream_t stream) {
+    long long n = g.bricks * n_views;
+    if (n == 0) return cudaSuccess;
+    k_visible<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(g, views_dev, n_views, coords, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,
+                                 uint8_t* mask, const uint32_t* depth, const float* prior,
+                                 float* tsdf, void* weight, int q8, cudaStream_t stream) {
+    if (g.bricks == 0) return cudaSuccess;
+    k_visible_one<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, v, coords, mask);
+    const int vec = vec4_ok(g) ? 4 : 1;
+    long long quads = quad_count(g, vec);
+    if (quads == 0) return cudaSuccess;
+    unsigned blocks = (unsigned)((quads + 255) / 256);
+    if (vec == 4) {
+        if (q8) k_integrate<4, true><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, prior, tsdf, weight, quads);
+        else k_integrate<4, false><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, prior, tsdf, weight, quads);
+    } else {
+        if (q8) k_integrate<1, true><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, prior, tsdf, weight, quads);
+        else k_integrate<1, false><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, prior, tsdf, weight, quads);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
+                                 const int32_t* coords, const uint8_t* mask,
+                                 const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                 float* tsdf, void* weight, int q8, cudaStream_t stream) {
+    const int vec = vec4_ok(g) ? 4 : 1;
+    long long quads = quad_count(g, vec);
+    if (quads == 0 || n_views == 0) return cudaSuccess;
+    unsigned blocks = (unsigned)((quads + 255) / 256);
+    if (vec == 4) {
+        if (q8) k_integrate_many<4, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, tsdf, weight, quads);
+        else k_integrate_many<4, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, tsdf, weight, quads);
+    } else {
+        if (q8) k_integrate_many<1, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, tsdf, weight, quads);
+        else k_integrate_many<1, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, tsdf, weight, quads);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_tsdf_fill(float* tsdf, void* weight, long long voxels, int q8,
+                                 cudaStream_t stream) {
+    if (voxels == 0) return cudaSuccess;
+    k_fill<<<(unsigned)((voxels + 255) / 256), 256, 0, stream>>>(tsdf, weight, voxels, q8);
+    return cudaGetLastError();
+}

@@ -1,0 +1,187 @@
+"""Seeded synthetic scenes and camera paths for the dense-reconstruction workloads.
+
+Images are ray-cast on the CPU by libl3dscene.so (csrc/scene.cpp): a unit sphere resting on the
+plane y = -1, both textured by a solid 3-octave value noise in [0, 1] (frequencies 24, 57 and
+131 per metre, amplitudes 0.5, 0.3 and 0.2), or a 4 x 3 x 2.5 m room holding textured cuboids.
+World y points up; cameras use computer-vision axes.  Every random choice derives from `seed`.
+
+Workloads (sizes as quoted for the benchmark):
+  small  8 views 320x240 on a circle of radius 1.5 m in the plane y = 0 looking at the origin,
+         fx = fy = 280, cx = 160, cy = 120; 4 sources, 3 iterations, depths 0.5-3 m;
+         TSDF 128^3 at 1 cm (centred at the origin), truncation 4 cm, uint16 weights.
+  scan   48 views 640x480 on a helix (2 turns, radius 1.2 -> 2.0 m, elevation -10 -> 40 deg),
+         fx = fy = 560, cx = 320, cy = 240; poses given to the solver carry 2 mm / 0.1 deg
+         noise, pixels Gaussian noise sigma 0.01; 8 sources, 5 iterations, depths 0.15-4 m;
+         TSDF 512^3 at 4 mm, truncation 2 cm, uint16 weights.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .camera import Intrinsics, Pose, StereoView, camera_center, look_at, rotation, views_array
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libl3dscene.so")
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise ImportError(f"{_LIB_PATH} is missing: run `python luvas.io-3d_b200/build.py`")
+        lib = C.CDLL(_LIB_PATH)
+        lib.l3d_scene_sphere.restype = C.c_int
+        lib.l3d_scene_sphere.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_uint32, C.c_double,
+                                         C.c_void_p, C.c_void_p]
+        lib.l3d_scene_room.restype = C.c_int
+        lib.l3d_scene_room.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_uint32, C.c_double,
+                                       C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+        _lib = lib
+    return _lib
+
+
+def render_sphere(views, sizes, seed: int, sigma: float = 0.0):
+    """Renders the sphere scene: lists of (H, W) float32 images and ground-truth z-depths."""
+    va = views_array(views)
+    sz = np.ascontiguousarray(np.asarray(sizes, dtype=np.int32).reshape(-1, 2))
+    total = int((sz[:, 0].astype(np.int64) * sz[:, 1]).sum())
+    img = np.empty(total, dtype=np.float32)
+    dep = np.empty(total, dtype=np.float32)
+    rc = _load().l3d_scene_sphere(va.ctypes.data, sz.ctypes.data, len(views), seed & 0xFFFFFFFF,
+                                  float(sigma), img.ctypes.data, dep.ctypes.data)
+    if rc:
+        raise RuntimeError("scene rendering failed")
+    return _split(img, sz), _split(dep, sz)
+
+
+def render_room(views, sizes, boxes: np.ndarray, seed: int, sigma: float = 0.0):
+    va = views_array(views)
+    sz = np.ascontiguousarray(np.asarray(sizes, dtype=np.int32).reshape(-1, 2))
+    bx = np.ascontiguousarray(boxes, dtype=np.float64).reshape(-1, 6)
+    total = int((sz[:, 0].astype(np.int64) * sz[:, 1]).sum())
+    img = np.empty(total, dtype=np.float32)
+    dep = np.empty(total, dtype=np.float32)
+    rc = _load().l3d_scene_room(va.ctypes.data, sz.ctypes.data, len(views), seed & 0xFFFFFFFF,
+                                float(sigma), bx.ctypes.data, bx.shape[0], img.ctypes.data,
+                                dep.ctypes.data)
+    if rc:
+        raise RuntimeError("scene rendering failed")
+    return _split(img, sz), _split(dep, sz)
+
+
+def _split(flat: np.ndarray, sizes: np.ndarray):
+    out, o = [], 0
+    for w, h in sizes:
+        n = int(w) * int(h)
+        out.append(flat[o:o + n].reshape(int(h), int(w)))
+        o += n
+    return out
+
+
+def circle_views(n: int, width: int, height: int, radius: float, f: float) -> list[StereoView]:
+    k = Intrinsics(f, f, width / 2.0, height / 2.0)
+    out = []
+    for i in range(n):
+        a = 2 * np.pi * i / n
+        c = (radius * np.sin(a), 0.0, radius * np.cos(a))
+        out.append(StereoView(k, look_at(c, (0.0, 0.0, 0.0))))
+    return out
+
+
+def helix_views(n: int, width: int, height: int, f: float, turns: float = 2.0,
+                r0: float = 1.2, r1: float = 2.0, e0: float = -10.0, e1: float = 40.0):
+    k = Intrinsics(f, f, width / 2.0, height / 2.0)
+    out = []
+    for i in range(n):
+        s = i / max(1, n - 1)
+        a = 2 * np.pi * turns * i / n
+        r = r0 + (r1 - r0) * s
+        e = np.radians(e0 + (e1 - e0) * s)
+        c = (r * np.cos(e) * np.sin(a), r * np.sin(e), r * np.cos(e) * np.cos(a))
+        out.append(StereoView(k, look_at(c, (0.0, 0.0, 0.0))))
+    return out
+
+
+def perturb(views, seed: int, trans: float, rot_deg: float) -> list[StereoView]:
+    """Moves each camera centre by `trans` metres and turns it by `rot_deg` degrees about a
+    random axis (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for v in views:
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        axis = rng.normal(size=3)
+        Rn = rotation(axis, np.radians(rot_deg)) @ v.pose.R
+        c = camera_center(v.pose) + trans * d
+        out.append(StereoView(v.intrinsics, Pose(Rn, -Rn @ c)))
+    return out
+
+
+def neighbour_sources(n: int, k: int, circular: bool) -> list[list[int]]:
+    """The k nearest other views by index distance (ties: the earlier view first)."""
+    out = []
+    for i in range(n):
+        if circular:
+            cand = sorted((j for j in range(n) if j != i),
+                          key=lambda j: (min(abs(j - i), n - abs(j - i)), (j - i) % n > n // 2, j))
+        else:
+            cand = sorted((j for j in range(n) if j != i), key=lambda j: (abs(j - i), j))
+        out.append(cand[:k])
+    return out
+
+
+@dataclass
+class Workload:
+    name: str
+    width: int
+    height: int
+    views: list                      # poses handed to the solver
+    true_views: list                 # poses the images were rendered with
+    images: list                     # (H, W) float32
+    truth: list                      # (H, W) float32 z-depth, 0 = sky
+    sources: list
+    ranges: list
+    iterations: int
+    tsdf_dims: tuple
+    tsdf_voxel: float
+    tsdf_origin: tuple
+    tsdf_truncation: float
+    needed: list = field(default_factory=list)
+    window: int = 6
+    dilation: int = 2
+
+    @property
+    def pixels(self) -> int:
+        return self.width * self.height
+
+
+def small(seed: int = 1, n_views: int = 8, width: int = 320, height: int = 240) -> Workload:
+    """8 views of 320x240 on a circle; 4 sources, 3 iterations; TSDF 128^3 at 1 cm."""
+    f = 280.0 * width / 320.0
+    views = circle_views(n_views, width, height, 1.5, f)
+    imgs, truth = render_sphere(views, [(width, height)] * n_views, seed)
+    src = neighbour_sources(n_views, min(4, n_views - 1), circular=True)
+    dims = (128, 128, 128)
+    return Workload("small", width, height, views, views, imgs, truth, src,
+                    [(0.5, 3.0)] * n_views, 3, dims, 0.01, (-0.64, -0.64, -0.64), 0.04,
+                    needed=[2] * n_views)
+
+
+def scan(seed: int = 2, n_views: int = 48, width: int = 640, height: int = 480,
+         tsdf_dim: int = 512) -> Workload:
+    """48 views of 640x480 on a helix with pose and pixel noise; 8 sources, 5 iterations;
+    TSDF 512^3 at 4 mm."""
+    f = 560.0 * width / 640.0
+    true_views = helix_views(n_views, width, height, f)
+    imgs, truth = render_sphere(true_views, [(width, height)] * n_views, seed, sigma=0.01)
+    views = perturb(true_views, seed + 1000, 0.002, 0.1)
+    src = neighbour_sources(n_views, min(8, n_views - 1), circular=False)
+    vox = 0.004 * 512 / tsdf_dim
+    half = tsdf_dim * vox / 2
+    return Workload("scan", width, height, views, true_views, imgs, truth, src,
+                    [(0.15, 4.0)] * n_views, 5, (tsdf_dim,) * 3, vox, (-half, -half, -half), 0.02,
+                    needed=[3] * n_views)

@@ -1,0 +1,271 @@
+"""ctypes wrapper of the CPU oracle (oracle/oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg, as the checker or the timed CPU baseline.  Nothing in the product imports it.
+Parity unpinned: the reference has no CPU implementation or golden vectors for this path; the
+known-answer tests in tests/test_oracle.py pin the restatement.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libl3doracle.so")
+
+INIT, INIT_COARSE, PROPAGATE, PACK, CONSISTENCY = range(5)
+
+
+class StereoArgs(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32), ("n_views", C.c_int32),
+        ("views", C.c_void_p), ("images", C.c_void_p),
+        ("ref", C.c_int32), ("sources", C.c_void_p), ("n_sources", C.c_int32),
+        ("min_depth", C.c_double), ("max_depth", C.c_double),
+        ("prior", C.c_void_p),
+        ("geometric", C.c_int32), ("iterations", C.c_int32),
+        ("win_n", C.c_int32), ("win_dil", C.c_int32), ("pack", C.c_int32),
+        ("from_coarse", C.c_int32), ("coarse_hyp", C.c_void_p),
+        ("coarse_w", C.c_int32), ("coarse_h", C.c_int32),
+        ("needed", C.c_int32), ("threads", C.c_int32),
+    ]
+
+
+class TsdfDesc(C.Structure):
+    _fields_ = [
+        ("origin", C.c_double * 3), ("voxel", C.c_double), ("truncation", C.c_double),
+        ("max_weight", C.c_double), ("prior_weight", C.c_double),
+        ("dense", C.c_int32), ("dims", C.c_int32 * 3), ("coords", C.c_void_p), ("count", C.c_int32),
+        ("weight_q8", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
+    ]
+
+
+class TsdfView(C.Structure):
+    _fields_ = [
+        ("k", C.c_double * 4), ("R", C.c_double * 9), ("t", C.c_double * 3),
+        ("max_depth", C.c_double), ("confidence", C.c_double), ("prior", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        lib = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        for pre in ("orc32", "orc64"):
+            getattr(lib, pre + "_solve").argtypes = [C.POINTER(StereoArgs), P, P, P]
+            getattr(lib, pre + "_kernel").argtypes = [C.POINTER(StereoArgs), C.c_int32, C.c_int32,
+                                                      C.c_int32, P, P, P, P]
+            getattr(lib, pre + "_plane_cost").argtypes = [C.POINTER(StereoArgs), P, P, P]
+            getattr(lib, pre + "_tsdf_integrate").argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView),
+                                                              P, P, P, C.c_int32]
+        lib.orc_tsdf_visible.argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView), P]
+        lib.orc_pack_sample.restype = C.c_uint32
+        lib.orc_pack_sample.argtypes = [C.c_float] * 5
+        lib.orc_unpack_depth.restype = C.c_float
+        lib.orc_unpack_depth.argtypes = [C.c_uint32]
+        lib.orc_unpack_normal.argtypes = [C.c_uint32, P]
+        lib.orc_pcg.restype = C.c_uint32
+        lib.orc_pcg.argtypes = [C.c_uint32]
+        lib.orc_expf.restype = C.c_float
+        lib.orc_expf.argtypes = [C.c_float]
+        lib.orc_sincosf.argtypes = [C.c_float, P, P]
+        lib.orc_f32_to_f16.restype = C.c_uint32
+        lib.orc_f32_to_f16.argtypes = [C.c_float]
+        lib.orc_f16_to_f32.restype = C.c_float
+        lib.orc_f16_to_f32.argtypes = [C.c_uint32]
+        lib.orc_seed.restype = C.c_uint32
+        lib.orc_seed.argtypes = [C.c_int32] * 4
+        _lib = lib
+    return _lib
+
+
+def _views_array(views) -> np.ndarray:
+    out = np.zeros((len(views), 16), dtype=np.float64)
+    for i, v in enumerate(views):
+        k = v.intrinsics
+        out[i, :4] = (k.fx, k.fy, k.cx, k.cy)
+        out[i, 4:13] = np.asarray(v.pose.R, dtype=np.float64).reshape(9)
+        out[i, 13:16] = np.asarray(v.pose.t, dtype=np.float64).reshape(3)
+    return out
+
+
+class Stereo:
+    """Oracle state for one image set: images (V, H, W) float32, packed depths (V, H, W) and the
+    hypothesis buffers of one reference view, in FP32 (`precision=32`) or FP64."""
+
+    def __init__(self, width, height, views, images, precision: int = 32, window: int = 6,
+                 dilation: int = 2, threads: int = 0):
+        self.W, self.H = int(width), int(height)
+        self.V = len(views)
+        self.views = _views_array(views)
+        self.images = np.ascontiguousarray(np.stack([np.asarray(i, dtype=np.float32) for i in images]))
+        assert self.images.shape == (self.V, self.H, self.W)
+        self.dt = np.float32 if precision == 32 else np.float64
+        self.pre = "orc32" if precision == 32 else "orc64"
+        self.hyp = np.zeros((self.H, self.W, 4), dtype=self.dt)
+        self.cost = np.zeros((self.H, self.W), dtype=self.dt)
+        self.depths = np.zeros((self.V, self.H, self.W), dtype=np.uint32)
+        self.filtered = np.zeros((self.H, self.W), dtype=np.uint32)
+        self.window, self.dilation, self.threads = window, dilation, threads
+        self.coarse = None  # (hyp (h, w, 4) in this precision)
+
+    def _args(self, ref, sources, min_depth=0.5, max_depth=3.0, prior=None, geometric=False,
+              iterations=3, pack=True, from_coarse=False, needed=0):
+        keep = []
+        a = StereoArgs()
+        a.width, a.height, a.n_views = self.W, self.H, self.V
+        a.views = self.views.ctypes.data
+        a.images = self.images.ctypes.data
+        a.ref = int(ref)
+        src = np.asarray(list(sources), dtype=np.int32)
+        keep.append(src)
+        a.sources = src.ctypes.data
+        a.n_sources = len(src)
+        a.min_depth, a.max_depth = float(min_depth), float(max_depth)
+        if prior is not None:
+            pr = np.ascontiguousarray(prior, dtype=np.float32)
+            keep.append(pr)
+            a.prior = pr.ctypes.data
+        a.geometric = int(bool(geometric))
+        a.iterations = int(iterations)
+        a.win_n, a.win_dil = self.window, self.dilation
+        a.pack = int(bool(pack))
+        if self.coarse is not None:
+            ch = np.ascontiguousarray(self.coarse, dtype=self.dt)
+            keep.append(ch)
+            a.coarse_hyp = ch.ctypes.data
+            a.coarse_h, a.coarse_w = ch.shape[0], ch.shape[1]
+        a.from_coarse = int(bool(from_coarse))
+        a.needed = int(needed)
+        a.threads = int(self.threads)
+        return a, keep
+
+    def solve(self, ref, sources, **kw) -> None:
+        a, keep = self._args(ref, sources, **kw)
+        rc = getattr(load(), self.pre + "_solve")(C.byref(a), self.hyp.ctypes.data,
+                                                  self.cost.ctypes.data, self.depths.ctypes.data)
+        assert rc == 0, "oracle rejected the arguments"
+
+    def kernel(self, kernel, ref, sources, iteration=0, phase=0, **kw) -> None:
+        a, keep = self._args(ref, sources, **kw)
+        rc = getattr(load(), self.pre + "_kernel")(C.byref(a), int(kernel), int(iteration),
+                                                   int(phase), self.hyp.ctypes.data,
+                                                   self.cost.ctypes.data, self.depths.ctypes.data,
+                                                   self.filtered.ctypes.data)
+        assert rc == 0, "oracle rejected the arguments"
+
+    def filter(self, ref, checks, needed) -> np.ndarray:
+        self.kernel(CONSISTENCY, ref, checks, needed=needed)
+        return self.filtered.copy()
+
+    def plane_cost(self, ref, sources, planes, **kw):
+        a, keep = self._args(ref, sources, **kw)
+        pl = np.ascontiguousarray(planes, dtype=self.dt)
+        cost = np.zeros((self.H, self.W), dtype=self.dt)
+        vc = np.zeros((self.H, self.W, 8), dtype=self.dt)
+        rc = getattr(load(), self.pre + "_plane_cost")(C.byref(a), pl.ctypes.data, cost.ctypes.data,
+                                                       vc.ctypes.data)
+        assert rc == 0
+        return cost, vc
+
+
+def tsdf_desc(width, height, voxel, origin, truncation, dense=None, coords=None,
+              weight_q8=False, max_weight=96.0, prior_weight=0.12):
+    d = TsdfDesc()
+    d.origin[:] = [float(o) for o in origin]
+    d.voxel, d.truncation = float(voxel), float(truncation)
+    d.max_weight, d.prior_weight = float(max_weight), float(prior_weight)
+    keep = []
+    if dense is not None:
+        d.dense = 1
+        d.dims[:] = [int(x) for x in dense]
+    else:
+        c = np.ascontiguousarray(coords, dtype=np.int32)
+        keep.append(c)
+        d.dense = 0
+        d.coords = c.ctypes.data
+        d.count = c.shape[0]
+    d.weight_q8 = int(bool(weight_q8))
+    d.width, d.height = int(width), int(height)
+    return d, keep
+
+
+def tsdf_view(k, R, t, max_depth, confidence=0.0, prior=None):
+    v = TsdfView()
+    v.k[:] = [float(x) for x in k]
+    v.R[:] = [float(x) for x in np.asarray(R, dtype=np.float64).reshape(9)]
+    v.t[:] = [float(x) for x in np.asarray(t, dtype=np.float64).reshape(3)]
+    v.max_depth, v.confidence = float(max_depth), float(confidence)
+    keep = []
+    if prior is not None:
+        p = np.ascontiguousarray(prior, dtype=np.float32)
+        keep.append(p)
+        v.prior = p.ctypes.data
+    return v, keep
+
+
+class Tsdf:
+    """Oracle TSDF volume (f32 tsdf; f32 or Q8.8 uint16 weights; FP64 with precision=64)."""
+
+    def __init__(self, width, height, voxel, origin, truncation, dense=None, coords=None,
+                 weight_q8=False, max_weight=96.0, prior_weight=0.12, precision=32, threads=0):
+        self.desc, self._keep = tsdf_desc(width, height, voxel, origin, truncation, dense, coords,
+                                          weight_q8, max_weight, prior_weight)
+        n = int(np.prod(dense)) if dense is not None else int(np.asarray(coords).shape[0]) * 512
+        self.dt = np.float32 if precision == 32 else np.float64
+        self.pre = "orc32" if precision == 32 else "orc64"
+        self.tsdf = np.ones(n, dtype=self.dt)
+        self.weight = np.zeros(n, dtype=np.uint16 if weight_q8 else self.dt)
+        self.threads = threads
+
+    def integrate(self, view_kw: dict, depth: np.ndarray) -> None:
+        v, keep = tsdf_view(**view_kw)
+        d = np.ascontiguousarray(depth, dtype=np.uint32)
+        rc = getattr(load(), self.pre + "_tsdf_integrate")(C.byref(self.desc), C.byref(v), d.ctypes.data,
+                                                           self.tsdf.ctypes.data,
+                                                           self.weight.ctypes.data, self.threads)
+        assert rc == 0
+
+    def visible(self, view_kw: dict) -> np.ndarray:
+        v, keep = tsdf_view(**view_kw)
+        if self.desc.dense:
+            nb = [(int(x) + 7) // 8 for x in self.desc.dims]
+            out = np.zeros(nb[0] * nb[1] * nb[2], dtype=np.uint8)
+        else:
+            out = np.zeros(self.desc.count, dtype=np.uint8)
+        load().orc_tsdf_visible(C.byref(self.desc), C.byref(v), out.ctypes.data)
+        return out
+
+
+def pack_sample(depth, n, cost) -> int:
+    return int(load().orc_pack_sample(float(depth), float(n[0]), float(n[1]), float(n[2]), float(cost)))
+
+
+def unpack_normal(packed) -> np.ndarray:
+    out = np.zeros(3, dtype=np.float32)
+    load().orc_unpack_normal(int(packed), out.ctypes.data)
+    return out
+
+
+def expf(x) -> float:
+    return float(load().orc_expf(float(x)))
+
+
+def sincosf(a):
+    s = C.c_float()
+    c = C.c_float()
+    load().orc_sincosf(float(a), C.byref(s), C.byref(c))
+    return s.value, c.value

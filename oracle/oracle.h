@@ -1,0 +1,110 @@
+/*
+ * CPU oracle of the dense-reconstruction path (PatchMatch MVS + TSDF integration).
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
+ * leg (and its --impl reference arm) load this library, and only as the checker or as the timed
+ * CPU baseline.  The product library (libluvas3d.so) never links or calls it.
+ *
+ * Parity unpinned: the reference implements these stages only as WGSL compute shaders
+ * (frontend/src/app/vision/mvs/patchmatch.wgsl.ts, frontend/src/app/vision/fusion/tsdf-volume.ts)
+ * run through WebGPU in Chrome, holds no golden vectors for them and cannot run here.  This file
+ * restates that WGSL line by line in C++; the known-answer tests under tests/ pin it.
+ */
+#ifndef L3D_ORACLE_H
+#define L3D_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Per-view camera, 16 doubles: fx fy cx cy | R (row-major, world -> camera) | t. */
+#define ORC_VIEW_DOUBLES 16
+
+enum { ORC_INIT = 0, ORC_INIT_COARSE = 1, ORC_PROPAGATE = 2, ORC_PACK = 3, ORC_CONSISTENCY = 4 };
+
+typedef struct {
+    int32_t width, height, n_views;
+    const double* views;       /* n_views * 16 */
+    const float* images;       /* n_views * height * width, values in [0, 1] */
+    int32_t ref;
+    const int32_t* sources;    /* n_sources layer indices (at most 8 are used) */
+    int32_t n_sources;
+    double min_depth, max_depth;
+    const float* prior;        /* width * height or NULL */
+    int32_t geometric;         /* flags bit 0 */
+    int32_t iterations;
+    int32_t win_n;             /* samples per window side (6 = reference) */
+    int32_t win_dil;           /* sample spacing (2 = reference) */
+    int32_t pack;
+    int32_t from_coarse;
+    const void* coarse_hyp;    /* coarse_w * coarse_h * 4 (same precision as the solve) */
+    int32_t coarse_w, coarse_h;
+    int32_t needed;            /* consistency: views that must agree */
+    int32_t threads;           /* OpenMP threads, <= 0 for the default */
+} orc_stereo_args;
+
+/* Full schedule of DenseStereo.solve (dense-stereo.ts:231-285) for one reference view. */
+int orc32_solve(const orc_stereo_args* a, float* hyp, float* cost, uint32_t* depths);
+int orc64_solve(const orc_stereo_args* a, double* hyp, double* cost, uint32_t* depths);
+
+/* One kernel over the whole image: init, init_coarse, propagate (one colour), pack or
+ * consistency.  `iteration` and `phase` fill the dispatch state; step = 0.5^iteration. */
+int orc32_kernel(const orc_stereo_args* a, int32_t kernel, int32_t iteration, int32_t phase,
+                 float* hyp, float* cost, uint32_t* depths, uint32_t* filtered);
+int orc64_kernel(const orc_stereo_args* a, int32_t kernel, int32_t iteration, int32_t phase,
+                 double* hyp, double* cost, uint32_t* depths, uint32_t* filtered);
+
+/* hypothesis_cost of a given plane per pixel (planes: P * 4 = n, d); view_costs gets the
+ * per-source view_cost (P * 8, unused slots 0) when not NULL. */
+int orc32_plane_cost(const orc_stereo_args* a, const float* planes, float* cost, float* view_costs);
+int orc64_plane_cost(const orc_stereo_args* a, const double* planes, double* cost,
+                     double* view_costs);
+
+/* TSDF integration of one packed depth map (tsdf-volume.ts:308-359 and 425-473). */
+typedef struct {
+    double origin[3];
+    double voxel;
+    double truncation;
+    double max_weight;
+    double prior_weight;
+    int32_t dense;             /* 1: dense grid dims[0..2]; 0: brick pool with coords */
+    int32_t dims[3];
+    const int32_t* coords;     /* brick pool: count * 4 (x, y, z, pad) */
+    int32_t count;
+    int32_t weight_q8;         /* 1: uint16 weights in Q8.8; 0: f32 weights */
+    int32_t width, height;     /* depth map size */
+} orc_tsdf_desc;
+
+typedef struct {
+    double k[4];
+    double R[9];
+    double t[3];
+    double max_depth;
+    double confidence;
+    const float* prior;        /* width * height or NULL */
+} orc_tsdf_view;
+
+int orc32_tsdf_integrate(const orc_tsdf_desc* d, const orc_tsdf_view* v, const uint32_t* depth,
+                         float* tsdf, void* weight, int32_t threads);
+int orc64_tsdf_integrate(const orc_tsdf_desc* d, const orc_tsdf_view* v, const uint32_t* depth,
+                         double* tsdf, double* weight, int32_t threads);
+/* Brick visibility of tsdf-volume.ts:425-439 (FP64); out: count (or dense brick count) bytes. */
+int orc_tsdf_visible(const orc_tsdf_desc* d, const orc_tsdf_view* v, uint8_t* out);
+
+/* Packing helpers (depth-packing.wgsl.ts:3-33) and primitives for unit tests. */
+uint32_t orc_pack_sample(float depth, float nx, float ny, float nz, float cost);
+float orc_unpack_depth(uint32_t packed);
+void orc_unpack_normal(uint32_t packed, float* n3);
+uint32_t orc_pcg(uint32_t v);
+float orc_expf(float x);
+void orc_sincosf(float a, float* s, float* c);
+uint32_t orc_f32_to_f16(float f);
+float orc_f16_to_f32(uint32_t h);
+uint32_t orc_seed(int32_t ref, int32_t iteration, int32_t phase, int32_t flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
