@@ -199,106 +199,136 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
-    from luvas3d import (DTYPE_F32, FORM_PLAIN, DenseStereo, IntegrationView, SolveOptions,
-                         StereoOptions, TsdfVolume)
+    from luvas3d import (DTYPE_F16, DTYPE_F32, FORM_FAST, FORM_PLAIN, DenseStereo,
+                         IntegrationView, SolveOptions, StereoOptions, TsdfVolume)
 
     w = build_workload(args)
     V, P = len(w.views), w.pixels
-    form = FORM_PLAIN
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
-    stereo = DenseStereo(w.width, w.height, w.views,
-                         StereoOptions(storage=DTYPE_F32, form=form, stream=sptr))
-    tsdf = TsdfVolume(w.width, w.height, w.tsdf_voxel, w.tsdf_origin, dense=w.tsdf_dims,
-                      truncation=w.tsdf_truncation, weight_q8=True, stream=sptr)
-    for i, im in enumerate(w.images):
-        stereo.set_image(i, im)
     refs = list(range(V))
     opts = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=w.iterations)
             for r in refs]
     iviews = [IntegrationView(v.intrinsics, v.pose, w.ranges[i][1]) for i, v in enumerate(w.views)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    vox = int(np.prod(w.tsdf_dims))
+    px_iters_step = V * P * w.iterations
+    tsdf = TsdfVolume(w.width, w.height, w.tsdf_voxel, w.tsdf_origin, dense=w.tsdf_dims,
+                      truncation=w.tsdf_truncation, weight_q8=True, stream=sptr)
+    mk = lambda n=4: [torch.cuda.Event(enable_timing=True) for _ in range(n)]
 
-    def step(evs):
+    def rec(ev):
+        with torch.cuda.stream(stream):
+            ev.record(stream)
+
+    def make_stereo(form):
+        storage = DTYPE_F16 if form == FORM_FAST else DTYPE_F32
+        st = DenseStereo(w.width, w.height, w.views,
+                         StereoOptions(storage=storage, form=form, stream=sptr))
+        for i, im in enumerate(w.images):
+            st.set_image(i, im)
+        return st
+
+    def step(st, evs):
         with torch.cuda.stream(stream):
             flush.fill_(1)
-            evs[0].record(stream)
-        stereo.solve_all(refs, opts)
-        with torch.cuda.stream(stream):
-            evs[1].record(stream)
+        rec(evs[0])
+        st.solve_all(refs, opts)
+        rec(evs[1])
         tsdf.reset()  # a fresh volume per scan (tsdf 1, weight 0), outside the timed TSDF stage
-        stereo.filter_all(refs, w.sources, w.needed)
-        with torch.cuda.stream(stream):
-            evs[2].record(stream)
-        tsdf.integrate_many(iviews, stereo=stereo, layers=refs)
-        with torch.cuda.stream(stream):
-            evs[3].record(stream)
+        st.filter_all(refs, w.sources, w.needed)
+        rec(evs[2])
+        tsdf.integrate_many(iviews, stereo=st, layers=refs)
+        rec(evs[3])
 
-    mk = lambda: [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    for _ in range(args.warmup):
-        step(mk())
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    launches0 = stereo.launches + tsdf.launches
-    clocks = ClockSampler(local)
-    clocks.start()
-    all_evs = []
-    t_wall = time.perf_counter()
-    for _ in range(args.steps):
-        evs = mk()
-        step(evs)
-        all_evs.append(evs)
-    torch.cuda.synchronize()
-    t_wall = time.perf_counter() - t_wall
-    launches = stereo.launches + tsdf.launches - launches0
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    pm_ms = [e[0].elapsed_time(e[1]) for e in all_evs]
-    filt_ms = [e[1].elapsed_time(e[2]) for e in all_evs]
-    ts_ms = [e[2].elapsed_time(e[3]) for e in all_evs]
-    step_ms = [e[0].elapsed_time(e[3]) for e in all_evs]
-    tot = torch.tensor([sum(pm_ms), sum(ts_ms), sum(step_ms)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    pm_s, ts_s, st_s = (float(x) / 1e3 for x in tot.tolist())
-    px_iters = V * P * w.iterations * args.steps * world
-    vox = int(np.prod(w.tsdf_dims))
+    def time_form(form, steps, warmup, sample_clocks):
+        st = make_stereo(form)
+        for _ in range(warmup):
+            step(st, mk())
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        l0 = st.launches + tsdf.launches
+        clocks = ClockSampler(local) if sample_clocks else None
+        if clocks:
+            clocks.start()
+        all_evs = []
+        for _ in range(steps):
+            evs = mk()
+            step(st, evs)
+            all_evs.append(evs)
+        torch.cuda.synchronize()
+        launches = st.launches + tsdf.launches - l0
+        if world > 1:
+            dist.barrier()
+        clk = clocks.stop() if clocks else None
+        ms = {k: [e[a].elapsed_time(e[b]) for e in all_evs]
+              for k, (a, b) in {"patchmatch": (0, 1), "filter": (1, 2), "tsdf": (2, 3),
+                                "step": (0, 3)}.items()}
+        tot = torch.tensor([sum(ms["patchmatch"]), sum(ms["tsdf"]), sum(ms["step"])],
+                           dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+        pm_s, ts_s, st_s = (float(x) / 1e3 for x in tot.tolist())
+        # propagate launches alone: solve with 5 iterations minus solve with 0 (init + pack)
+        per = {}
+        for its in (0, w.iterations):
+            o2 = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=its)
+                  for r in refs]
+            a, b = mk(2)
+            rec(a)
+            for _ in range(2):
+                st.solve_all(refs, o2)
+            rec(b)
+            torch.cuda.synchronize()
+            per[its] = a.elapsed_time(b) / 2
+        n_prop = 2 * w.iterations * (1 if form == FORM_FAST else V)
+        prop_ms = (per[w.iterations] - per[0]) / n_prop
+        return st, {"pm_s": pm_s, "ts_s": ts_s, "st_s": st_s, "ms": ms, "clk": clk,
+                    "launches": launches, "prop_ms": prop_ms,
+                    "px_iters_per_s": px_iters_step * steps * world / pm_s}
+
+    plain_steps = max(1, min(args.steps, 2)) if args.form == "auto" else args.steps
+    res = {}
+    stereo = None
+    forms = {"auto": [FORM_PLAIN, FORM_FAST], "plain": [FORM_PLAIN], "fast": [FORM_FAST]}[args.form]
+    for form in forms:
+        chosen = form == forms[-1]
+        st, r = time_form(form, args.steps if chosen else plain_steps, args.warmup, chosen)
+        res[form] = r
+        if chosen:
+            stereo = st
+        else:
+            st.destroy()
+    chosen_form = forms[-1]
+    R = res[chosen_form]
+    clk = R["clk"]
+    value = R["px_iters_per_s"]
     voxel_updates = vox * V * args.steps * world
-    value = px_iters / pm_s
 
-    # ---- roofline of the dominant kernel (red/black propagate), timed alone -------------------
+    # ---- roofline of the dominant kernel (red/black propagate) ------------------------------
     peaks, peak_kind = _peaks()
-    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    from luvas3d import KERNEL_PROPAGATE
-    reps = 10
-    with torch.cuda.stream(stream):
-        ev_a.record(stream)
-    for i in range(reps):
-        stereo.dispatch(KERNEL_PROPAGATE, 0, opts[0], iteration=1, phase=i & 1)
-    with torch.cuda.stream(stream):
-        ev_b.record(stream)
-    torch.cuda.synchronize()
-    prop_ms = ev_a.elapsed_time(ev_b) / reps
     S = len(w.sources[0])
     flop_per_px_phase = 14 * S * (18 + 36 * 37 + 15) + 36 * 26
-    prop_flops = flop_per_px_phase * (P / 2)
-    achieved = prop_flops / (prop_ms / 1e3) / 1e12
-    fp32_peak = 148 * 128 * 2 * (clk.get("sm_mhz") or 1965.0) * 1e6 / 1e12
+    views_per_launch = V if chosen_form == FORM_FAST else 1
+    prop_flops = flop_per_px_phase * (P / 2) * views_per_launch
+    achieved = prop_flops / (R["prop_ms"] / 1e3) / 1e12
+    sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    tsdf_ms = sum(R["ms"]["tsdf"]) / len(R["ms"]["tsdf"])
     tsdf_bytes = vox * 12
-    tsdf_gbs = tsdf_bytes / (sum(ts_ms) / len(ts_ms) / 1e3) / 1e9
+    tsdf_gbs = tsdf_bytes / (tsdf_ms / 1e3) / 1e9
 
     # ---- end to end through the C ABI with pinned host buffers ------------------------------
     e2e = None
     if not args.no_e2e:
+        import ctypes as C
+        from luvas3d import _lib
+        lib = _lib.load()
         pinned = [torch.from_numpy(np.ascontiguousarray(im)).pin_memory() for im in w.images]
         out_f = torch.empty((V, w.height, w.width), dtype=torch.int32).pin_memory()
         out_t = torch.empty(vox, dtype=torch.float32).pin_memory()
         out_w = torch.empty(vox, dtype=torch.int16).pin_memory()
-        import ctypes as C
-        from luvas3d import _lib
-        lib = _lib.load()
 
         def e2e_step():
             for i, im in enumerate(pinned):
@@ -315,19 +345,17 @@ def main():
 
         e2e_step()
         torch.cuda.synchronize()
-        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            ea.record(stream)
+        ea, eb = mk(2)
+        rec(ea)
         for _ in range(args.steps):
             e2e_step()
-        with torch.cuda.stream(stream):
-            eb.record(stream)
+        rec(eb)
         torch.cuda.synchronize()
         e2e_s = torch.tensor([ea.elapsed_time(eb) / 1e3], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
-        e2e = {"value": px_iters / float(e2e_s.item()), "unit": "px-iters/s",
-               "h2d_bytes_per_step": V * P * 4,
+        e2e = {"value": px_iters_step * args.steps * world / float(e2e_s.item()),
+               "unit": "px-iters/s", "h2d_bytes_per_step": V * P * 4,
                "d2h_bytes_per_step": V * P * 4 + vox * 6,
                "ms_per_step": float(e2e_s.item()) * 1e3 / args.steps,
                "includes": "image upload from pinned host memory, PatchMatch, filter, TSDF, "
@@ -338,33 +366,45 @@ def main():
         cpu = cpu_baseline(w, os.cpu_count() or 1)
         cpu.pop("seconds", None)
 
+    def stage(r):
+        return {k: sum(v) / len(v) for k, v in r["ms"].items()}
+
     line = {
         "metric": METRIC, "value": value, "unit": "px-iters/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": st_s * 1e3 / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": R["st_s"] * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f16 images, f32 arithmetic" if chosen_form == FORM_FAST else "f32",
         "data": "synthetic (seeded sphere-on-plane scene, value-noise texture)",
         "config": {"workload": "scan: 48 views 640x480, 8 sources, 5 iterations, window 11x11 "
                                "dilated by 2, TSDF 512^3 at 4 mm, trunc 2 cm, Q8.8 weights",
-                   "form": "plain", "l2": "flushed (256 MB write) before every step",
+                   "form": "fast" if chosen_form == FORM_FAST else "plain",
+                   "l2": "flushed (256 MB write) before every step",
                    "parallelism": f"replica x{world}"},
-        "tsdf_voxel_updates_per_s": voxel_updates / ts_s,
-        "stage_ms": {"patchmatch": sum(pm_ms) / len(pm_ms), "filter": sum(filt_ms) / len(filt_ms),
-                     "tsdf": sum(ts_ms) / len(ts_ms)},
-        "roofline": {"kernel": "k_propagate (plain FP32, one colour of one view)",
+        "tsdf_voxel_updates_per_s": voxel_updates / R["ts_s"],
+        "stage_ms": stage(R),
+        "plain": ({"px_iters_per_s": res[FORM_PLAIN]["px_iters_per_s"],
+                   "stage_ms": stage(res[FORM_PLAIN]),
+                   "propagate_launch_ms": res[FORM_PLAIN]["prop_ms"]}
+                  if FORM_PLAIN in res else None),
+        "speedup_vs_plain": (value / res[FORM_PLAIN]["px_iters_per_s"]
+                             if FORM_PLAIN in res and chosen_form != FORM_PLAIN else None),
+        "roofline": {"kernel": ("k_fast_propagate (all 48 views, one colour)"
+                                if chosen_form == FORM_FAST else "k_propagate (one view, one colour)"),
                      "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
-                     "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2) at the "
-                                    "sampled median SM clock",
-                     "launch_ms": prop_ms, "flop_per_launch": prop_flops},
-        "roofline_tsdf": {"kernel": "k_integrate_many", "bound": "hbm", "achieved": tsdf_gbs,
-                          "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 flops) at "
+                                    "the sampled median SM clock",
+                     "launch_ms": R["prop_ms"], "flop_per_launch": prop_flops,
+                     "flop_model": "14 candidates x sources x (18 + 36 x 37 + 15) + 936 per "
+                                   "pixel of the colour"},
+        "roofline_tsdf": {"kernel": "k_integrate_many (48 views per sweep)", "bound": "hbm",
+                          "achieved": tsdf_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                           "frac": tsdf_gbs / peaks.get("hbm_gbs", 6650.0),
                           "peak_source": peak_kind, "bytes_per_launch": tsdf_bytes},
         "clocks": clk,
-        "gpu_launches": launches,
+        "gpu_launches": R["launches"],
         "e2e": e2e,
         "cpu_baseline": cpu,
-        "wall_s_timed": t_wall,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -92,6 +92,15 @@ struct l3d_stereo {
     float4* planes = nullptr;          /* plane_cost scratch */
     float* plane_out = nullptr;
     long long launches = 0;
+    /* fast form */
+    std::vector<cudaArray_t> arrays;   /* per view (F16/F32 storage): texture-sampled copy */
+    std::vector<cudaTextureObject_t> texs;
+    L3dFastView* fviews_dev = nullptr; /* capacity fview_cap */
+    int* tile_start_dev = nullptr;
+    L3dFastView* fviews_host = nullptr;  /* pinned staging */
+    int* tile_start_host = nullptr;
+    int fview_cap = 0;
+    cudaEvent_t staged = nullptr;      /* after the last copy out of the pinned staging */
 };
 
 namespace {
@@ -281,6 +290,184 @@ int solve_one(l3d_stereo* s, int ref, const l3d_solve_opts* o, float4* hyp, floa
     return L3D_OK;
 }
 
+/* ---- fast form ---- */
+
+bool fast_tex(const l3d_stereo* s) { return s->opts.storage != L3D_DTYPE_BF16; }
+
+int fast_capacity(l3d_stereo* s, int n) {
+    if (s->fview_cap >= n) return L3D_OK;
+    cudaStreamSynchronize(s->stream);
+    cudaFree(s->fviews_dev);
+    cudaFree(s->tile_start_dev);
+    cudaFreeHost(s->fviews_host);
+    cudaFreeHost(s->tile_start_host);
+    s->fviews_dev = nullptr;
+    s->tile_start_dev = nullptr;
+    s->fviews_host = nullptr;
+    s->tile_start_host = nullptr;
+    s->fview_cap = 0;
+    L3D_CUDA(cudaMalloc(&s->fviews_dev, (size_t)n * sizeof(L3dFastView)), "view table");
+    L3D_CUDA(cudaMalloc(&s->tile_start_dev, (size_t)(n + 1) * sizeof(int)), "view table");
+    L3D_CUDA(cudaMallocHost(&s->fviews_host, (size_t)n * sizeof(L3dFastView)), "view staging");
+    L3D_CUDA(cudaMallocHost(&s->tile_start_host, (size_t)(n + 1) * sizeof(int)), "view staging");
+    s->fview_cap = n;
+    return L3D_OK;
+}
+
+/* The parameters of one reference view for the fast kernels: DenseStereo.params
+ * (dense-stereo.ts:360-401) with the homography base shifted by half a texel for the texture
+ * unit (Bt = S B, ktt = S kt, S = [[1, 0, .5], [0, 1, .5], [0, 0, 1]]), composed in FP64. */
+L3dFastView fast_view(const l3d_stereo* s, int ref, const l3d_solve_opts* o, long long pix_off) {
+    L3dParams p = build_params(s, ref, o->sources, std::min(o->n_sources, L3D_MAX_SOURCES),
+                               o->min_depth, o->max_depth, 0, 0, 1.0, o->geometric ? 1 : 0, 0, 0, 0);
+    L3dFastView v;
+    std::memset(&v, 0, sizeof(v));
+    for (int i = 0; i < 4; i++) {
+        v.k[i] = p.k[i];
+        v.kinv[i] = p.kinv[i];
+        v.range[i] = p.range[i];
+    }
+    v.W = s->W;
+    v.H = s->H;
+    v.ref = ref;
+    v.n = p.n;
+    v.flags = p.flags;
+    v.iterations = o->iterations;
+    v.tiles_x = ((s->W + 1) / 2 + 15) / 16;
+    v.pix_off = pix_off;
+    v.ref_img_off = (long long)ref * s->P;
+    v.ref_dep_off = p.ref_dep_off;
+    v.ref_tex = fast_tex(s) ? (unsigned long long)s->texs[ref] : 0ull;
+    v.has_prior = o->prior != nullptr && !o->geometric;
+    v.pack = o->pack ? 1 : 0;
+    const l3d_view& rv = s->views[ref];
+    const double kr[4] = {rv.intrinsics.fx, rv.intrinsics.fy, rv.intrinsics.cx, rv.intrinsics.cy};
+    for (int k = 0; k < p.n; k++) {
+        const L3dSrc& ps = p.src[k];
+        L3dFastSrc& f = v.src[k];
+        const l3d_view& sv = s->views[o->sources[k]];
+        const double kv[4] = {sv.intrinsics.fx, sv.intrinsics.fy, sv.intrinsics.cx, sv.intrinsics.cy};
+        double R[9], t[3];
+        relative_pose(rv.pose, sv.pose, R, t);
+        double A[9], B[9], kt[3];
+        for (int c = 0; c < 3; c++) {
+            A[0 * 3 + c] = kv[0] * R[0 * 3 + c] + kv[2] * R[2 * 3 + c];
+            A[1 * 3 + c] = kv[1] * R[1 * 3 + c] + kv[3] * R[2 * 3 + c];
+            A[2 * 3 + c] = R[2 * 3 + c];
+        }
+        for (int r = 0; r < 3; r++) {
+            B[r * 3 + 0] = A[r * 3 + 0] / kr[0];
+            B[r * 3 + 1] = A[r * 3 + 1] / kr[1];
+            B[r * 3 + 2] = A[r * 3 + 2] - A[r * 3 + 0] * kr[2] / kr[0] - A[r * 3 + 1] * kr[3] / kr[1];
+        }
+        kt[0] = kv[0] * t[0] + kv[2] * t[2];
+        kt[1] = kv[1] * t[1] + kv[3] * t[2];
+        kt[2] = t[2];
+        for (int c = 0; c < 3; c++) {
+            f.Bt[0 * 3 + c] = (float)(B[0 * 3 + c] + 0.5 * B[2 * 3 + c]);
+            f.Bt[1 * 3 + c] = (float)(B[1 * 3 + c] + 0.5 * B[2 * 3 + c]);
+            f.Bt[2 * 3 + c] = (float)B[2 * 3 + c];
+        }
+        f.ktt[0] = (float)(kt[0] + 0.5 * kt[2]);
+        f.ktt[1] = (float)(kt[1] + 0.5 * kt[2]);
+        f.ktt[2] = (float)kt[2];
+        for (int i = 0; i < 4; i++) f.k[i] = ps.k[i];
+        for (int i = 0; i < 9; i++) f.R[i] = ps.R[i];
+        for (int i = 0; i < 3; i++) f.t[i] = ps.t[i];
+        f.W = ps.W;
+        f.H = ps.H;
+        f.img_off = ps.img_off;
+        f.dep_off = ps.dep_off;
+        f.tex = fast_tex(s) ? (unsigned long long)s->texs[o->sources[k]] : 0ull;
+    }
+    return v;
+}
+
+/* Uploads the view table of a batch (pinned staging guarded by an event) and returns the
+ * device-side description for the fast launchers. */
+int fast_batch(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* opts, float4* hyp,
+               float* cost, float* prior, bool per_view_offsets, L3dFastDev* out) {
+    int rc = fast_capacity(s, n);
+    if (rc) return rc;
+    L3D_CUDA(cudaEventSynchronize(s->staged), "staging wait");
+    int tiles = 0;
+    for (int i = 0; i < n; i++) {
+        long long off = per_view_offsets ? (long long)refs[i] * s->P : 0;
+        L3dFastView v = fast_view(s, refs[i], &opts[i], off);
+        v.tile_start = tiles;
+        s->fviews_host[i] = v;
+        s->tile_start_host[i] = tiles;
+        tiles += v.tiles_x * ((s->H + 7) / 8);
+        if (v.has_prior) {
+            L3D_CUDA(cudaMemcpyAsync(prior + off, opts[i].prior, s->P * sizeof(float),
+                                     cudaMemcpyHostToDevice, s->stream), "prior upload");
+        }
+    }
+    s->tile_start_host[n] = tiles;
+    L3D_CUDA(cudaMemcpyAsync(s->fviews_dev, s->fviews_host, (size_t)n * sizeof(L3dFastView),
+                             cudaMemcpyHostToDevice, s->stream), "view table upload");
+    L3D_CUDA(cudaMemcpyAsync(s->tile_start_dev, s->tile_start_host, (size_t)(n + 1) * sizeof(int),
+                             cudaMemcpyHostToDevice, s->stream), "view table upload");
+    L3D_CUDA(cudaEventRecord(s->staged, s->stream), "event record");
+    L3dFastDev d;
+    d.views = s->fviews_dev;
+    d.tile_start = s->tile_start_dev;
+    d.n_views = n;
+    d.total_tiles = tiles;
+    d.images = s->images;
+    d.storage = s->opts.storage;
+    d.hyp = hyp;
+    d.cost = cost;
+    d.prior = prior;
+    d.depths = s->depths;
+    *out = d;
+    return L3D_OK;
+}
+
+int fast_launch(l3d_stereo* s, int kernel, const L3dFastDev& d, int it, int phase) {
+    cudaError_t e = l3d_launch_fast(kernel, d, it, phase, 1, s->stream);
+    s->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return L3D_OK;
+}
+
+int fast_pack(l3d_stereo* s, const L3dFastDev& d) {
+    cudaError_t e = l3d_launch_fast_pack(d, s->P, s->stream);
+    s->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return L3D_OK;
+}
+
+/* The schedule of DenseStereo.solve for every view of a batch at once: init, iterations x
+ * (colour 0, colour 1), pack. */
+int fast_solve(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* opts, bool all) {
+    int nn = 0;
+    std::vector<int32_t> r;
+    std::vector<l3d_solve_opts> o;
+    int max_it = 0;
+    bool any_pack = false;
+    for (int i = 0; i < n; i++) {
+        if (std::min(opts[i].n_sources, L3D_MAX_SOURCES) == 0) continue;  /* dense-stereo.ts:233 */
+        if (opts[i].from_coarse) return fail(L3D_EINVAL, "the fast form has no coarse-to-fine start");
+        r.push_back(refs[i]);
+        o.push_back(opts[i]);
+        max_it = std::max(max_it, opts[i].iterations);
+        any_pack |= opts[i].pack != 0;
+        nn++;
+    }
+    if (nn == 0) return L3D_OK;
+    L3dFastDev d;
+    int rc = all ? fast_batch(s, nn, r.data(), o.data(), s->hyp_all, s->cost_all, s->prior_all, true, &d)
+                 : fast_batch(s, nn, r.data(), o.data(), s->hyp, s->cost, s->prior, false, &d);
+    if (rc) return rc;
+    if ((rc = fast_launch(s, L3D_K_INIT, d, 0, 0))) return rc;
+    for (int it = 0; it < max_it; it++)
+        for (int phase = 0; phase < 2; phase++)
+            if ((rc = fast_launch(s, L3D_K_PROPAGATE, d, it, phase))) return rc;
+    if (any_pack && (rc = fast_pack(s, d))) return rc;
+    return L3D_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -322,8 +509,8 @@ int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_
         return fail(L3D_EINVAL, "the plain form stores images as F32");
     if (o.storage != L3D_DTYPE_F32 && o.storage != L3D_DTYPE_F16 && o.storage != L3D_DTYPE_BF16)
         return fail(L3D_EINVAL, "image storage must be F32, F16 or BF16");
-    if (o.form == L3D_FORM_FAST)
-        return fail(L3D_EINVAL, "the fast form is not available in this build");
+    if (o.form == L3D_FORM_FAST && !(o.window == 6 && o.dilation == 2))
+        return fail(L3D_EINVAL, "the fast form uses the reference window (6 samples, dilation 2)");
     for (int i = 0; i < n_views; i++) {
         const l3d_intrinsics& k = views[i].intrinsics;
         if (!(k.fx != 0.0) || !(k.fy != 0.0) || !std::isfinite(k.fx) || !std::isfinite(k.fy))
@@ -354,7 +541,34 @@ int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_
     }
     e = cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming);
     if (e != cudaSuccess) return cleanup(cuda_fail(e, "event creation"));
+    e = cudaEventCreateWithFlags(&s->staged, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "event creation"));
     size_t esize = dtype_size(o.storage);
+    if (o.form == L3D_FORM_FAST && o.storage != L3D_DTYPE_BF16) {
+        /* texture-sampled copies: block-linear CUDA arrays with hardware bilinear filtering,
+         * clamp-to-edge addressing and unnormalised coordinates (texel centres at +0.5) */
+        cudaChannelFormatDesc ch = o.storage == L3D_DTYPE_F16 ? cudaCreateChannelDescHalf()
+                                                              : cudaCreateChannelDesc<float>();
+        s->arrays.assign(n_views, nullptr);
+        s->texs.assign(n_views, 0);
+        for (int i = 0; i < n_views; i++) {
+            if ((e = cudaMallocArray(&s->arrays[i], &ch, width, height)) != cudaSuccess)
+                return cleanup(cuda_fail(e, "image array allocation"));
+            cudaResourceDesc res;
+            std::memset(&res, 0, sizeof(res));
+            res.resType = cudaResourceTypeArray;
+            res.res.array.array = s->arrays[i];
+            cudaTextureDesc td;
+            std::memset(&td, 0, sizeof(td));
+            td.addressMode[0] = cudaAddressModeClamp;
+            td.addressMode[1] = cudaAddressModeClamp;
+            td.filterMode = cudaFilterModeLinear;
+            td.readMode = cudaReadModeElementType;
+            td.normalizedCoords = 0;
+            if ((e = cudaCreateTextureObject(&s->texs[i], &res, &td, nullptr)) != cudaSuccess)
+                return cleanup(cuda_fail(e, "texture creation"));
+        }
+    }
     if ((e = cudaMalloc(&s->images, (size_t)n_views * s->P * esize)) != cudaSuccess ||
         (e = dalloc(&s->depths, (size_t)s->n_maps * s->P)) != cudaSuccess ||
         (e = dalloc(&s->hyp, (size_t)s->P)) != cudaSuccess ||
@@ -403,12 +617,19 @@ int l3d_stereo_set_image(l3d_stereo* s, int32_t layer, int32_t dtype, const void
                                        s->opts.storage, s->stream);
     s->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "image conversion");
+    if (!s->arrays.empty()) {
+        size_t rb = (size_t)s->W * out_es;
+        L3D_CUDA(cudaMemcpy2DToArrayAsync(s->arrays[layer], 0, 0, dst, rb, rb, s->H,
+                                          cudaMemcpyDeviceToDevice, s->stream),
+                 "image array copy");
+    }
     return L3D_OK;
 }
 
 int l3d_stereo_solve(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o) {
     int rc = check_solve(s, ref, o);
     if (rc) return rc;
+    if (s->opts.form == L3D_FORM_FAST) return fast_solve(s, 1, &ref, o, false);
     return solve_one(s, ref, o, s->hyp, s->cost, s->prior);
 }
 
@@ -420,11 +641,15 @@ int l3d_stereo_solve_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
         int rc = check_solve(s, refs[i], &opts[i]);
         if (rc) return rc;
     }
+    for (int i = 0; i < n_refs; i++)
+        for (int j = 0; j < i; j++)
+            if (refs[i] == refs[j]) return fail(L3D_EINVAL, "reference layer %d appears twice", refs[i]);
     if (!s->hyp_all) {
         L3D_CUDA(dalloc(&s->hyp_all, (size_t)s->V * s->P), "hyp_all allocation");
         L3D_CUDA(dalloc(&s->cost_all, (size_t)s->V * s->P), "cost_all allocation");
         L3D_CUDA(dalloc(&s->prior_all, (size_t)s->V * s->P), "prior_all allocation");
     }
+    if (s->opts.form == L3D_FORM_FAST) return fast_solve(s, n_refs, refs, opts, true);
     for (int i = 0; i < n_refs; i++) {
         int r = refs[i];
         int rc = solve_one(s, r, &opts[i], s->hyp_all + (size_t)r * s->P, s->cost_all + (size_t)r * s->P,
@@ -445,6 +670,16 @@ int l3d_stereo_dispatch(l3d_stereo* s, int32_t kernel, int32_t ref, const l3d_so
         return fail(L3D_ESTATE, "init_coarse needs a coarse level");
     if (phase != 0 && phase != 1) return fail(L3D_EINVAL, "phase must be 0 or 1");
     int n = std::min(o->n_sources, L3D_MAX_SOURCES);
+    if (s->opts.form == L3D_FORM_FAST) {
+        if (kernel == L3D_KERNEL_INIT_COARSE) return fail(L3D_EINVAL, "the fast form has no init_coarse");
+        l3d_solve_opts one = *o;
+        one.iterations = iteration + 1;
+        one.pack = 1;
+        L3dFastDev fd;
+        if ((rc = fast_batch(s, 1, &ref, &one, s->hyp, s->cost, s->prior, false, &fd))) return rc;
+        if (kernel == L3D_KERNEL_PACK) return fast_pack(s, fd);
+        return fast_launch(s, kernel == L3D_KERNEL_INIT ? L3D_K_INIT : L3D_K_PROPAGATE, fd, iteration, phase);
+    }
     L3dStereoDev d = dev_of(s);
     if (kernel == L3D_KERNEL_INIT && o->prior && !o->geometric) {
         rc = upload_prior(s, o->prior, s->prior);
@@ -566,6 +801,17 @@ int l3d_stereo_plane_cost(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o, c
         L3D_CUDA(dalloc(&s->plane_out, (size_t)s->P * (1 + L3D_MAX_SOURCES)), "plane scratch");
     }
     L3D_CUDA(cudaMemcpyAsync(s->planes, planes, s->P * 16, cudaMemcpyHostToDevice, s->stream), "planes upload");
+    if (s->opts.form == L3D_FORM_FAST) {
+        if (view_costs) return fail(L3D_EINVAL, "the fast form reports the combined cost only");
+        L3dFastDev fd;
+        l3d_solve_opts one = *o;
+        one.prior = nullptr;
+        if ((rc = fast_batch(s, 1, &ref, &one, s->hyp, s->cost, s->prior, false, &fd))) return rc;
+        cudaError_t e = l3d_launch_fast_plane_cost(fd, s->planes, s->plane_out, s->stream);
+        s->launches++;
+        if (e != cudaSuccess) return cuda_fail(e, "plane cost launch");
+        return read_dev(s, cost, s->plane_out, s->P * 4, "read plane cost");
+    }
     int n = std::min(o->n_sources, L3D_MAX_SOURCES);
     L3dParams p = build_params(s, ref, o->sources, n, o->min_depth, o->max_depth, 0, 0, 1.0,
                                o->geometric ? 1 : 0, 0, 0, 0);
@@ -622,6 +868,15 @@ void l3d_stereo_destroy(l3d_stereo* s) {
     cudaFree(s->staging);
     cudaFree(s->planes);
     cudaFree(s->plane_out);
+    for (cudaTextureObject_t t : s->texs)
+        if (t) cudaDestroyTextureObject(t);
+    for (cudaArray_t a : s->arrays)
+        if (a) cudaFreeArray(a);
+    cudaFree(s->fviews_dev);
+    cudaFree(s->tile_start_dev);
+    cudaFreeHost(s->fviews_host);
+    cudaFreeHost(s->tile_start_host);
+    if (s->staged) cudaEventDestroy(s->staged);
     if (s->done) cudaEventDestroy(s->done);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;

@@ -89,6 +89,63 @@ struct L3dStereoDev {
 
 cudaError_t l3d_launch_plain(int kernel, const L3dParams& p, const L3dStereoDev& d, int win,
                              int dil, cudaStream_t stream);
+
+/* ---- fast form: every reference view of a batch in one launch per kernel ---- */
+
+/* One source of one reference view.  Bt/ktt are the homography base and K_s t with the
+ * texture's half-texel offset folded in (rows 0 and 1 plus 0.5 x row 2), so q.xy / q.z is
+ * directly the filtering coordinate. */
+struct L3dFastSrc {
+    float Bt[9];
+    float ktt[3];
+    float k[4];
+    float R[9];
+    float t[3];
+    int W, H;
+    long long img_off;         /* element offset of the source image (linear storage) */
+    long long dep_off;         /* element offset of the source's packed depth map */
+    unsigned long long tex;    /* cudaTextureObject_t (F16/F32 storage), 0 otherwise */
+};
+
+struct L3dFastView {
+    float k[4];
+    float kinv[4];
+    float range[4];            /* 1/min depth, 1/max depth, unused, geometric weight */
+    int W, H, ref, n;
+    unsigned flags;            /* bit 0: geometric pass */
+    int iterations;
+    int tiles_x;               /* pixel tiles per row of one colour */
+    int tile_start;            /* first tile of this view in the launch */
+    long long pix_off;         /* element offset of this view in hyp_all / cost_all / prior_all */
+    long long ref_img_off;
+    long long ref_dep_off;
+    unsigned long long ref_tex;
+    int has_prior;
+    int pack;                  /* store the packed depth map in the pack launch */
+    L3dFastSrc src[L3D_MAX_SOURCES];
+};
+
+struct L3dFastDev {
+    const L3dFastView* views;  /* device array */
+    const int* tile_start;     /* n_views + 1 prefix sums of tiles per view */
+    int n_views;
+    int total_tiles;
+    const void* images;        /* linear storage (BF16 sampling path) */
+    int storage;               /* L3D_DTYPE_F32/F16 (texture path) or BF16 (loads) */
+    float4* hyp;               /* hyp_all */
+    float* cost;               /* cost_all */
+    const float* prior;        /* prior_all (rows of views with has_prior) */
+    uint32_t* depths;
+};
+
+/* kernel: L3D_K_INIT or L3D_K_PROPAGATE; iteration/phase select the RNG stream and the
+ * refinement step; views with fewer iterations than `iteration + 1` are skipped. */
+cudaError_t l3d_launch_fast(int kernel, const L3dFastDev& d, int iteration, int phase,
+                            int lanes, cudaStream_t stream);
+/* pack of every view with pack != 0; max_pixels bounds the views' width * height */
+cudaError_t l3d_launch_fast_pack(const L3dFastDev& d, long long max_pixels, cudaStream_t stream);
+cudaError_t l3d_launch_fast_plane_cost(const L3dFastDev& d, const float4* planes, float* cost,
+                                       cudaStream_t stream);
 cudaError_t l3d_launch_plane_cost(const L3dParams& p, const L3dStereoDev& d, const float4* planes,
                                   float* cost, float* view_costs, int win, int dil,
                                   cudaStream_t stream);

@@ -1,0 +1,550 @@
+/*
+ * PatchMatch multi-view stereo, fast form: every reference view of a batch in one launch per
+ * kernel (init, each red/black colour, pack).
+ *
+ * Same algorithm, RNG stream and candidate schedule as frontend/src/app/vision/mvs/
+ * patchmatch.wgsl.ts (init 255-289, propagate 349-423, pack 425-433); what changes is how the
+ * multi-view NCC is evaluated:
+ *   - source images are FP16 (or FP32) CUDA arrays read through the texture unit with hardware
+ *     bilinear filtering at q.xy / q.z (the same filtered fetch the WGSL's textureSampleLevel
+ *     does); BF16 storage is sampled from linear memory with FP32 bilinear weights;
+ *   - the warped window is convex (q.z is affine and each image bound is a linear inequality in
+ *     the reference pixel once multiplied by q.z > 0), so its four corner samples decide whether
+ *     any of the 36 samples leaves the image: one test replaces 36 per-sample bounds checks and
+ *     the sample loop runs branch-free with incremental homogeneous coordinates;
+ *   - the NCC sums are accumulated in FP32 on values shifted by the reference window's centre
+ *     pixel (the shifted-data form of the weighted variance, which removes the cancellation of
+ *     E[x^2] - E[x]^2), with the reference terms w and w (r - c) precomputed per pixel;
+ *   - the k-best view mean keeps the three smallest costs in registers (same sum order as the
+ *     reference's partial selection sort).
+ * Blocks are tiles of 16 x 8 pixels of one colour of one view; a block loads its view's
+ * parameters (homography bases composed in FP64 on the host) into shared memory.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "l3d_fmath.h"
+#include "l3d_internal.h"
+
+namespace {
+
+constexpr int TX = 16;   /* colour columns per tile */
+constexpr int TY = 8;    /* rows per tile */
+constexpr int S = 36;    /* 6 x 6 window, offsets -5, -3, ..., 5 */
+
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float dot3f(float3 a, float3 b) {
+    return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x));
+}
+__device__ __forceinline__ float3 normalize_fast(float3 v) {
+    float il = rsqrtf(dot3f(v, v));
+    return make_float3(v.x * il, v.y * il, v.z * il);
+}
+
+__device__ __forceinline__ float unpack_depth(uint32_t packed) {
+    return l3d_f16_to_f32(packed & 0xffffu);
+}
+__device__ __forceinline__ float3 unpack_normal(uint32_t packed) {
+    float ex = (float)((packed >> 16) & 63u) * (2.0f / 63.0f) - 1.0f;
+    float ey = (float)((packed >> 22) & 63u) * (2.0f / 63.0f) - 1.0f;
+    float3 n = make_float3(ex, ey, (1.0f - fabsf(ex)) - fabsf(ey));
+    if (n.z < 0.0f) {
+        float nx = (1.0f - fabsf(n.y)) * (n.x >= 0.0f ? 1.0f : -1.0f);
+        float ny = (1.0f - fabsf(n.x)) * (n.y >= 0.0f ? 1.0f : -1.0f);
+        n.x = nx;
+        n.y = ny;
+    }
+    return normalize_fast(n);
+}
+__device__ __forceinline__ uint32_t pack_sample(float depth, float3 n, float cost) {
+    if (!(depth > 0.0f) || !(cost < 1.0f)) return 0u;
+    float s = (fabsf(n.x) + fabsf(n.y)) + fabsf(n.z);
+    float ex = n.x / s, ey = n.y / s;
+    if (n.z < 0.0f) {
+        float nx = (1.0f - fabsf(ey)) * (ex >= 0.0f ? 1.0f : -1.0f);
+        float ny = (1.0f - fabsf(ex)) * (ey >= 0.0f ? 1.0f : -1.0f);
+        ex = nx;
+        ey = ny;
+    }
+    float cx = fminf(fmaxf(fmaf(ex, 0.5f, 0.5f), 0.0f), 1.0f);
+    float cy = fminf(fmaxf(fmaf(ey, 0.5f, 0.5f), 0.0f), 1.0f);
+    uint32_t qx = (uint32_t)fmaf(cx, 63.0f, 0.5f);
+    uint32_t qy = (uint32_t)fmaf(cy, 63.0f, 0.5f);
+    uint32_t c = min(15u, (uint32_t)(cost * 15.0f));
+    return (l3d_f32_to_f16(depth) & 0xffffu) | (qx << 16) | (qy << 22) | (c << 28);
+}
+
+/* Image access: texture path (F16/F32 CUDA arrays, hardware bilinear) or BF16 linear memory. */
+template <bool TEX>
+struct Img {
+    /* value at filtering coordinate (u, v) = texel coordinate + 0.5 */
+    static __device__ __forceinline__ float sample(unsigned long long tex, const uint16_t* img,
+                                                   int W, int H, float u, float v) {
+        if (TEX) {
+            return tex2D<float>((cudaTextureObject_t)tex, u, v);
+        } else {
+            float x = u - 0.5f, y = v - 0.5f;
+            float x0 = floorf(x), y0 = floorf(y);
+            float fx = x - x0, fy = y - y0;
+            int ix0 = min(max((int)x0, 0), W - 1), iy0 = min(max((int)y0, 0), H - 1);
+            int ix1 = min(ix0 + 1, W - 1), iy1 = min(iy0 + 1, H - 1);
+            const uint16_t* r0 = img + (long long)iy0 * W;
+            const uint16_t* r1 = img + (long long)iy1 * W;
+            float a = __uint_as_float((uint32_t)__ldg(r0 + ix0) << 16);
+            float b = __uint_as_float((uint32_t)__ldg(r0 + ix1) << 16);
+            float c = __uint_as_float((uint32_t)__ldg(r1 + ix0) << 16);
+            float e = __uint_as_float((uint32_t)__ldg(r1 + ix1) << 16);
+            float top = fmaf(fx, b - a, a);
+            float bot = fmaf(fx, e - c, c);
+            return fmaf(fy, bot - top, top);
+        }
+    }
+    static __device__ __forceinline__ float texel(unsigned long long tex, const uint16_t* img,
+                                                  int W, int H, int x, int y) {
+        if (TEX) {
+            return tex2D<float>((cudaTextureObject_t)tex, (float)x + 0.5f, (float)y + 0.5f);
+        } else {
+            x = min(max(x, 0), W - 1);
+            y = min(max(y, 0), H - 1);
+            return __uint_as_float((uint32_t)__ldg(img + (long long)y * W + x) << 16);
+        }
+    }
+};
+
+/* Per-pixel state: the reference window as w and w (r - c), c = centre pixel. */
+struct FPix {
+    float rw[S], rwr[S];
+    float center, inv_sum, mean_r, var_r;
+    uint32_t rng;
+    float px, py;
+    float3 ray;
+};
+
+template <bool TEX>
+struct Fast {
+    const L3dFastView& v;
+    const L3dFastDev& d;
+    __device__ Fast(const L3dFastView& view, const L3dFastDev& dev) : v(view), d(dev) {}
+
+    __device__ const uint16_t* img(long long off) const {
+        return (const uint16_t*)d.images + off;
+    }
+
+    __device__ float3 ray_of(float x, float y) const {
+        return make_float3((x - v.k[2]) / v.k[0], (y - v.k[3]) / v.k[1], 1.0f);
+    }
+
+    __device__ float random(FPix& s) const { return l3d_random(&s.rng); }
+
+    /* prepare_window (patchmatch.wgsl.ts:90-110), shifted by the centre pixel */
+    __device__ void prepare(FPix& s, int x, int y) const {
+        const uint16_t* ri = img(v.ref_img_off);
+        const float center = Img<TEX>::texel(v.ref_tex, ri, v.W, v.H, x, y);
+        const float ic1 = 1.0f / (2.0f * 0.06f * 0.06f);
+        float sw = 0.0f, sr = 0.0f, srr = 0.0f;
+#pragma unroll
+        for (int i = 0; i < S; i++) {
+            const int ox = (i % 6) * 2 - 5, oy = (i / 6) * 2 - 5;
+            const float spatial = (float)(ox * ox + oy * oy) / (2.0f * 5.0f * 5.0f);
+            float val = Img<TEX>::texel(v.ref_tex, ri, v.W, v.H, x + ox, y + oy);
+            float dc = val - center;
+            float w = __expf(-(dc * dc) * ic1 - spatial);
+            s.rw[i] = w;
+            s.rwr[i] = w * dc;
+            sw += w;
+            sr = fmaf(w, dc, sr);
+            srr = fmaf(w * dc, dc, srr);
+        }
+        s.center = center;
+        s.inv_sum = 1.0f / sw;
+        s.mean_r = sr * s.inv_sum;
+        s.var_r = fmaxf(fmaf(-s.mean_r, s.mean_r, srr * s.inv_sum), 0.0f);
+    }
+
+    /* view_cost (patchmatch.wgsl.ts:130-159) with H = Bt + ktt u^T. */
+    __device__ float view_cost(const FPix& s, const L3dFastSrc& src, const float* u) const {
+        float h[9];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) h[r * 3 + c] = fmaf(src.ktt[r], u[c], src.Bt[r * 3 + c]);
+        const float x0 = s.px - 5.0f, y0 = s.py - 5.0f;
+        /* q at the window's top-left sample and its steps along x and y (2 pixels) */
+        const float qx0 = fmaf(h[0], x0, fmaf(h[1], y0, h[2]));
+        const float qy0 = fmaf(h[3], x0, fmaf(h[4], y0, h[5]));
+        const float qz0 = fmaf(h[6], x0, fmaf(h[7], y0, h[8]));
+        const float dxx = 2.0f * h[0], dxy = 2.0f * h[3], dxz = 2.0f * h[6];
+        const float dyx = 2.0f * h[1], dyy = 2.0f * h[4], dyz = 2.0f * h[7];
+        /* the four corner samples decide validity for the whole (convex) window */
+        const float umax = (float)src.W - 0.5f, vmax = (float)src.H - 0.5f;
+        bool ok = true;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float fx = (c & 1) ? 5.0f : 0.0f, fy = (c & 2) ? 5.0f : 0.0f;
+            float qz = fmaf(dyz, fy, fmaf(dxz, fx, qz0));
+            float qx = fmaf(dyx, fy, fmaf(dxx, fx, qx0));
+            float qy = fmaf(dyy, fy, fmaf(dxy, fx, qy0));
+            ok = ok && qz > 1e-6f && qx >= 0.5f * qz && qy >= 0.5f * qz && qx <= umax * qz &&
+                 qy <= vmax * qz;
+        }
+        if (!ok) return 2.0f;
+        const uint16_t* si = img(src.img_off);
+        float ss = 0.0f, sss = 0.0f, srs = 0.0f;
+        float rx = qx0, ry = qy0, rz = qz0;
+#pragma unroll
+        for (int r = 0; r < 6; r++) {
+            float qx = rx, qy = ry, qz = rz;
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                const int i = r * 6 + c;
+                float iz = rcp_fast(qz);
+                float val = Img<TEX>::sample(src.tex, si, src.W, src.H, qx * iz, qy * iz);
+                float sv = val - s.center;  /* s' = s - c; r' = r - c lives in rwr / rw */
+                float t = s.rw[i] * sv;
+                ss += t;
+                sss = fmaf(t, sv, sss);
+                srs = fmaf(s.rwr[i], sv, srs);
+                qx += dxx;
+                qy += dxy;
+                qz += dxz;
+            }
+            rx += dyx;
+            ry += dyy;
+            rz += dyz;
+        }
+        float mean = ss * s.inv_sum;
+        float var_s = fmaxf(fmaf(-mean, mean, sss * s.inv_sum), 0.0f);
+        float prod = s.var_r * var_s;
+        if (prod < 1e-10f) return 1.0f;  /* sqrt(prod) < 1e-5 */
+        float cov = fmaf(-s.mean_r, mean, srs * s.inv_sum);
+        return fminf(fmaxf(1.0f - cov * rsqrtf(prod), 0.0f), 2.0f);
+    }
+
+    /* reproject (patchmatch.wgsl.ts:166-190) */
+    __device__ bool reproject(const L3dFastSrc& sv, float px, float py, float3 x, float* dist,
+                              float* z) const {
+        const float* R = sv.R;
+        float3 xs = make_float3(fmaf(R[2], x.z, fmaf(R[1], x.y, fmaf(R[0], x.x, sv.t[0]))),
+                                fmaf(R[5], x.z, fmaf(R[4], x.y, fmaf(R[3], x.x, sv.t[1]))),
+                                fmaf(R[8], x.z, fmaf(R[7], x.y, fmaf(R[6], x.x, sv.t[2]))));
+        if (!(xs.z > 1e-6f)) return false;
+        float iz = 1.0f / xs.z;
+        float rx = rintf(fmaf(sv.k[0] * xs.x, iz, sv.k[2]));
+        float ry = rintf(fmaf(sv.k[1] * xs.y, iz, sv.k[3]));
+        if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)sv.W && ry < (float)sv.H)) return false;
+        uint32_t packed = __ldg(d.depths + sv.dep_off + (long long)(int)ry * sv.W + (int)rx);
+        float ds = unpack_depth(packed);
+        if (!(ds > 0.0f) || (packed >> 28) > L3D_FILTER_COST) return false;
+        float3 e = make_float3(((rx - sv.k[2]) / sv.k[0]) * ds - sv.t[0],
+                               ((ry - sv.k[3]) / sv.k[1]) * ds - sv.t[1], ds - sv.t[2]);
+        float3 back = make_float3(fmaf(R[6], e.z, fmaf(R[3], e.y, R[0] * e.x)),
+                                  fmaf(R[7], e.z, fmaf(R[4], e.y, R[1] * e.x)),
+                                  fmaf(R[8], e.z, fmaf(R[5], e.y, R[2] * e.x)));
+        if (!(back.z > 1e-6f)) return false;
+        float bz = 1.0f / back.z;
+        float dx = fmaf(v.k[0] * back.x, bz, v.k[2]) - px;
+        float dy = fmaf(v.k[1] * back.y, bz, v.k[3]) - py;
+        *dist = sqrtf(fmaf(dx, dx, dy * dy));
+        *z = back.z;
+        return true;
+    }
+
+    /* hypothesis_cost (patchmatch.wgsl.ts:192-233) */
+    __device__ float hypothesis_cost(const FPix& s, float3 n, float dd) const {
+        if (!(dd > 0.0f)) return 2.0f;
+        float inv = 1.0f / dd;
+        if (inv > v.range[0] || inv < v.range[1]) return 2.0f;
+        if (dot3f(n, s.ray) >= -1e-3f) return 2.0f;
+        const int count = v.n;
+        if (count == 0) return 2.0f;
+        float3 x = make_float3(s.ray.x * dd, s.ray.y * dd, dd);
+        float ir = 1.0f / dot3f(n, x);
+        float u[3];
+        u[0] = (n.x * v.kinv[0]) * ir;
+        u[1] = (n.y * v.kinv[1]) * ir;
+        u[2] = fmaf(n.x, v.kinv[2], fmaf(n.y, v.kinv[3], n.z)) * ir;
+        const bool geometric = (v.flags & 1u) != 0u;
+        /* the three smallest view costs, ascending */
+        float b0 = 3.0e38f, b1 = 3.0e38f, b2 = 3.0e38f;
+        for (int k = 0; k < count; k++) {
+            float c = view_cost(s, v.src[k], u);
+            if (geometric) {
+                float dist, z;
+                bool ok = reproject(v.src[k], s.px, s.py, x, &dist, &z);
+                c = fmaf(v.range[3], ok ? fminf(dist, 3.0f) : 3.0f, c);
+            }
+            if (c < b2) {
+                if (c < b1) {
+                    b2 = b1;
+                    if (c < b0) {
+                        b1 = b0;
+                        b0 = c;
+                    } else {
+                        b1 = c;
+                    }
+                } else {
+                    b2 = c;
+                }
+            }
+        }
+        const int kk = max(1, min(3, count - 1));
+        float total = b0;
+        if (kk > 1) total = total + b1;
+        if (kk > 2) total = total + b2;
+        return total / (float)kk;
+    }
+
+    /* random_normal, random_depth (patchmatch.wgsl.ts:235-249) */
+    __device__ float3 random_normal(FPix& s) const {
+        float z = fmaf(random(s), 2.0f, -1.0f);
+        float a = random(s) * 6.2831853f;
+        float r = sqrtf(fmaxf(0.0f, fmaf(-z, z, 1.0f)));
+        float sn, cs;
+        __sincosf(a, &sn, &cs);
+        float3 n = make_float3(r * cs, r * sn, z);
+        float3 view = normalize_fast(s.ray);
+        if (dot3f(n, view) > 0.0f) n = make_float3(-n.x, -n.y, -n.z);
+        return normalize_fast(make_float3(fmaf(view.x, -0.5f, n.x), fmaf(view.y, -0.5f, n.y),
+                                          fmaf(view.z, -0.5f, n.z)));
+    }
+    __device__ float random_depth(FPix& s) const {
+        float t = random(s);
+        return 1.0f / fmaf(v.range[0], t, v.range[1] * (1.0f - t));
+    }
+
+    __device__ void begin(FPix& s, int x, int y, int iteration, int phase) const {
+        s.px = (float)x;
+        s.py = (float)y;
+        uint32_t seed = (uint32_t)(v.ref + 1) * 0x9e3779b1u + (uint32_t)iteration * 97u +
+                        (uint32_t)phase * 13u + (v.flags & 1u) * 7u;
+        s.rng = l3d_pcg((uint32_t)(y * v.W + x) ^
+                        l3d_pcg(seed + (uint32_t)iteration * 7919u + (uint32_t)phase * 104729u));
+        prepare(s, x, y);
+        s.ray = ray_of(s.px, s.py);
+    }
+};
+
+/* Block -> (view, tile) and the view's parameters in shared memory. */
+__device__ __forceinline__ int find_view(const L3dFastDev& d, int tile) {
+    int lo = 0, hi = d.n_views - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(d.tile_start + mid) <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+/* The view table has an 8-byte aligned stride (static_assert below), so it is copied in 8-byte
+ * words. */
+static_assert(sizeof(L3dFastView) % 8 == 0, "view table stride must be a multiple of 8 bytes");
+static_assert(alignof(L3dFastView) >= 8, "view table must be 8-byte aligned");
+__device__ __forceinline__ void load_view(L3dFastView& dst, const L3dFastView* src) {
+    const unsigned long long* s = (const unsigned long long*)src;
+    unsigned long long* o = (unsigned long long*)&dst;
+    for (int i = threadIdx.x; i < (int)(sizeof(L3dFastView) / 8); i += blockDim.x) o[i] = __ldg(s + i);
+    __syncthreads();
+}
+
+__device__ __forceinline__ void near_offset(int i, int* ox, int* oy) {
+    int m = (i + 1) / 2;
+    *ox = (i & 1) ? -m : m;
+    *oy = -(m + 1);
+}
+__device__ __forceinline__ void orient(int ox, int oy, int dir, int* rx, int* ry) {
+    switch (dir) {
+        case 1: *rx = ox; *ry = -oy; break;
+        case 2: *rx = oy; *ry = ox; break;
+        case 3: *rx = -oy; *ry = ox; break;
+        default: *rx = ox; *ry = oy; break;
+    }
+}
+
+template <bool TEX>
+__global__ void __launch_bounds__(128) k_fast_init(const L3dFastDev d) {
+    __shared__ __align__(16) L3dFastView sv;
+    load_view(sv, d.views + find_view(d, blockIdx.x));
+    const int local = blockIdx.x - sv.tile_start;
+    const int y = (local / sv.tiles_x) * TY + threadIdx.x / TX;
+    /* init covers every pixel: a tile spans 32 image columns, two pixels per thread */
+    Fast<TEX> f(sv, d);
+    for (int half = 0; half < 2; half++) {
+        const int xx = (local % sv.tiles_x) * (2 * TX) + (threadIdx.x % TX) * 2 + half;
+        if (xx >= sv.W || y >= sv.H) continue;
+        FPix s;
+        f.begin(s, xx, y, 0, 0);
+        const long long index = (long long)y * sv.W + xx;
+        float3 n = f.random_normal(s);
+        float dd = f.random_depth(s);
+        if (sv.flags & 1u) {
+            uint32_t packed = d.depths[sv.ref_dep_off + index];
+            if (unpack_depth(packed) > 0.0f) {
+                dd = unpack_depth(packed);
+                n = unpack_normal(packed);
+            }
+        }
+        float c = f.hypothesis_cost(s, n, dd);
+        if (!(sv.flags & 1u) && sv.has_prior) {
+            float pd = d.prior[sv.pix_off + index];
+            if (pd > 0.0f) {
+                float3 vv = normalize_fast(s.ray);
+                float3 pn = make_float3(-vv.x, -vv.y, -vv.z);
+                float pc = f.hypothesis_cost(s, pn, pd);
+                if (pc < c) {
+                    c = pc;
+                    n = pn;
+                    dd = pd;
+                }
+            }
+        }
+        d.hyp[sv.pix_off + index] = make_float4(n.x, n.y, n.z, dd);
+        d.cost[sv.pix_off + index] = c;
+    }
+}
+
+template <bool TEX>
+__global__ void __launch_bounds__(128) k_fast_propagate(const L3dFastDev d, int iteration,
+                                                        int phase, float step) {
+    __shared__ __align__(16) L3dFastView sv;
+    load_view(sv, d.views + find_view(d, blockIdx.x));
+    if (iteration >= sv.iterations) return;
+    const int local = blockIdx.x - sv.tile_start;
+    const int y = (local / sv.tiles_x) * TY + threadIdx.x / TX;
+    const int x = ((local % sv.tiles_x) * TX + threadIdx.x % TX) * 2 + ((y + phase) & 1);
+    if (x >= sv.W || y >= sv.H) return;
+    Fast<TEX> f(sv, d);
+    FPix s;
+    f.begin(s, x, y, iteration, phase);
+    const int W = sv.W, H = sv.H;
+    const long long base = sv.pix_off;
+    const long long index = (long long)y * W + x;
+    float4 b = d.hyp[base + index];
+    float3 bn = make_float3(b.x, b.y, b.z);
+    float bd = b.w;
+    float best_cost = d.cost[base + index];
+    for (int region = 0; region < 8; region++) {
+        const int count = region < 4 ? 7 : 11;
+        int chosen = -1;
+        float chosen_cost = 1e9f;
+        for (int i = 0; i < count; i++) {
+            int ox = 0, oy = -3 - 2 * i;
+            if (region < 4) near_offset(i, &ox, &oy);
+            int rx, ry;
+            orient(ox, oy, region & 3, &rx, &ry);
+            int qx = x + rx, qy = y + ry;
+            if (qx < 0 || qy < 0 || qx >= W || qy >= H) continue;
+            int qi = qy * W + qx;
+            float c = d.cost[base + qi];
+            if (c < chosen_cost) {
+                chosen_cost = c;
+                chosen = qi;
+            }
+        }
+        if (chosen < 0) continue;
+        float4 h = d.hyp[base + chosen];
+        float3 hn = make_float3(h.x, h.y, h.z);
+        float3 rq = f.ray_of((float)(chosen % W), (float)(chosen / W));
+        float den = dot3f(hn, s.ray);
+        if (fabsf(den) < 1e-6f) continue;
+        float dd = dot3f(hn, make_float3(rq.x * h.w, rq.y * h.w, h.w)) / den;
+        float c = f.hypothesis_cost(s, hn, dd);
+        if (c < best_cost) {
+            best_cost = c;
+            bn = hn;
+            bd = dd;
+        }
+    }
+    float3 view = normalize_fast(s.ray);
+    float3 n_random = f.random_normal(s);
+    float d_random = f.random_depth(s);
+    float e = (fmaf(f.random(s), 2.0f, -1.0f) * 0.15f) * step;
+    float d_perturbed = 1.0f / ((1.0f / bd) * (1.0f + e));
+    float r1 = f.random(s), r2 = f.random(s), r3 = f.random(s);
+    float3 n_perturbed = normalize_fast(make_float3(bn.x + (fmaf(r1, 2.0f, -1.0f) * 0.6f) * step,
+                                                    bn.y + (fmaf(r2, 2.0f, -1.0f) * 0.6f) * step,
+                                                    bn.z + (fmaf(r3, 2.0f, -1.0f) * 0.6f) * step));
+    if (dot3f(n_perturbed, view) >= 0.0f) n_perturbed = bn;
+    const float3 cur_n = bn;
+    const float cur_d = bd;
+    for (int c = 0; c < 6; c++) {
+        float3 nn = (c == 0 || c == 3) ? n_random : ((c == 1 || c == 5) ? n_perturbed : cur_n);
+        float dv = (c == 0 || c == 2) ? d_random : ((c == 1 || c == 4) ? d_perturbed : cur_d);
+        float cand = f.hypothesis_cost(s, nn, dv);
+        if (cand < best_cost) {
+            best_cost = cand;
+            bn = nn;
+            bd = dv;
+        }
+    }
+    d.hyp[base + index] = make_float4(bn.x, bn.y, bn.z, bd);
+    d.cost[base + index] = best_cost;
+}
+
+__global__ void k_fast_pack(const L3dFastDev d) {
+    const L3dFastView* v = d.views + blockIdx.y;
+    if (!__ldg(&v->pack)) return;
+    const int W = __ldg(&v->W), H = __ldg(&v->H);
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)W * H) return;
+    const long long base = __ldg(&v->pix_off);
+    float4 h = d.hyp[base + i];
+    d.depths[__ldg(&v->ref_dep_off) + i] = pack_sample(h.w, make_float3(h.x, h.y, h.z), d.cost[base + i]);
+}
+
+template <bool TEX>
+__global__ void __launch_bounds__(128) k_fast_plane_cost(const L3dFastDev d, const float4* planes,
+                                                         float* cost) {
+    __shared__ __align__(16) L3dFastView sv;
+    load_view(sv, d.views + find_view(d, blockIdx.x));
+    const int local = blockIdx.x - sv.tile_start;
+    const int y = (local / sv.tiles_x) * TY + threadIdx.x / TX;
+    Fast<TEX> f(sv, d);
+    for (int half = 0; half < 2; half++) {
+        const int x = (local % sv.tiles_x) * (2 * TX) + (threadIdx.x % TX) * 2 + half;
+        if (x >= sv.W || y >= sv.H) continue;
+        FPix s;
+        f.begin(s, x, y, 0, 0);
+        const long long index = (long long)y * sv.W + x;
+        float4 p = planes[sv.pix_off + index];
+        cost[sv.pix_off + index] = f.hypothesis_cost(s, make_float3(p.x, p.y, p.z), p.w);
+    }
+}
+
+}  // namespace
+
+cudaError_t l3d_launch_fast(int kernel, const L3dFastDev& d, int iteration, int phase, int lanes,
+                            cudaStream_t stream) {
+    (void)lanes;
+    const bool tex = d.storage != 3; /* BF16 is sampled from linear memory */
+    if (d.total_tiles <= 0) return cudaSuccess;
+    if (kernel == L3D_K_INIT) {
+        if (tex) k_fast_init<true><<<d.total_tiles, 128, 0, stream>>>(d);
+        else k_fast_init<false><<<d.total_tiles, 128, 0, stream>>>(d);
+    } else if (kernel == L3D_K_PROPAGATE) {
+        float step = ldexpf(1.0f, -iteration);
+        if (tex) k_fast_propagate<true><<<d.total_tiles, 128, 0, stream>>>(d, iteration, phase, step);
+        else k_fast_propagate<false><<<d.total_tiles, 128, 0, stream>>>(d, iteration, phase, step);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_fast_pack(const L3dFastDev& d, long long max_pixels, cudaStream_t stream) {
+    if (d.n_views <= 0 || max_pixels <= 0) return cudaSuccess;
+    dim3 grid((unsigned)((max_pixels + 255) / 256), (unsigned)d.n_views);
+    k_fast_pack<<<grid, 256, 0, stream>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_fast_plane_cost(const L3dFastDev& d, const float4* planes, float* cost,
+                                       cudaStream_t stream) {
+    if (d.total_tiles <= 0) return cudaSuccess;
+    if (d.storage != 3) k_fast_plane_cost<true><<<d.total_tiles, 128, 0, stream>>>(d, planes, cost);
+    else k_fast_plane_cost<false><<<d.total_tiles, 128, 0, stream>>>(d, planes, cost);
+    return cudaGetLastError();
+}

@@ -1,0 +1,129 @@
+"""The fast PatchMatch form (FP16/BF16 image storage, texture-filtered samples, batched views).
+
+It is not bit-exact by design (hardware bilinear weights, FP16/BF16 storage, approximate
+reciprocals), so it is checked the way a precision change is checked: the NCC cost of fixed
+planes against the FP64 oracle, depth accuracy against ground truth next to the plain FP32 form,
+and determinism (a batch equals its views solved one at a time).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import arc_workload, assert_bit_equal
+from luvas3d import (DTYPE_BF16, DTYPE_F16, DTYPE_F32, FORM_FAST, FORM_PLAIN, DenseStereo,
+                     L3dError, SolveOptions, StereoOptions, packing)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def arc():
+    return arc_workload(n=5, W=256, H=192, f=224.0)
+
+
+def make(views, imgs, W, H, form=FORM_FAST, storage=DTYPE_F16):
+    s = DenseStereo(W, H, views, StereoOptions(form=form, storage=storage))
+    for i, im in enumerate(imgs):
+        s.set_image(i, np.asarray(im, dtype=np.float32))
+    return s
+
+
+@pytest.mark.parametrize("storage", [DTYPE_F16, DTYPE_BF16, DTYPE_F32])
+def test_fixed_plane_cost_close_to_fp64(arc, storage):
+    views, imgs, truth, srcs = arc
+    W, H = 256, 192
+    # planes of the true surface (depth from the ray cast, normal facing the camera)
+    planes = np.zeros((H, W, 4), dtype=np.float32)
+    planes[..., 2] = -1.0
+    planes[..., 3] = np.where(truth[2] > 0, truth[2], 1.0)
+    o = oracle.Stereo(W, H, views, imgs, 64)
+    want, _ = o.plane_cost(2, srcs[2], planes.astype(np.float64), min_depth=0.5, max_depth=5.0)
+    s = make(views, imgs, W, H, storage=storage)
+    got = s.plane_cost(2, SolveOptions(srcs[2], 0.5, 5.0), planes)
+    valid = (want < 1.5) & (got < 1.5)
+    assert valid.mean() > 0.7
+    assert np.array_equal(want >= 1.5, got >= 1.5) or np.mean((want >= 1.5) != (got >= 1.5)) < 0.01
+    err = np.abs(got[valid] - want[valid])
+    p99 = np.percentile(err, 99)
+    print(f"storage {storage}: cost error vs FP64 max {err.max():.2e} p99 {p99:.2e} "
+          f"median {np.median(err):.2e}")
+    tol = {DTYPE_F32: 2e-3, DTYPE_F16: 5e-3, DTYPE_BF16: 2e-2}[storage]
+    assert p99 < tol
+
+
+def depth_stats(hyp, truth):
+    m = truth > 0
+    rel = np.abs(hyp[..., 3] - truth) / np.where(m, truth, 1)
+    return np.median(rel[m]), (rel[m] < 0.01).mean()
+
+
+@pytest.mark.parametrize("storage", [DTYPE_F16, DTYPE_BF16])
+def test_fast_depth_accuracy_matches_plain(arc, storage):
+    views, imgs, truth, srcs = arc
+    W, H = 256, 192
+    plain = make(views, imgs, W, H, form=FORM_PLAIN, storage=DTYPE_F32)
+    fast = make(views, imgs, W, H, storage=storage)
+    opts = SolveOptions(srcs[2], 0.5, 5.0, iterations=5)
+    plain.solve(2, opts)
+    fast.solve(2, opts)
+    pm, pf = depth_stats(plain.read_hypotheses()[0], truth[2])
+    fm, ff = depth_stats(fast.read_hypotheses()[0], truth[2])
+    print(f"plain median {pm:.2e} within1% {pf:.3f} | fast({storage}) median {fm:.2e} within1% {ff:.3f}")
+    assert fm < max(1.25 * pm, pm + 3e-4)
+    assert ff > pf - 0.03
+    # packed maps valid on a similar share of pixels
+    vp = (plain.depth_map(2) != 0).mean()
+    vf = (fast.depth_map(2) != 0).mean()
+    assert abs(vp - vf) < 0.05
+
+
+def test_batch_equals_single_views(arc):
+    views, imgs, truth, srcs = arc
+    W, H = 256, 192
+    a = make(views, imgs, W, H)
+    b = make(views, imgs, W, H)
+    opts = [SolveOptions(srcs[r], 0.5, 5.0, iterations=3) for r in range(5)]
+    a.solve_all(list(range(5)), opts)
+    for r in range(5):
+        b.solve(r, opts[r])
+        hb, cb = b.read_hypotheses()
+        ha, ca = a.read_hypotheses_layer(r)
+        assert_bit_equal(ha, hb, f"view {r} hyp")
+        assert_bit_equal(ca, cb, f"view {r} cost")
+        assert_bit_equal(a.depth_map(r), b.depth_map(r), f"view {r} packed")
+
+
+def test_mixed_iterations_and_pack_flags(arc):
+    views, imgs, truth, srcs = arc
+    W, H = 256, 192
+    a = make(views, imgs, W, H)
+    b = make(views, imgs, W, H)
+    opts = [SolveOptions(srcs[r], 0.5, 5.0, iterations=1 + r % 3, pack=r != 1) for r in range(5)]
+    a.solve_all(list(range(5)), opts)
+    for r in range(5):
+        b.solve(r, opts[r])
+        assert_bit_equal(a.read_hypotheses_layer(r)[0], b.read_hypotheses()[0], f"view {r}")
+    assert np.all(a.depth_map(1) == 0)
+
+
+def test_geometric_batch_runs_and_keeps_accuracy(arc):
+    views, imgs, truth, srcs = arc
+    W, H = 256, 192
+    a = make(views, imgs, W, H)
+    refs = list(range(5))
+    a.solve_all(refs, [SolveOptions(srcs[r], 0.5, 5.0, iterations=4) for r in refs])
+    before = depth_stats(a.read_hypotheses_layer(2)[0], truth[2])
+    a.solve_all(refs, [SolveOptions(srcs[r], 0.5, 5.0, iterations=1, geometric=True) for r in refs])
+    after = depth_stats(a.read_hypotheses_layer(2)[0], truth[2])
+    print("photometric", before, "geometric", after)
+    assert after[0] < before[0] * 1.5 + 1e-4
+
+
+def test_fast_form_rejections(arc):
+    views, imgs, truth, srcs = arc
+    with pytest.raises(L3dError):
+        DenseStereo(64, 48, views, StereoOptions(form=FORM_FAST, storage=DTYPE_F16, window=11,
+                                                 dilation=1))
+    s = make(views, [im[:48, :64] for im in imgs], 64, 48)
+    with pytest.raises(L3dError):
+        s.solve_all([0, 0], [SolveOptions([1], 0.5, 5.0)] * 2)
