@@ -259,6 +259,30 @@ int64_t l3d_tsdf_launches(const l3d_tsdf* t);
 /* TsdfVolume.destroy() (tsdf-volume.ts:484-495). */
 void l3d_tsdf_destroy(l3d_tsdf* t);
 
+/* Largest volume, in 8^3 bricks, that l3d_tsdf_integrate_noalloc accepts (a dense grid has
+ * ceil(X/8) * ceil(Y/8) * ceil(Z/8) bricks; 2^20 covers 768^3). */
+#define L3D_NOALLOC_MAX_BRICKS (1 << 20)
+
+/* Integrates one packed depth map into a TSDF volume without allocating any device memory.
+ * No counterpart in the reference: it exists for callers that cannot let this library call
+ * cudaMalloc, because their device memory is owned by another allocator (a framework's caching
+ * allocator, a pool sized once at start-up) or because an allocation's device-wide
+ * synchronisation would stall the rest of their pipeline.  The caller owns every buffer: desc
+ * describes the volume as for l3d_tsdf_create (desc->coords and desc->stream are ignored),
+ * coords_dev holds the brick pool's coordinates on the device (NULL for a dense grid),
+ * depth_dev the width * height packed map, prior_dev an optional width * height prior (NULL =
+ * none; view->prior is ignored), tsdf_dev and weight_dev the volume (16-byte aligned, tsdf 1 and
+ * weight 0 for a fresh volume).  The update equals l3d_tsdf_integrate bit for bit.
+ * The per-brick visibility flags live in a static device array of L3D_NOALLOC_MAX_BRICKS bytes
+ * that every GPU using the library keeps until exit; larger volumes are rejected with
+ * L3D_EINVAL.  The first call on each device looks that array's address up (make it before any
+ * stream capture); all calls share the array, so calls whose kernels overlap on the GPU race.
+ * Work is enqueued on `stream` (a cudaStream_t, NULL = the default stream). */
+int l3d_tsdf_integrate_noalloc(const l3d_tsdf_desc* desc, const int32_t* coords_dev,
+                               const uint32_t* depth_dev, const float* prior_dev,
+                               const l3d_integration_view* view, float* tsdf_dev,
+                               void* weight_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -470,6 +470,8 @@ int fast_solve(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
 
 }  // namespace
 
+void l3d_set_error(const char* msg) { g_error = msg ? msg : ""; }
+
 extern "C" {
 
 size_t l3d_last_error(char* buf, size_t size) {

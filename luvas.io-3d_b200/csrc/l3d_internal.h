@@ -165,4 +165,7 @@ cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_
 cudaError_t l3d_launch_tsdf_fill(float* tsdf, void* weight, long long voxels, int q8,
                                  cudaStream_t stream);
 
+/* Sets the calling thread's l3d_last_error() message (capi.cu). */
+void l3d_set_error(const char* msg);
+
 #endif

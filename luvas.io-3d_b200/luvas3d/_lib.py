@@ -18,6 +18,7 @@ FORM_PLAIN, FORM_FAST = 0, 1
 WEIGHT_F32, WEIGHT_Q8 = 0, 1
 KERNEL_INIT, KERNEL_INIT_COARSE, KERNEL_PROPAGATE, KERNEL_PACK, KERNEL_CONSISTENCY = range(5)
 MAX_SOURCES = 8
+NOALLOC_MAX_BRICKS = 1 << 20
 
 
 class L3dError(RuntimeError):
@@ -144,6 +145,8 @@ SIGNATURES = [
     ("l3d_tsdf_synchronize", C.c_int, [_P]),
     ("l3d_tsdf_launches", C.c_int64, [_P]),
     ("l3d_tsdf_destroy", None, [_P]),
+    ("l3d_tsdf_integrate_noalloc", C.c_int, [C.POINTER(TsdfDesc), _P, _P, _P,
+                                             C.POINTER(IntegrationView), _P, _P, _P]),
 ]
 
 _lib = None
