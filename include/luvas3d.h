@@ -88,7 +88,7 @@ typedef struct {
     const l3d_stereo* coarse; /* CoarseLevel (dense-stereo.ts:78-82): its planes seed from_coarse
                                  solves; it must outlive this handle.  NULL = none */
     int32_t depth_maps;       /* 1: a packed depth map per view (default); 0: one map */
-    int32_t storage;          /* device image storage: F32 (plain form), F16 or BF16 */
+    int32_t storage;          /* device image storage: F32 (plain form); U8, F16, BF16 or F32 (fast) */
     int32_t form;             /* L3D_FORM_PLAIN or L3D_FORM_FAST */
     int32_t window;           /* samples per window side: 6 (reference, offsets +-1,3,5) or 11 */
     int32_t dilation;         /* spacing of window samples: 2 (reference) or 1 */
@@ -224,6 +224,13 @@ int l3d_stereo_stream(const l3d_stereo* s, void** stream);
 int l3d_stereo_synchronize(l3d_stereo* s);
 /* Device kernels launched by this handle since creation (for launch accounting). */
 int64_t l3d_stereo_launches(const l3d_stereo* s);
+
+/* Fast-form kernel variant (no reference counterpart; the reference has one WGSL kernel):
+ * window rows sampled by the texture unit (6, 4, 3 or 2; the others use software bilinear
+ * on the LSU path) + 8 for the 2x2 quad lane mapping.  All variants compute the same algorithm;
+ * results differ only by the texture unit's 8-bit filter weights on the rows it samples. */
+int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant);
+int32_t l3d_stereo_variant(const l3d_stereo* s);
 /* DenseStereo.destroy() (dense-stereo.ts:403-416). */
 void l3d_stereo_destroy(l3d_stereo* s);
 

@@ -22,6 +22,10 @@
 #include "../../include/luvas3d.h"
 #include "l3d_internal.h"
 
+/* Fast-form kernel variant: window rows through the texture unit (0..6; the others use software
+ * bilinear on the pair image) + 8 for the 2x2 quad lane mapping. */
+#define L3D_FAST_DEFAULT_VARIANT 14
+
 namespace {
 
 thread_local std::string g_error;
@@ -101,6 +105,8 @@ struct l3d_stereo {
     int* tile_start_host = nullptr;
     int fview_cap = 0;
     cudaEvent_t staged = nullptr;      /* after the last copy out of the pinned staging */
+    uint32_t* pairs = nullptr;         /* fast form: half2(texel, right neighbour) per pixel */
+    int variant = L3D_FAST_DEFAULT_VARIANT;
 };
 
 namespace {
@@ -415,6 +421,7 @@ int fast_batch(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
     d.n_views = n;
     d.total_tiles = tiles;
     d.images = s->images;
+    d.pairs = s->pairs;
     d.storage = s->opts.storage;
     d.hyp = hyp;
     d.cost = cost;
@@ -425,7 +432,7 @@ int fast_batch(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
 }
 
 int fast_launch(l3d_stereo* s, int kernel, const L3dFastDev& d, int it, int phase) {
-    cudaError_t e = l3d_launch_fast(kernel, d, it, phase, 1, s->stream);
+    cudaError_t e = l3d_launch_fast(kernel, d, it, phase, s->variant, s->stream);
     s->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
     return L3D_OK;
@@ -509,8 +516,9 @@ int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_
         return fail(L3D_EINVAL, "unknown form %d", o.form);
     if (o.form == L3D_FORM_PLAIN && o.storage != L3D_DTYPE_F32)
         return fail(L3D_EINVAL, "the plain form stores images as F32");
-    if (o.storage != L3D_DTYPE_F32 && o.storage != L3D_DTYPE_F16 && o.storage != L3D_DTYPE_BF16)
-        return fail(L3D_EINVAL, "image storage must be F32, F16 or BF16");
+    if (o.storage != L3D_DTYPE_F32 && o.storage != L3D_DTYPE_F16 && o.storage != L3D_DTYPE_BF16 &&
+        o.storage != L3D_DTYPE_U8)
+        return fail(L3D_EINVAL, "image storage must be U8, F32, F16 or BF16");
     if (o.form == L3D_FORM_FAST && !(o.window == 6 && o.dilation == 2))
         return fail(L3D_EINVAL, "the fast form uses the reference window (6 samples, dilation 2)");
     for (int i = 0; i < n_views; i++) {
@@ -549,8 +557,9 @@ int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_
     if (o.form == L3D_FORM_FAST && o.storage != L3D_DTYPE_BF16) {
         /* texture-sampled copies: block-linear CUDA arrays with hardware bilinear filtering,
          * clamp-to-edge addressing and unnormalised coordinates (texel centres at +0.5) */
-        cudaChannelFormatDesc ch = o.storage == L3D_DTYPE_F16 ? cudaCreateChannelDescHalf()
-                                                              : cudaCreateChannelDesc<float>();
+        cudaChannelFormatDesc ch = o.storage == L3D_DTYPE_F16  ? cudaCreateChannelDescHalf()
+                                   : o.storage == L3D_DTYPE_U8 ? cudaCreateChannelDesc<unsigned char>()
+                                                               : cudaCreateChannelDesc<float>();
         s->arrays.assign(n_views, nullptr);
         s->texs.assign(n_views, 0);
         for (int i = 0; i < n_views; i++) {
@@ -565,11 +574,17 @@ int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_
             td.addressMode[0] = cudaAddressModeClamp;
             td.addressMode[1] = cudaAddressModeClamp;
             td.filterMode = cudaFilterModeLinear;
-            td.readMode = cudaReadModeElementType;
+            /* U8 texels read as value / 255 (the r8unorm format of the reference's textures) */
+            td.readMode = o.storage == L3D_DTYPE_U8 ? cudaReadModeNormalizedFloat
+                                                    : cudaReadModeElementType;
             td.normalizedCoords = 0;
             if ((e = cudaCreateTextureObject(&s->texs[i], &res, &td, nullptr)) != cudaSuccess)
                 return cleanup(cuda_fail(e, "texture creation"));
         }
+        if ((e = dalloc(&s->pairs, (size_t)n_views * s->P)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "pair image allocation"));
+        if ((e = cudaMemsetAsync(s->pairs, 0, (size_t)n_views * s->P * 4, s->stream)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "device clear"));
     }
     if ((e = cudaMalloc(&s->images, (size_t)n_views * s->P * esize)) != cudaSuccess ||
         (e = dalloc(&s->depths, (size_t)s->n_maps * s->P)) != cudaSuccess ||
@@ -624,6 +639,12 @@ int l3d_stereo_set_image(l3d_stereo* s, int32_t layer, int32_t dtype, const void
         L3D_CUDA(cudaMemcpy2DToArrayAsync(s->arrays[layer], 0, 0, dst, rb, rb, s->H,
                                           cudaMemcpyDeviceToDevice, s->stream),
                  "image array copy");
+    }
+    if (s->pairs) {
+        e = l3d_launch_make_pairs(dst, s->opts.storage, s->W, s->H, s->pairs + (size_t)layer * s->P,
+                                  s->stream);
+        s->launches++;
+        if (e != cudaSuccess) return cuda_fail(e, "pair image");
     }
     return L3D_OK;
 }
@@ -809,7 +830,7 @@ int l3d_stereo_plane_cost(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o, c
         l3d_solve_opts one = *o;
         one.prior = nullptr;
         if ((rc = fast_batch(s, 1, &ref, &one, s->hyp, s->cost, s->prior, false, &fd))) return rc;
-        cudaError_t e = l3d_launch_fast_plane_cost(fd, s->planes, s->plane_out, s->stream);
+        cudaError_t e = l3d_launch_fast_plane_cost(fd, s->planes, s->plane_out, s->variant, s->stream);
         s->launches++;
         if (e != cudaSuccess) return cuda_fail(e, "plane cost launch");
         return read_dev(s, cost, s->plane_out, s->P * 4, "read plane cost");
@@ -854,6 +875,18 @@ int l3d_stereo_synchronize(l3d_stereo* s) {
 
 int64_t l3d_stereo_launches(const l3d_stereo* s) { return s ? s->launches : -1; }
 
+int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant) {
+    if (!s) return fail(L3D_EINVAL, "NULL handle");
+    if (s->opts.form != L3D_FORM_FAST) return fail(L3D_ESTATE, "variants select fast-form kernels");
+    const int rows = variant & 7, rest = variant & ~15;
+    if (rest || !(rows == 6 || rows == 4 || rows == 3 || rows == 2))
+        return fail(L3D_EINVAL, "variant %d: texture rows must be 6, 4, 3 or 2 (+8 for quads)", variant);
+    s->variant = variant;
+    return L3D_OK;
+}
+
+int32_t l3d_stereo_variant(const l3d_stereo* s) { return s ? s->variant : -1; }
+
 void l3d_stereo_destroy(l3d_stereo* s) {
     if (!s) return;
     if (s->stream) cudaStreamSynchronize(s->stream);
@@ -874,6 +907,7 @@ void l3d_stereo_destroy(l3d_stereo* s) {
         if (t) cudaDestroyTextureObject(t);
     for (cudaArray_t a : s->arrays)
         if (a) cudaFreeArray(a);
+    cudaFree(s->pairs);
     cudaFree(s->fviews_dev);
     cudaFree(s->tile_start_dev);
     cudaFreeHost(s->fviews_host);
@@ -908,6 +942,7 @@ struct l3d_tsdf {
     int map_cap = 0;
     float* priors = nullptr;          /* uploaded priors, prior_cap * P */
     int prior_cap = 0;
+    float4* normals = nullptr;        /* decoded normal per 12-bit normal code */
     L3dTsdfView* views_host = nullptr;      /* pinned staging for views */
     const uint32_t** ptrs_host = nullptr;   /* pinned staging for depth pointers */
     long long launches = 0;
@@ -1086,6 +1121,11 @@ int l3d_tsdf_create(const l3d_tsdf_desc* d, l3d_tsdf** out) {
         if ((e = cudaStreamSynchronize(t->stream)) != cudaSuccess)
             return cleanup(cuda_fail(e, "coords upload"));
     }
+    if ((e = cudaMalloc(&t->normals, 4096 * sizeof(float4))) != cudaSuccess)
+        return cleanup(cuda_fail(e, "normal table allocation"));
+    if ((e = l3d_launch_normal_table(t->normals, t->stream)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "normal table"));
+    t->launches++;
     int rc = l3d_tsdf_reset(t);
     if (rc) return cleanup(rc);
     *out = t;
@@ -1181,8 +1221,8 @@ int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* l
     cudaError_t e = l3d_launch_tsdf_visible(t->g, t->views, n, t->coords, t->mask, t->stream);
     t->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "visibility launch");
-    e = l3d_launch_tsdf_many(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors, t->tsdf,
-                             t->weight, t->q8, t->stream);
+    e = l3d_launch_tsdf_many(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
+                             t->normals, t->tsdf, t->weight, t->q8, t->stream);
     t->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
     if (src && (rc = before_stereo(t, src))) return rc;
@@ -1232,6 +1272,7 @@ void l3d_tsdf_destroy(l3d_tsdf* t) {
     cudaFree(t->depth_ptrs);
     cudaFree(t->maps);
     cudaFree(t->priors);
+    cudaFree(t->normals);
     cudaFreeHost(t->views_host);
     cudaFreeHost(t->ptrs_host);
     if (t->done) cudaEventDestroy(t->done);

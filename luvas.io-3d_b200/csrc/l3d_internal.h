@@ -131,6 +131,7 @@ struct L3dFastDev {
     int n_views;
     int total_tiles;
     const void* images;        /* linear storage (BF16 sampling path) */
+    const uint32_t* pairs;     /* pair image (half2 of a texel and its right neighbour) or NULL */
     int storage;               /* L3D_DTYPE_F32/F16 (texture path) or BF16 (loads) */
     float4* hyp;               /* hyp_all */
     float* cost;               /* cost_all */
@@ -139,13 +140,18 @@ struct L3dFastDev {
 };
 
 /* kernel: L3D_K_INIT or L3D_K_PROPAGATE; iteration/phase select the RNG stream and the
- * refinement step; views with fewer iterations than `iteration + 1` are skipped. */
+ * refinement step; views with fewer iterations than `iteration + 1` are skipped.  variant:
+ * window rows sampled by the texture unit (0..6, the rest from the pair image) + 8 for the 2x2
+ * quad lane mapping. */
 cudaError_t l3d_launch_fast(int kernel, const L3dFastDev& d, int iteration, int phase,
-                            int lanes, cudaStream_t stream);
+                            int variant, cudaStream_t stream);
+/* pair image of one layer: half2(texel, right neighbour) from the linear storage */
+cudaError_t l3d_launch_make_pairs(const void* img, int storage, int W, int H, uint32_t* pairs,
+                                  cudaStream_t stream);
 /* pack of every view with pack != 0; max_pixels bounds the views' width * height */
 cudaError_t l3d_launch_fast_pack(const L3dFastDev& d, long long max_pixels, cudaStream_t stream);
 cudaError_t l3d_launch_fast_plane_cost(const L3dFastDev& d, const float4* planes, float* cost,
-                                       cudaStream_t stream);
+                                       int variant, cudaStream_t stream);
 cudaError_t l3d_launch_plane_cost(const L3dParams& p, const L3dStereoDev& d, const float4* planes,
                                   float* cost, float* view_costs, int win, int dil,
                                   cudaStream_t stream);
@@ -158,10 +164,13 @@ cudaError_t l3d_launch_tsdf_visible(const L3dTsdfGrid& g, const L3dTsdfView* vie
 cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,
                                  uint8_t* mask, const uint32_t* depth, const float* prior,
                                  float* tsdf, void* weight, int q8, cudaStream_t stream);
+/* normals[code] = unpack_normal(code << 16) for the 4096 normal codes */
+cudaError_t l3d_launch_normal_table(float4* normals, cudaStream_t stream);
 cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
                                  const int32_t* coords, const uint8_t* mask,
                                  const uint32_t* const* depth_ptrs_dev, const float* priors,
-                                 float* tsdf, void* weight, int q8, cudaStream_t stream);
+                                 const float4* normals, float* tsdf, void* weight, int q8,
+                                 cudaStream_t stream);
 cudaError_t l3d_launch_tsdf_fill(float* tsdf, void* weight, long long voxels, int q8,
                                  cudaStream_t stream);
 

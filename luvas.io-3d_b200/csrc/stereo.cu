@@ -587,7 +587,10 @@ __global__ void k_convert(const uint8_t* src, int dtype, long long stride, int W
         default: v = l3d_u2f((uint32_t)((const uint16_t*)row)[x] << 16); break; /* bf16 */
     }
     long long o = (long long)y * W + x;
-    if (storage == 1) {
+    if (storage == 0) {
+        /* r8unorm: round to the nearest of 256 levels */
+        ((uint8_t*)dst)[o] = (uint8_t)rintf(fminf(fmaxf(v, 0.0f), 1.0f) * 255.0f);
+    } else if (storage == 1) {
         ((float*)dst)[o] = v;
     } else if (storage == 2) {
         ((uint16_t*)dst)[o] = (uint16_t)l3d_f32_to_f16(v);

@@ -23,6 +23,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cuda_fp16.h>
+
 #include "l3d_fmath.h"
 #include "l3d_internal.h"
 
@@ -115,6 +117,26 @@ struct Img {
     }
 };
 
+/* Software bilinear sample from the pair image (each texel stores itself and its right
+ * neighbour as half2), at filtering coordinate (u, v): two 32-bit loads on the LSU path, FP32
+ * weights.  Used for the window rows the texture unit does not take. */
+__device__ __forceinline__ float pair_sample(const uint32_t* __restrict__ pairs, int W, int H,
+                                             float u, float v) {
+    float x = u - 0.5f, y = v - 0.5f;
+    int x0 = __float2int_rd(x), y0 = __float2int_rd(y);
+    float fx = x - (float)x0, fy = y - (float)y0;
+    x0 = min(max(x0, 0), W - 1);
+    y0 = min(max(y0, 0), H - 1);
+    int y1 = min(y0 + 1, H - 1);
+    uint32_t t = __ldg(pairs + (long long)y0 * W + x0);
+    uint32_t b = __ldg(pairs + (long long)y1 * W + x0);
+    float2 tf = __half22float2(*reinterpret_cast<const __half2*>(&t));
+    float2 bf = __half22float2(*reinterpret_cast<const __half2*>(&b));
+    float top = fmaf(fx, tf.y - tf.x, tf.x);
+    float bot = fmaf(fx, bf.y - bf.x, bf.x);
+    return fmaf(fy, bot - top, top);
+}
+
 /* Per-pixel state: the reference window as w and w (r - c), c = centre pixel. */
 struct FPix {
     float rw[S], rwr[S];
@@ -124,7 +146,9 @@ struct FPix {
     float3 ray;
 };
 
-template <bool TEX>
+/* TEX: texture-unit sampling of F16/F32 arrays (false: BF16 linear memory).  TEXROWS: window
+ * rows (of 6) sampled by the texture unit; the other rows use pair_sample (TEX only). */
+template <bool TEX, int TEXROWS = 6>
 struct Fast {
     const L3dFastView& v;
     const L3dFastDev& d;
@@ -194,9 +218,13 @@ struct Fast {
         if (!ok) return 2.0f;
         const uint16_t* si = img(src.img_off);
         float ss = 0.0f, sss = 0.0f, srs = 0.0f;
+        /* rows [0, TEXROWS) through the texture unit, rows [TEXROWS, 6) through pair_sample: two
+         * loops with constant bounds, so each unrolls into straight-line code with all its
+         * fetches in flight together */
+        constexpr int RT = TEX ? TEXROWS : 6;
         float rx = qx0, ry = qy0, rz = qz0;
 #pragma unroll
-        for (int r = 0; r < 6; r++) {
+        for (int r = 0; r < RT; r++) {
             float qx = rx, qy = ry, qz = rz;
 #pragma unroll
             for (int c = 0; c < 6; c++) {
@@ -215,6 +243,30 @@ struct Fast {
             rx += dyx;
             ry += dyy;
             rz += dyz;
+        }
+        if constexpr (TEX && TEXROWS < 6) {
+            const uint32_t* sp = d.pairs + src.img_off;
+#pragma unroll
+            for (int r = TEXROWS; r < 6; r++) {
+                float qx = rx, qy = ry, qz = rz;
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    const int i = r * 6 + c;
+                    float iz = rcp_fast(qz);
+                    float val = pair_sample(sp, src.W, src.H, qx * iz, qy * iz);
+                    float sv = val - s.center;
+                    float t = s.rw[i] * sv;
+                    ss += t;
+                    sss = fmaf(t, sv, sss);
+                    srs = fmaf(s.rwr[i], sv, srs);
+                    qx += dxx;
+                    qy += dxy;
+                    qz += dxz;
+                }
+                rx += dyx;
+                ry += dyy;
+                rz += dyz;
+            }
         }
         float mean = ss * s.inv_sum;
         float var_s = fmaxf(fmaf(-mean, mean, sss * s.inv_sum), 0.0f);
@@ -364,14 +416,14 @@ __device__ __forceinline__ void orient(int ox, int oy, int dir, int* rx, int* ry
     }
 }
 
-template <bool TEX>
+template <bool TEX, int TEXROWS>
 __global__ void __launch_bounds__(128) k_fast_init(const L3dFastDev d) {
     __shared__ __align__(16) L3dFastView sv;
     load_view(sv, d.views + find_view(d, blockIdx.x));
     const int local = blockIdx.x - sv.tile_start;
     const int y = (local / sv.tiles_x) * TY + threadIdx.x / TX;
     /* init covers every pixel: a tile spans 32 image columns, two pixels per thread */
-    Fast<TEX> f(sv, d);
+    Fast<TEX, TEXROWS> f(sv, d);
     for (int half = 0; half < 2; half++) {
         const int xx = (local % sv.tiles_x) * (2 * TX) + (threadIdx.x % TX) * 2 + half;
         if (xx >= sv.W || y >= sv.H) continue;
@@ -406,17 +458,28 @@ __global__ void __launch_bounds__(128) k_fast_init(const L3dFastDev d) {
     }
 }
 
-template <bool TEX>
-__global__ void __launch_bounds__(128) k_fast_propagate(const L3dFastDev d, int iteration,
+/* QUAD: the four lanes of each hardware quad take a 2 x 2 block of this colour's pixels (tighter
+ * texture footprints per quad request); otherwise four consecutive pixels of one row. */
+template <bool TEX, int TEXROWS, bool QUAD>
+__global__ void __launch_bounds__(128, 3) k_fast_propagate(const L3dFastDev d, int iteration,
                                                         int phase, float step) {
     __shared__ __align__(16) L3dFastView sv;
     load_view(sv, d.views + find_view(d, blockIdx.x));
     if (iteration >= sv.iterations) return;
     const int local = blockIdx.x - sv.tile_start;
-    const int y = (local / sv.tiles_x) * TY + threadIdx.x / TX;
-    const int x = ((local % sv.tiles_x) * TX + threadIdx.x % TX) * 2 + ((y + phase) & 1);
+    int tx, ty;
+    if (QUAD) {
+        const int q = threadIdx.x >> 2, j = threadIdx.x & 3;
+        tx = (q % (TX / 2)) * 2 + (j & 1);
+        ty = (q / (TX / 2)) * 2 + (j >> 1);
+    } else {
+        tx = threadIdx.x % TX;
+        ty = threadIdx.x / TX;
+    }
+    const int y = (local / sv.tiles_x) * TY + ty;
+    const int x = ((local % sv.tiles_x) * TX + tx) * 2 + ((y + phase) & 1);
     if (x >= sv.W || y >= sv.H) return;
-    Fast<TEX> f(sv, d);
+    Fast<TEX, TEXROWS> f(sv, d);
     FPix s;
     f.begin(s, x, y, iteration, phase);
     const int W = sv.W, H = sv.H;
@@ -495,14 +558,14 @@ __global__ void k_fast_pack(const L3dFastDev d) {
     d.depths[__ldg(&v->ref_dep_off) + i] = pack_sample(h.w, make_float3(h.x, h.y, h.z), d.cost[base + i]);
 }
 
-template <bool TEX>
+template <bool TEX, int TEXROWS>
 __global__ void __launch_bounds__(128) k_fast_plane_cost(const L3dFastDev d, const float4* planes,
                                                          float* cost) {
     __shared__ __align__(16) L3dFastView sv;
     load_view(sv, d.views + find_view(d, blockIdx.x));
     const int local = blockIdx.x - sv.tile_start;
     const int y = (local / sv.tiles_x) * TY + threadIdx.x / TX;
-    Fast<TEX> f(sv, d);
+    Fast<TEX, TEXROWS> f(sv, d);
     for (int half = 0; half < 2; half++) {
         const int x = (local % sv.tiles_x) * (2 * TX) + (threadIdx.x % TX) * 2 + half;
         if (x >= sv.W || y >= sv.H) continue;
@@ -516,22 +579,79 @@ __global__ void __launch_bounds__(128) k_fast_plane_cost(const L3dFastDev d, con
 
 }  // namespace
 
-cudaError_t l3d_launch_fast(int kernel, const L3dFastDev& d, int iteration, int phase, int lanes,
-                            cudaStream_t stream) {
-    (void)lanes;
-    const bool tex = d.storage != 3; /* BF16 is sampled from linear memory */
-    if (d.total_tiles <= 0) return cudaSuccess;
+namespace {
+
+template <int TEXROWS, bool QUAD>
+cudaError_t launch_tex(int kernel, const L3dFastDev& d, int iteration, int phase, cudaStream_t st) {
     if (kernel == L3D_K_INIT) {
-        if (tex) k_fast_init<true><<<d.total_tiles, 128, 0, stream>>>(d);
-        else k_fast_init<false><<<d.total_tiles, 128, 0, stream>>>(d);
-    } else if (kernel == L3D_K_PROPAGATE) {
-        float step = ldexpf(1.0f, -iteration);
-        if (tex) k_fast_propagate<true><<<d.total_tiles, 128, 0, stream>>>(d, iteration, phase, step);
-        else k_fast_propagate<false><<<d.total_tiles, 128, 0, stream>>>(d, iteration, phase, step);
+        k_fast_init<true, TEXROWS><<<d.total_tiles, 128, 0, st>>>(d);
     } else {
-        return cudaErrorInvalidValue;
+        float step = ldexpf(1.0f, -iteration);
+        k_fast_propagate<true, TEXROWS, QUAD><<<d.total_tiles, 128, 0, st>>>(d, iteration, phase, step);
     }
     return cudaGetLastError();
+}
+
+__global__ void k_make_pairs(const void* img, int storage, int W, int H, uint32_t* pairs) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W) return;
+    const long long row = (long long)y * W;
+    const int x1 = min(x + 1, W - 1);
+    float a, b;
+    if (storage == 0) {
+        a = (float)((const uint8_t*)img)[row + x] / 255.0f;
+        b = (float)((const uint8_t*)img)[row + x1] / 255.0f;
+    } else if (storage == 1) {
+        a = ((const float*)img)[row + x];
+        b = ((const float*)img)[row + x1];
+    } else if (storage == 2) {
+        a = l3d_f16_to_f32(((const uint16_t*)img)[row + x]);
+        b = l3d_f16_to_f32(((const uint16_t*)img)[row + x1]);
+    } else {
+        a = __uint_as_float((uint32_t)((const uint16_t*)img)[row + x] << 16);
+        b = __uint_as_float((uint32_t)((const uint16_t*)img)[row + x1] << 16);
+    }
+    pairs[row + x] = l3d_f32_to_f16(a) | (l3d_f32_to_f16(b) << 16);
+}
+
+}  // namespace
+
+cudaError_t l3d_launch_make_pairs(const void* img, int storage, int W, int H, uint32_t* pairs,
+                                  cudaStream_t stream) {
+    dim3 grid((W + 127) / 128, H);
+    k_make_pairs<<<grid, 128, 0, stream>>>(img, storage, W, H, pairs);
+    return cudaGetLastError();
+}
+
+/* variant = texture rows (0..6) + 8 x quad mapping. */
+cudaError_t l3d_launch_fast(int kernel, const L3dFastDev& d, int iteration, int phase, int variant,
+                            cudaStream_t stream) {
+    if (d.total_tiles <= 0) return cudaSuccess;
+    if (kernel != L3D_K_INIT && kernel != L3D_K_PROPAGATE) return cudaErrorInvalidValue;
+    if (d.storage == 3) { /* BF16 is sampled from linear memory */
+        if (kernel == L3D_K_INIT) {
+            k_fast_init<false, 6><<<d.total_tiles, 128, 0, stream>>>(d);
+        } else {
+            float step = ldexpf(1.0f, -iteration);
+            k_fast_propagate<false, 6, false><<<d.total_tiles, 128, 0, stream>>>(d, iteration, phase, step);
+        }
+        return cudaGetLastError();
+    }
+    const int rows = variant & 7;
+    const bool quad = (variant & 8) != 0;
+    if (!d.pairs && rows < 6) return cudaErrorInvalidValue;
+    switch (rows + (quad ? 8 : 0)) {
+        case 6: return launch_tex<6, false>(kernel, d, iteration, phase, stream);
+        case 4: return launch_tex<4, false>(kernel, d, iteration, phase, stream);
+        case 3: return launch_tex<3, false>(kernel, d, iteration, phase, stream);
+        case 2: return launch_tex<2, false>(kernel, d, iteration, phase, stream);
+        case 14: return launch_tex<6, true>(kernel, d, iteration, phase, stream);
+        case 12: return launch_tex<4, true>(kernel, d, iteration, phase, stream);
+        case 11: return launch_tex<3, true>(kernel, d, iteration, phase, stream);
+        case 10: return launch_tex<2, true>(kernel, d, iteration, phase, stream);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t l3d_launch_fast_pack(const L3dFastDev& d, long long max_pixels, cudaStream_t stream) {
@@ -542,9 +662,13 @@ cudaError_t l3d_launch_fast_pack(const L3dFastDev& d, long long max_pixels, cuda
 }
 
 cudaError_t l3d_launch_fast_plane_cost(const L3dFastDev& d, const float4* planes, float* cost,
-                                       cudaStream_t stream) {
+                                       int variant, cudaStream_t stream) {
     if (d.total_tiles <= 0) return cudaSuccess;
-    if (d.storage != 3) k_fast_plane_cost<true><<<d.total_tiles, 128, 0, stream>>>(d, planes, cost);
-    else k_fast_plane_cost<false><<<d.total_tiles, 128, 0, stream>>>(d, planes, cost);
+    const int rows = variant & 7;
+    if (d.storage == 3) k_fast_plane_cost<false, 6><<<d.total_tiles, 128, 0, stream>>>(d, planes, cost);
+    else if (rows == 6 || !d.pairs) k_fast_plane_cost<true, 6><<<d.total_tiles, 128, 0, stream>>>(d, planes, cost);
+    else if (rows == 4) k_fast_plane_cost<true, 4><<<d.total_tiles, 128, 0, stream>>>(d, planes, cost);
+    else if (rows == 3) k_fast_plane_cost<true, 3><<<d.total_tiles, 128, 0, stream>>>(d, planes, cost);
+    else k_fast_plane_cost<true, 2><<<d.total_tiles, 128, 0, stream>>>(d, planes, cost);
     return cudaGetLastError();
 }

@@ -97,6 +97,60 @@ __device__ __forceinline__ bool observe(const L3dTsdfGrid& g, const L3dTsdfView&
     return true;
 }
 
+/* observe() with the same results, reordered for the many-view sweep: the depth and the
+ * truncation test come first (most voxels of a view lie behind the surface or outside the
+ * truncation band), and the decoded normal comes from `normals`, a table of unpack_normal over
+ * all 4096 normal codes computed with the same arithmetic. */
+__device__ __forceinline__ bool observe_lut(const L3dTsdfGrid& g, const L3dTsdfView& v,
+                                            const uint32_t* __restrict__ depth,
+                                            const float* __restrict__ prior,
+                                            const float4* __restrict__ normals, int gx, int gy,
+                                            int gz, float* obs, float* wout) {
+    float wx = fmaf((float)gx + 0.5f, g.voxel, g.origin[0]);
+    float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
+    float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
+    const float* R = v.R;
+    float3 cam = make_float3(fmaf(R[2], wz, fmaf(R[1], wy, fmaf(R[0], wx, v.t[0]))),
+                             fmaf(R[5], wz, fmaf(R[4], wy, fmaf(R[3], wx, v.t[1]))),
+                             fmaf(R[8], wz, fmaf(R[7], wy, fmaf(R[6], wx, v.t[2]))));
+    if (!(cam.z > 0.01f)) return false;
+    float iz = 1.0f / cam.z;
+    float rx = rintf(fmaf(v.k[0] * cam.x, iz, v.k[2]));
+    float ry = rintf(fmaf(v.k[1] * cam.y, iz, v.k[3]));
+    if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)g.W && ry < (float)g.H)) return false;
+    long long i = (long long)(int)ry * g.W + (int)rx;
+    uint32_t packed = __ldg(depth + i);
+    float d = l3d_f16_to_f32(packed & 0xffffu);
+    const bool stereo = d > 0.0f;
+    if (!stereo) d = prior ? __ldg(prior + i) : 0.0f;
+    if (!(d > 0.0f)) return false;
+    float sdf = d - cam.z;
+    if (sdf < -g.mu) return false;
+    float w;
+    if (stereo) {
+        float4 n4 = __ldg(normals + ((packed >> 16) & 4095u));
+        float3 cn = normalize3f(cam);
+        w = maxw(0.2f, fabsf(dot3f(make_float3(n4.x, n4.y, n4.z), cn)));
+        if (v.conf > 0.0f) {
+            float c = (float)(packed >> 28) / 8.0f;
+            float r = clampw(v.conf / d, 0.5f, 2.0f);
+            w = w * ((maxw(0.15f, (1.0f - c) * (1.0f - c)) * r) * r);
+        }
+    } else {
+        w = g.prior_weight;
+    }
+    *obs = minw(1.0f, sdf / g.mu);
+    *wout = w;
+    return true;
+}
+
+__global__ void k_normal_table(float4* normals) {
+    const uint32_t code = blockIdx.x * blockDim.x + threadIdx.x;
+    if (code >= 4096u) return;
+    float3 n = unpack_normal(code << 16);
+    normals[code] = make_float4(n.x, n.y, n.z, 0.0f);
+}
+
 __device__ __forceinline__ void apply_f32(float& t, float& w0, float obs, float w, float maxw_) {
     t = fmaf(t, w0, obs * w) / (w0 + w);
     w0 = minw(w0 + w, maxw_);
@@ -252,6 +306,7 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
                                                         const uint8_t* __restrict__ mask,
                                                         const uint32_t* const* __restrict__ depths,
                                                         const float* __restrict__ priors,
+                                                        const float4* __restrict__ normals,
                                                         float* __restrict__ tsdf,
                                                         void* __restrict__ weight, long long quads) {
     long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -272,7 +327,7 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
 #pragma unroll
         for (int j = 0; j < VEC; j++) {
             float obs, w;
-            if (!observe(g, v, depth, prior, gx + j, gy, gz, &obs, &w)) continue;
+            if (!observe_lut(g, v, depth, prior, normals, gx + j, gy, gz, &obs, &w)) continue;
             if (!loaded) {
                 loaded = true;
 #pragma unroll
@@ -345,20 +400,26 @@ cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, con
     return cudaGetLastError();
 }
 
+cudaError_t l3d_launch_normal_table(float4* normals, cudaStream_t stream) {
+    k_normal_table<<<16, 256, 0, stream>>>(normals);
+    return cudaGetLastError();
+}
+
 cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
                                  const int32_t* coords, const uint8_t* mask,
                                  const uint32_t* const* depth_ptrs_dev, const float* priors,
-                                 float* tsdf, void* weight, int q8, cudaStream_t stream) {
+                                 const float4* normals, float* tsdf, void* weight, int q8,
+                                 cudaStream_t stream) {
     const int vec = vec4_ok(g) ? 4 : 1;
     long long quads = quad_count(g, vec);
     if (quads == 0 || n_views == 0) return cudaSuccess;
     unsigned blocks = (unsigned)((quads + 255) / 256);
     if (vec == 4) {
-        if (q8) k_integrate_many<4, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, tsdf, weight, quads);
-        else k_integrate_many<4, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, tsdf, weight, quads);
+        if (q8) k_integrate_many<4, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
+        else k_integrate_many<4, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
     } else {
-        if (q8) k_integrate_many<1, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, tsdf, weight, quads);
-        else k_integrate_many<1, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, tsdf, weight, quads);
+        if (q8) k_integrate_many<1, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
+        else k_integrate_many<1, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
     }
     return cudaGetLastError();
 }

@@ -133,6 +133,8 @@ SIGNATURES = [
     ("l3d_stereo_stream", C.c_int, [_P, C.POINTER(_P)]),
     ("l3d_stereo_synchronize", C.c_int, [_P]),
     ("l3d_stereo_launches", C.c_int64, [_P]),
+    ("l3d_stereo_set_variant", C.c_int, [_P, _I]),
+    ("l3d_stereo_variant", C.c_int32, [_P]),
     ("l3d_stereo_destroy", None, [_P]),
     ("l3d_tsdf_create", C.c_int, [C.POINTER(TsdfDesc), C.POINTER(_P)]),
     ("l3d_tsdf_integrate", C.c_int, [_P, _P, _P, C.POINTER(IntegrationView)]),

@@ -252,6 +252,15 @@ class DenseStereo:
     def launches(self) -> int:
         return int(self._lib.l3d_stereo_launches(self._h()))
 
+    @property
+    def variant(self) -> int:
+        """Fast-form kernel variant: texture-sampled window rows + 8 x quad lane mapping."""
+        return int(self._lib.l3d_stereo_variant(self._h()))
+
+    @variant.setter
+    def variant(self, v: int) -> None:
+        _lib.check(self._lib.l3d_stereo_set_variant(self._h(), int(v)))
+
     def synchronize(self) -> None:
         _lib.check(self._lib.l3d_stereo_synchronize(self._h()))
 

@@ -10,7 +10,7 @@ import pytest
 
 import oracle
 from helpers import arc_workload, assert_bit_equal
-from luvas3d import (DTYPE_BF16, DTYPE_F16, DTYPE_F32, FORM_FAST, FORM_PLAIN, DenseStereo,
+from luvas3d import (DTYPE_BF16, DTYPE_F16, DTYPE_F32, DTYPE_U8, FORM_FAST, FORM_PLAIN, DenseStereo,
                      L3dError, SolveOptions, StereoOptions, packing)
 
 pytestmark = pytest.mark.gpu
@@ -28,7 +28,7 @@ def make(views, imgs, W, H, form=FORM_FAST, storage=DTYPE_F16):
     return s
 
 
-@pytest.mark.parametrize("storage", [DTYPE_F16, DTYPE_BF16, DTYPE_F32])
+@pytest.mark.parametrize("storage", [DTYPE_F16, DTYPE_BF16, DTYPE_F32, DTYPE_U8])
 def test_fixed_plane_cost_close_to_fp64(arc, storage):
     views, imgs, truth, srcs = arc
     W, H = 256, 192
@@ -47,7 +47,8 @@ def test_fixed_plane_cost_close_to_fp64(arc, storage):
     p99 = np.percentile(err, 99)
     print(f"storage {storage}: cost error vs FP64 max {err.max():.2e} p99 {p99:.2e} "
           f"median {np.median(err):.2e}")
-    tol = {DTYPE_F32: 2e-3, DTYPE_F16: 5e-3, DTYPE_BF16: 2e-2}[storage]
+    # U8 (the reference's r8unorm textures) is limited by the 1/255 quantization of the inputs
+    tol = {DTYPE_F32: 2e-3, DTYPE_F16: 5e-3, DTYPE_BF16: 2e-2, DTYPE_U8: 1.5e-2}[storage]
     assert p99 < tol
 
 
@@ -57,7 +58,7 @@ def depth_stats(hyp, truth):
     return np.median(rel[m]), (rel[m] < 0.01).mean()
 
 
-@pytest.mark.parametrize("storage", [DTYPE_F16, DTYPE_BF16])
+@pytest.mark.parametrize("storage", [DTYPE_F16, DTYPE_BF16, DTYPE_U8])
 def test_fast_depth_accuracy_matches_plain(arc, storage):
     views, imgs, truth, srcs = arc
     W, H = 256, 192
@@ -75,6 +76,45 @@ def test_fast_depth_accuracy_matches_plain(arc, storage):
     vp = (plain.depth_map(2) != 0).mean()
     vf = (fast.depth_map(2) != 0).mean()
     assert abs(vp - vf) < 0.05
+
+
+@pytest.mark.parametrize("variant", [6, 14, 4, 12, 3, 11, 2, 10])
+def test_every_variant_keeps_accuracy(arc, variant):
+    """Kernel variants split the window rows between the texture unit and software bilinear on
+    the LSU path, and map hardware quads to rows or 2x2 blocks; accuracy must not change."""
+    views, imgs, truth, srcs = arc
+    W, H = 256, 192
+    plain = make(views, imgs, W, H, form=FORM_PLAIN, storage=DTYPE_F32)
+    fast = make(views, imgs, W, H)
+    fast.variant = variant
+    assert fast.variant == variant
+    opts = SolveOptions(srcs[2], 0.5, 5.0, iterations=5)
+    plain.solve(2, opts)
+    fast.solve(2, opts)
+    pm, pf = depth_stats(plain.read_hypotheses()[0], truth[2])
+    fm, ff = depth_stats(fast.read_hypotheses()[0], truth[2])
+    print(f"variant {variant}: fast median {fm:.2e} within1% {ff:.3f} (plain {pm:.2e} {pf:.3f})")
+    assert fm < max(1.25 * pm, pm + 3e-4)
+    assert ff > pf - 0.03
+    planes = np.zeros((H, W, 4), dtype=np.float32)
+    planes[..., 2] = -1.0
+    planes[..., 3] = np.where(truth[2] > 0, truth[2], 1.0)
+    o = oracle.Stereo(W, H, views, imgs, 64)
+    want, _ = o.plane_cost(2, srcs[2], planes.astype(np.float64), min_depth=0.5, max_depth=5.0)
+    got = fast.plane_cost(2, SolveOptions(srcs[2], 0.5, 5.0), planes)
+    valid = (want < 1.5) & (got < 1.5)
+    assert np.percentile(np.abs(got[valid] - want[valid]), 99) < 5e-3
+
+
+def test_variant_validation(arc):
+    views, imgs, truth, srcs = arc
+    fast = make(views, imgs, 256, 192)
+    for bad in (5, 1, 7, 16, -1):
+        with pytest.raises(L3dError):
+            fast.variant = bad
+    plain = make(views, imgs, 256, 192, form=FORM_PLAIN, storage=DTYPE_F32)
+    with pytest.raises(L3dError):
+        plain.variant = 6
 
 
 def test_batch_equals_single_views(arc):
