@@ -102,8 +102,19 @@ class ClockSampler:
 def build_workload(args):
     from luvas3d import scenes
 
-    return scenes.scan(n_views=args.views, width=args.width, height=args.height,
-                       tsdf_dim=args.tsdf_dim)
+    if args.workload == "room":
+        return scenes.room(n_views=args.views or 96, tsdf_dim=args.tsdf_dim or 768)
+    return scenes.scan(n_views=args.views or 48, width=args.width, height=args.height,
+                       tsdf_dim=args.tsdf_dim or 512)
+
+
+def workload_name(w) -> str:
+    if w.name == "room":
+        return (f"room: {len(w.views)} views of mixed sizes (480x360..1280x960), 20 cuboids, "
+                f"8 sources, 5 iterations, TSDF {w.tsdf_dims[0]}^3 at {w.tsdf_voxel * 1000:.0f} mm")
+    return (f"scan: {len(w.views)} views {w.width}x{w.height}, 8 sources, 5 iterations, window "
+            f"11x11 dilated by 2, TSDF {w.tsdf_dims[0]}^3 at {w.tsdf_voxel * 1000:.0f} mm, "
+            f"trunc {w.tsdf_truncation * 100:.0f} cm, Q8.8 weights")
 
 
 def cpu_baseline(w, threads: int, budget_s: float = 20.0) -> dict:
@@ -113,6 +124,7 @@ def cpu_baseline(w, threads: int, budget_s: float = 20.0) -> dict:
     import oracle
 
     o = oracle.Stereo(w.width, w.height, w.views, w.images, 32, threads=threads)
+    h0, w0 = w.images[0].shape
     t0 = time.perf_counter()
     o.kernel(oracle.INIT, 0, w.sources[0], min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
     t_init = time.perf_counter() - t0
@@ -121,12 +133,12 @@ def cpu_baseline(w, threads: int, budget_s: float = 20.0) -> dict:
         o.kernel(oracle.PROPAGATE, 0, w.sources[0], iteration=0, phase=phase,
                  min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
     t_prop = time.perf_counter() - t0
-    pm = w.pixels / (t_init / 2 + t_prop) if False else w.pixels / t_prop
+    pm = w.images[0].size / t_prop
     # TSDF: one view into the full volume
     o.kernel(oracle.PACK, 0, w.sources[0], min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
     v = w.views[0]
     k = v.intrinsics
-    ot = oracle.Tsdf(w.width, w.height, w.tsdf_voxel, w.tsdf_origin, w.tsdf_truncation,
+    ot = oracle.Tsdf(w0, h0, w.tsdf_voxel, w.tsdf_origin, w.tsdf_truncation,
                      dense=w.tsdf_dims, weight_q8=True, threads=threads)
     t0 = time.perf_counter()
     ot.integrate(dict(k=(k.fx, k.fy, k.cx, k.cy), R=v.pose.R, t=v.pose.t,
@@ -135,7 +147,7 @@ def cpu_baseline(w, threads: int, budget_s: float = 20.0) -> dict:
     vox = int(np.prod(w.tsdf_dims))
     return {"value": pm, "unit": "px-iters/s", "cores": threads, "kind": "port",
             "sample": (f"FP32 oracle: 1 reference view x 1 red/black iteration at "
-                       f"{w.width}x{w.height}, {len(w.sources[0])} sources "
+                       f"{w0}x{h0}, {len(w.sources[0])} sources "
                        f"({t_prop:.2f} s); TSDF 1 view into {w.tsdf_dims[0]}^3 ({t_tsdf:.2f} s)"),
             "tsdf_voxel_updates_per_s": vox / t_tsdf, "seconds": t_prop + t_tsdf}
 
@@ -157,10 +169,9 @@ def run_reference(args, rank: int, world: int) -> None:
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "px-iters/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * w.pixels / v, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "scan: 48 views 640x480, 8 sources, 5 iterations, TSDF 512^3",
-                   "sample": r["sample"]},
+        "ms_per_step": 1e3 * w.pixels * w.iterations / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(w), "sample": r["sample"]},
         "tsdf_voxel_updates_per_s": statistics.median(tv),
         "cpu_baseline": {"value": v, "unit": "px-iters/s", "cores": threads, "kind": "port",
                          "sample": r["sample"]},
@@ -176,10 +187,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="auto", choices=["auto", "plain", "fast"])
-    ap.add_argument("--views", type=int, default=48)
+    ap.add_argument("--workload", default="scan", choices=["scan", "room"])
+    ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--width", type=int, default=640)
     ap.add_argument("--height", type=int, default=480)
-    ap.add_argument("--tsdf-dim", type=int, default=512)
+    ap.add_argument("--tsdf-dim", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -203,7 +215,8 @@ def main():
                          IntegrationView, SolveOptions, StereoOptions, TsdfVolume)
 
     w = build_workload(args)
-    V, P = len(w.views), w.pixels
+    V = len(w.views)
+    sizes = w.sizes or [(w.width, w.height)] * V
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
     refs = list(range(V))
@@ -212,8 +225,9 @@ def main():
     iviews = [IntegrationView(v.intrinsics, v.pose, w.ranges[i][1]) for i, v in enumerate(w.views)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     vox = int(np.prod(w.tsdf_dims))
-    px_iters_step = V * P * w.iterations
-    tsdf = TsdfVolume(w.width, w.height, w.tsdf_voxel, w.tsdf_origin, dense=w.tsdf_dims,
+    px_iters_step = w.pixels * w.iterations
+    tsdf = TsdfVolume(max(s[0] for s in sizes), max(s[1] for s in sizes), w.tsdf_voxel,
+                      w.tsdf_origin, dense=w.tsdf_dims,
                       truncation=w.tsdf_truncation, weight_q8=True, stream=sptr)
     mk = lambda n=4: [torch.cuda.Event(enable_timing=True) for _ in range(n)]
 
@@ -221,12 +235,18 @@ def main():
         with torch.cuda.stream(stream):
             ev.record(stream)
 
+    tuned = {}
+
     def make_stereo(form):
         storage = DTYPE_F16 if form == FORM_FAST else DTYPE_F32
         st = DenseStereo(w.width, w.height, w.views,
-                         StereoOptions(storage=storage, form=form, stream=sptr))
+                         StereoOptions(storage=storage, form=form, stream=sptr), sizes=sizes)
         for i, im in enumerate(w.images):
             st.set_image(i, im)
+        if form == FORM_FAST:
+            # kernel variant picked by timing one iteration of this batch, then graph replay
+            tuned["variant"], tuned["ms"] = st.autotune(refs, opts)
+            st.set_graphs(True)
         return st
 
     def step(st, evs):
@@ -311,7 +331,7 @@ def main():
     S = len(w.sources[0])
     flop_per_px_phase = 14 * S * (18 + 36 * 37 + 15) + 36 * 26
     views_per_launch = V if chosen_form == FORM_FAST else 1
-    prop_flops = flop_per_px_phase * (P / 2) * views_per_launch
+    prop_flops = flop_per_px_phase * (w.pixels / V / 2) * views_per_launch
     achieved = prop_flops / (R["prop_ms"] / 1e3) / 1e12
     sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
@@ -326,7 +346,8 @@ def main():
         from luvas3d import _lib
         lib = _lib.load()
         pinned = [torch.from_numpy(np.ascontiguousarray(im)).pin_memory() for im in w.images]
-        out_f = torch.empty((V, w.height, w.width), dtype=torch.int32).pin_memory()
+        out_f = torch.empty(w.pixels, dtype=torch.int32).pin_memory()
+        f_off = np.concatenate([[0], np.cumsum([a * b for a, b in sizes])])
         out_t = torch.empty(vox, dtype=torch.float32).pin_memory()
         out_w = torch.empty(vox, dtype=torch.int16).pin_memory()
 
@@ -339,7 +360,7 @@ def main():
             tsdf.integrate_many(iviews, stereo=stereo, layers=refs)
             for r in refs:
                 _lib.check(lib.l3d_stereo_read_filtered_layer(
-                    stereo._h(), r, C.c_void_p(out_f[r].data_ptr())))
+                    stereo._h(), r, C.c_void_p(out_f[int(f_off[r]):].data_ptr())))
             _lib.check(lib.l3d_tsdf_read(tsdf._h(), C.c_void_p(out_t.data_ptr()),
                                          C.c_void_p(out_w.data_ptr())))
 
@@ -355,8 +376,8 @@ def main():
         if world > 1:
             dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
         e2e = {"value": px_iters_step * args.steps * world / float(e2e_s.item()),
-               "unit": "px-iters/s", "h2d_bytes_per_step": V * P * 4,
-               "d2h_bytes_per_step": V * P * 4 + vox * 6,
+               "unit": "px-iters/s", "h2d_bytes_per_step": w.pixels * 4,
+               "d2h_bytes_per_step": w.pixels * 4 + vox * 6,
                "ms_per_step": float(e2e_s.item()) * 1e3 / args.steps,
                "includes": "image upload from pinned host memory, PatchMatch, filter, TSDF, "
                            "read-back of the filtered maps and the TSDF volume"}
@@ -375,9 +396,10 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f16 images, f32 arithmetic" if chosen_form == FORM_FAST else "f32",
         "data": "synthetic (seeded sphere-on-plane scene, value-noise texture)",
-        "config": {"workload": "scan: 48 views 640x480, 8 sources, 5 iterations, window 11x11 "
-                               "dilated by 2, TSDF 512^3 at 4 mm, trunc 2 cm, Q8.8 weights",
+        "config": {"workload": workload_name(w),
                    "form": "fast" if chosen_form == FORM_FAST else "plain",
+                   "variant": tuned.get("variant"),
+                   "graphs": chosen_form == FORM_FAST,
                    "l2": "flushed (256 MB write) before every step",
                    "parallelism": f"replica x{world}"},
         "tsdf_voxel_updates_per_s": voxel_updates / R["ts_s"],
@@ -388,7 +410,7 @@ def main():
                   if FORM_PLAIN in res else None),
         "speedup_vs_plain": (value / res[FORM_PLAIN]["px_iters_per_s"]
                              if FORM_PLAIN in res and chosen_form != FORM_PLAIN else None),
-        "roofline": {"kernel": ("k_fast_propagate (all 48 views, one colour)"
+        "roofline": {"kernel": (f"k_fast_propagate (all {V} views, one colour)"
                                 if chosen_form == FORM_FAST else "k_propagate (one view, one colour)"),
                      "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
@@ -397,7 +419,7 @@ def main():
                      "launch_ms": R["prop_ms"], "flop_per_launch": prop_flops,
                      "flop_model": "14 candidates x sources x (18 + 36 x 37 + 15) + 936 per "
                                    "pixel of the colour"},
-        "roofline_tsdf": {"kernel": "k_integrate_many (48 views per sweep)", "bound": "hbm",
+        "roofline_tsdf": {"kernel": f"k_integrate_many ({V} views per sweep)", "bound": "hbm",
                           "achieved": tsdf_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                           "frac": tsdf_gbs / peaks.get("hbm_gbs", 6650.0),
                           "peak_source": peak_kind, "bytes_per_launch": tsdf_bytes},

@@ -162,6 +162,14 @@ void l3d_stereo_opts_default(l3d_stereo_opts* opts);
 int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_view* views,
                       const l3d_stereo_opts* opts, l3d_stereo** out);
 
+/* A DenseStereo whose views have their own image sizes (sizes: n_views (width, height) pairs).
+ * No reference counterpart (the reference keeps one texture array of one size); all calls work
+ * per view, buffers are concatenated per view.  Coarse-to-fine levels need equal sizes. */
+int l3d_stereo_create_sized(int32_t n_views, const l3d_view* views, const int32_t* sizes,
+                            const l3d_stereo_opts* opts, l3d_stereo** out);
+/* Image size of one view. */
+int l3d_stereo_view_size(const l3d_stereo* s, int32_t layer, int32_t* width, int32_t* height);
+
 /* DenseStereo.setImage(layer, gray) (dense-stereo.ts:221-228).  dtype is the host element type;
  * row_stride_bytes = 0 means tightly packed rows. */
 int l3d_stereo_set_image(l3d_stereo* s, int32_t layer, int32_t dtype, const void* pixels,
@@ -231,6 +239,17 @@ int64_t l3d_stereo_launches(const l3d_stereo* s);
  * results differ only by the texture unit's 8-bit filter weights on the rows it samples. */
 int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant);
 int32_t l3d_stereo_variant(const l3d_stereo* s);
+
+/* Times every fast-form variant on one iteration of the given batch (it overwrites that batch's
+ * hypotheses) and keeps the fastest; best_variant / best_ms (either may be NULL) report it.
+ * No reference counterpart. */
+int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
+                        const l3d_solve_opts* opts, int32_t* best_variant, float* best_ms);
+
+/* Fast form: when enabled, l3d_stereo_solve_all captures a batch's launches into a CUDA graph on
+ * first use and replays the graph for identical requests (batches with priors are launched
+ * directly).  No reference counterpart. */
+int l3d_stereo_set_graphs(l3d_stereo* s, int32_t enable);
 /* DenseStereo.destroy() (dense-stereo.ts:403-416). */
 void l3d_stereo_destroy(l3d_stereo* s);
 

@@ -73,8 +73,14 @@ cudaError_t dalloc(T** p, size_t count) {
 /* ------------------------------------------------------------------ stereo handle ---------- */
 
 struct l3d_stereo {
-    int W = 0, H = 0, V = 0;
-    long long P = 0;
+    int W = 0, H = 0, V = 0;           /* W, H: size of view 0 (every view's size when uniform) */
+    long long P = 0;                   /* largest view's pixel count */
+    std::vector<int> Wv, Hv;           /* per-view image size */
+    std::vector<long long> offv;       /* per-view offset in the concatenated per-view arrays */
+    long long Ptot = 0;                /* sum of the views' pixel counts */
+    bool uniform = true;
+    int hyp_ref = 0;                   /* view whose planes the single-view buffers hold */
+    int filtered_ref = 0;              /* view of the last filter() */
     std::vector<l3d_view> views;
     l3d_stereo_opts opts{};
     cudaStream_t stream = nullptr;
@@ -107,6 +113,15 @@ struct l3d_stereo {
     cudaEvent_t staged = nullptr;      /* after the last copy out of the pinned staging */
     uint32_t* pairs = nullptr;         /* fast form: half2(texel, right neighbour) per pixel */
     int variant = L3D_FAST_DEFAULT_VARIANT;
+    /* CUDA graphs of batched solves, keyed by the request (fast form, no priors) */
+    struct Graph {
+        std::vector<int64_t> key;
+        cudaGraphExec_t exec = nullptr;
+        L3dFastView* views = nullptr;  /* the batch's own view table */
+        int* tile_start = nullptr;
+    };
+    bool graphs = false;
+    std::vector<Graph> graph_cache;
 };
 
 namespace {
@@ -144,8 +159,8 @@ L3dParams build_params(const l3d_stereo* s, int ref, const int32_t* sources, int
     p.kinv[1] = 1.0f / p.k[1];
     p.kinv[2] = (-p.k[2]) / p.k[0];
     p.kinv[3] = (-p.k[3]) / p.k[1];
-    p.W = s->W;
-    p.H = s->H;
+    p.W = s->Wv[ref];
+    p.H = s->Hv[ref];
     p.ref = ref;
     p.n = std::min(n, L3D_MAX_SOURCES);
     p.range[0] = (float)(1.0 / min_depth);
@@ -159,7 +174,7 @@ L3dParams build_params(const l3d_stereo* s, int ref, const int32_t* sources, int
     p.needed = (unsigned)needed;
     if (coarse_w > 0 && coarse_h > 0) {
         /* scaleIntrinsics (geometry/camera.ts:28-36) */
-        double sx = (double)coarse_w / s->W, sy = (double)coarse_h / s->H;
+        double sx = (double)coarse_w / p.W, sy = (double)coarse_h / p.H;
         p.ck[0] = (float)(kr[0] * sx);
         p.ck[1] = (float)(kr[1] * sy);
         p.ck[2] = (float)((kr[2] + 0.5) * sx - 0.5);
@@ -167,8 +182,8 @@ L3dParams build_params(const l3d_stereo* s, int ref, const int32_t* sources, int
         p.cW = coarse_w;
         p.cH = coarse_h;
     }
-    p.ref_off = (long long)ref * s->P;
-    p.ref_dep_off = s->n_maps > 1 ? (long long)ref * s->P : 0;
+    p.ref_off = s->offv[ref];
+    p.ref_dep_off = s->n_maps > 1 ? s->offv[ref] : 0;
     for (int k = 0; k < p.n; k++) {
         const l3d_view& v = s->views[sources[k]];
         const double kv[4] = {v.intrinsics.fx, v.intrinsics.fy, v.intrinsics.cx, v.intrinsics.cy};
@@ -194,10 +209,10 @@ L3dParams build_params(const l3d_stereo* s, int ref, const int32_t* sources, int
         o.kt[1] = (float)(kv[1] * t[1] + kv[3] * t[2]);
         o.kt[2] = (float)t[2];
         o.layer = sources[k];
-        o.W = s->W;
-        o.H = s->H;
-        o.img_off = (long long)sources[k] * s->P;
-        o.dep_off = s->n_maps > 1 ? (long long)sources[k] * s->P : 0;
+        o.W = s->Wv[sources[k]];
+        o.H = s->Hv[sources[k]];
+        o.img_off = s->offv[sources[k]];
+        o.dep_off = s->n_maps > 1 ? s->offv[sources[k]] : 0;
     }
     return p;
 }
@@ -240,8 +255,9 @@ int check_solve(const l3d_stereo* s, int ref, const l3d_solve_opts* o) {
     return L3D_OK;
 }
 
-int upload_prior(l3d_stereo* s, const float* prior, float* dst) {
-    L3D_CUDA(cudaMemcpyAsync(dst, prior, s->P * sizeof(float), cudaMemcpyHostToDevice, s->stream),
+int upload_prior(l3d_stereo* s, int ref, const float* prior, float* dst) {
+    const size_t n = (size_t)s->Wv[ref] * s->Hv[ref];
+    L3D_CUDA(cudaMemcpyAsync(dst, prior, n * sizeof(float), cudaMemcpyHostToDevice, s->stream),
              "prior upload");
     return L3D_OK;
 }
@@ -264,7 +280,7 @@ int solve_one(l3d_stereo* s, int ref, const l3d_solve_opts* o, float4* hyp, floa
     d.hyp = hyp;
     d.cost = cost;
     if (o->prior && !o->geometric) {
-        int rc = upload_prior(s, o->prior, prior_dev);
+        int rc = upload_prior(s, ref, o->prior, prior_dev);
         if (rc) return rc;
         d.prior = prior_dev;
     }
@@ -333,15 +349,15 @@ L3dFastView fast_view(const l3d_stereo* s, int ref, const l3d_solve_opts* o, lon
         v.kinv[i] = p.kinv[i];
         v.range[i] = p.range[i];
     }
-    v.W = s->W;
-    v.H = s->H;
+    v.W = s->Wv[ref];
+    v.H = s->Hv[ref];
     v.ref = ref;
     v.n = p.n;
     v.flags = p.flags;
     v.iterations = o->iterations;
-    v.tiles_x = ((s->W + 1) / 2 + 15) / 16;
+    v.tiles_x = ((v.W + 1) / 2 + 15) / 16;
     v.pix_off = pix_off;
-    v.ref_img_off = (long long)ref * s->P;
+    v.ref_img_off = s->offv[ref];
     v.ref_dep_off = p.ref_dep_off;
     v.ref_tex = fast_tex(s) ? (unsigned long long)s->texs[ref] : 0ull;
     v.has_prior = o->prior != nullptr && !o->geometric;
@@ -398,14 +414,14 @@ int fast_batch(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
     L3D_CUDA(cudaEventSynchronize(s->staged), "staging wait");
     int tiles = 0;
     for (int i = 0; i < n; i++) {
-        long long off = per_view_offsets ? (long long)refs[i] * s->P : 0;
+        long long off = per_view_offsets ? s->offv[refs[i]] : 0;
         L3dFastView v = fast_view(s, refs[i], &opts[i], off);
         v.tile_start = tiles;
         s->fviews_host[i] = v;
         s->tile_start_host[i] = tiles;
-        tiles += v.tiles_x * ((s->H + 7) / 8);
+        tiles += v.tiles_x * ((v.H + 7) / 8);
         if (v.has_prior) {
-            L3D_CUDA(cudaMemcpyAsync(prior + off, opts[i].prior, s->P * sizeof(float),
+            L3D_CUDA(cudaMemcpyAsync(prior + off, opts[i].prior, (size_t)v.W * v.H * sizeof(float),
                                      cudaMemcpyHostToDevice, s->stream), "prior upload");
         }
     }
@@ -447,6 +463,100 @@ int fast_pack(l3d_stereo* s, const L3dFastDev& d) {
 
 /* The schedule of DenseStereo.solve for every view of a batch at once: init, iterations x
  * (colour 0, colour 1), pack. */
+/* The launches of one batched solve (init, iterations x two colours, pack). */
+int fast_schedule(l3d_stereo* s, const L3dFastDev& d, int max_it, bool any_pack) {
+    int rc;
+    if ((rc = fast_launch(s, L3D_K_INIT, d, 0, 0))) return rc;
+    for (int it = 0; it < max_it; it++)
+        for (int phase = 0; phase < 2; phase++)
+            if ((rc = fast_launch(s, L3D_K_PROPAGATE, d, it, phase))) return rc;
+    if (any_pack && (rc = fast_pack(s, d))) return rc;
+    return L3D_OK;
+}
+
+/* Request key of a batched solve: everything that shapes the launches and their parameters. */
+std::vector<int64_t> graph_key(const l3d_stereo* s, const std::vector<int32_t>& r,
+                               const std::vector<l3d_solve_opts>& o) {
+    std::vector<int64_t> k;
+    k.push_back(s->variant);
+    for (size_t i = 0; i < r.size(); i++) {
+        const l3d_solve_opts& q = o[i];
+        k.push_back(r[i]);
+        k.push_back(q.n_sources);
+        for (int j = 0; j < std::min(q.n_sources, L3D_MAX_SOURCES); j++) k.push_back(q.sources[j]);
+        int64_t a, b;
+        std::memcpy(&a, &q.min_depth, 8);
+        std::memcpy(&b, &q.max_depth, 8);
+        k.push_back(a);
+        k.push_back(b);
+        k.push_back(q.geometric * 4 + q.pack * 2);
+        k.push_back(q.iterations);
+    }
+    return k;
+}
+
+void free_graph(l3d_stereo::Graph& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    cudaFree(g.views);
+    cudaFree(g.tile_start);
+    g.exec = nullptr;
+    g.views = nullptr;
+    g.tile_start = nullptr;
+}
+
+/* Captures the batch's launches into a CUDA graph on first use and replays it afterwards.  The
+ * graph owns a copy of the view table, so replays need no host staging. */
+int fast_solve_graph(l3d_stereo* s, const std::vector<int32_t>& r, const std::vector<l3d_solve_opts>& o,
+                     int max_it, bool any_pack) {
+    std::vector<int64_t> key = graph_key(s, r, o);
+    for (auto& g : s->graph_cache)
+        if (g.key == key) {
+            L3D_CUDA(cudaGraphLaunch(g.exec, s->stream), "graph launch");
+            s->launches += 2 + 2 * max_it;
+            return L3D_OK;
+        }
+    const int n = (int)r.size();
+    L3dFastDev d;
+    int rc = fast_batch(s, n, r.data(), o.data(), s->hyp_all, s->cost_all, s->prior_all, true, &d);
+    if (rc) return rc;
+    l3d_stereo::Graph g;
+    g.key = key;
+    L3D_CUDA(cudaMalloc(&g.views, (size_t)n * sizeof(L3dFastView)), "graph view table");
+    L3D_CUDA(cudaMalloc(&g.tile_start, (size_t)(n + 1) * sizeof(int)), "graph view table");
+    L3D_CUDA(cudaMemcpyAsync(g.views, d.views, (size_t)n * sizeof(L3dFastView), cudaMemcpyDeviceToDevice,
+                             s->stream), "graph view table");
+    L3D_CUDA(cudaMemcpyAsync(g.tile_start, d.tile_start, (size_t)(n + 1) * sizeof(int),
+                             cudaMemcpyDeviceToDevice, s->stream), "graph view table");
+    d.views = g.views;
+    d.tile_start = g.tile_start;
+    cudaGraph_t graph = nullptr;
+    L3D_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+    rc = fast_schedule(s, d, max_it, any_pack);
+    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        free_graph(g);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        free_graph(g);
+        return cuda_fail(e, "graph capture");
+    }
+    e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        free_graph(g);
+        return cuda_fail(e, "graph instantiation");
+    }
+    if (s->graph_cache.size() >= 8) {  /* keep the eight most recent batches */
+        free_graph(s->graph_cache.front());
+        s->graph_cache.erase(s->graph_cache.begin());
+    }
+    s->graph_cache.push_back(g);
+    L3D_CUDA(cudaGraphLaunch(g.exec, s->stream), "graph launch");
+    return L3D_OK;
+}
+
 int fast_solve(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* opts, bool all) {
     int nn = 0;
     std::vector<int32_t> r;
@@ -463,16 +573,14 @@ int fast_solve(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
         nn++;
     }
     if (nn == 0) return L3D_OK;
+    bool any_prior = false;
+    for (auto& q : o) any_prior |= q.prior != nullptr && !q.geometric;
+    if (all && s->graphs && !any_prior) return fast_solve_graph(s, r, o, max_it, any_pack);
     L3dFastDev d;
     int rc = all ? fast_batch(s, nn, r.data(), o.data(), s->hyp_all, s->cost_all, s->prior_all, true, &d)
                  : fast_batch(s, nn, r.data(), o.data(), s->hyp, s->cost, s->prior, false, &d);
     if (rc) return rc;
-    if ((rc = fast_launch(s, L3D_K_INIT, d, 0, 0))) return rc;
-    for (int it = 0; it < max_it; it++)
-        for (int phase = 0; phase < 2; phase++)
-            if ((rc = fast_launch(s, L3D_K_PROPAGATE, d, it, phase))) return rc;
-    if (any_pack && (rc = fast_pack(s, d))) return rc;
-    return L3D_OK;
+    return fast_schedule(s, d, max_it, any_pack);
 }
 
 }  // namespace
@@ -504,9 +612,29 @@ int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_
                       const l3d_stereo_opts* opts, l3d_stereo** out) {
     if (!out) return fail(L3D_EINVAL, "out is NULL");
     *out = nullptr;
-    if (width <= 0 || height <= 0) return fail(L3D_EINVAL, "image size must be positive");
-    if ((long long)width * height >= (1ll << 31)) return fail(L3D_EINVAL, "image too large");
     if (n_views <= 0 || !views) return fail(L3D_EINVAL, "need at least one view");
+    std::vector<int32_t> sizes(2 * (size_t)n_views);
+    for (int i = 0; i < n_views; i++) {
+        sizes[2 * i] = width;
+        sizes[2 * i + 1] = height;
+    }
+    return l3d_stereo_create_sized(n_views, views, sizes.data(), opts, out);
+}
+
+int l3d_stereo_create_sized(int32_t n_views, const l3d_view* views, const int32_t* sizes,
+                            const l3d_stereo_opts* opts, l3d_stereo** out) {
+    if (!out) return fail(L3D_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (n_views <= 0 || !views || !sizes) return fail(L3D_EINVAL, "need at least one view and its size");
+    long long ptot = 0, pmax = 0;
+    for (int i = 0; i < n_views; i++) {
+        const int w = sizes[2 * i], h = sizes[2 * i + 1];
+        if (w <= 0 || h <= 0) return fail(L3D_EINVAL, "image size must be positive");
+        if ((long long)w * h >= (1ll << 31)) return fail(L3D_EINVAL, "image too large");
+        ptot += (long long)w * h;
+        pmax = std::max(pmax, (long long)w * h);
+    }
+    const int width = sizes[0], height = sizes[1];
     l3d_stereo_opts o;
     if (opts) o = *opts;
     else l3d_stereo_opts_default(&o);
@@ -534,7 +662,23 @@ int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_
     s->W = width;
     s->H = height;
     s->V = n_views;
-    s->P = (long long)width * height;
+    s->P = pmax;
+    s->Ptot = ptot;
+    s->Wv.resize(n_views);
+    s->Hv.resize(n_views);
+    s->offv.resize(n_views);
+    long long acc = 0;
+    for (int i = 0; i < n_views; i++) {
+        s->Wv[i] = sizes[2 * i];
+        s->Hv[i] = sizes[2 * i + 1];
+        s->offv[i] = acc;
+        acc += (long long)s->Wv[i] * s->Hv[i];
+        s->uniform = s->uniform && s->Wv[i] == width && s->Hv[i] == height;
+    }
+    if (o.coarse && (!s->uniform || !o.coarse->uniform)) {
+        delete s;
+        return fail(L3D_EINVAL, "coarse-to-fine levels need views of one size");
+    }
     s->views.assign(views, views + n_views);
     s->opts = o;
     s->n_maps = o.depth_maps ? n_views : 1;
@@ -563,7 +707,7 @@ int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_
         s->arrays.assign(n_views, nullptr);
         s->texs.assign(n_views, 0);
         for (int i = 0; i < n_views; i++) {
-            if ((e = cudaMallocArray(&s->arrays[i], &ch, width, height)) != cudaSuccess)
+            if ((e = cudaMallocArray(&s->arrays[i], &ch, s->Wv[i], s->Hv[i])) != cudaSuccess)
                 return cleanup(cuda_fail(e, "image array allocation"));
             cudaResourceDesc res;
             std::memset(&res, 0, sizeof(res));
@@ -581,21 +725,22 @@ int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_
             if ((e = cudaCreateTextureObject(&s->texs[i], &res, &td, nullptr)) != cudaSuccess)
                 return cleanup(cuda_fail(e, "texture creation"));
         }
-        if ((e = dalloc(&s->pairs, (size_t)n_views * s->P)) != cudaSuccess)
+        if ((e = dalloc(&s->pairs, (size_t)s->Ptot)) != cudaSuccess)
             return cleanup(cuda_fail(e, "pair image allocation"));
-        if ((e = cudaMemsetAsync(s->pairs, 0, (size_t)n_views * s->P * 4, s->stream)) != cudaSuccess)
+        if ((e = cudaMemsetAsync(s->pairs, 0, (size_t)s->Ptot * 4, s->stream)) != cudaSuccess)
             return cleanup(cuda_fail(e, "device clear"));
     }
-    if ((e = cudaMalloc(&s->images, (size_t)n_views * s->P * esize)) != cudaSuccess ||
-        (e = dalloc(&s->depths, (size_t)s->n_maps * s->P)) != cudaSuccess ||
+    const size_t depth_len = s->n_maps > 1 ? (size_t)s->Ptot : (size_t)s->P;
+    if ((e = cudaMalloc(&s->images, (size_t)s->Ptot * esize)) != cudaSuccess ||
+        (e = dalloc(&s->depths, depth_len)) != cudaSuccess ||
         (e = dalloc(&s->hyp, (size_t)s->P)) != cudaSuccess ||
         (e = dalloc(&s->cost, (size_t)s->P)) != cudaSuccess ||
         (e = dalloc(&s->prior, (size_t)s->P)) != cudaSuccess ||
         (e = dalloc(&s->filtered, (size_t)s->P)) != cudaSuccess)
         return cleanup(cuda_fail(e, "device allocation"));
     /* zero-initialised like WebGPU buffers */
-    if ((e = cudaMemsetAsync(s->images, 0, (size_t)n_views * s->P * esize, s->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(s->depths, 0, (size_t)s->n_maps * s->P * 4, s->stream)) != cudaSuccess ||
+    if ((e = cudaMemsetAsync(s->images, 0, (size_t)s->Ptot * esize, s->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(s->depths, 0, depth_len * 4, s->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(s->hyp, 0, (size_t)s->P * 16, s->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(s->cost, 0, (size_t)s->P * 4, s->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(s->prior, 0, (size_t)s->P * 4, s->stream)) != cudaSuccess ||
@@ -611,10 +756,11 @@ int l3d_stereo_set_image(l3d_stereo* s, int32_t layer, int32_t dtype, const void
     if (layer < 0 || layer >= s->V) return fail(L3D_EINVAL, "layer %d out of range [0, %d)", layer, s->V);
     size_t es = dtype_size(dtype);
     if (!es) return fail(L3D_EINVAL, "unknown dtype %d", dtype);
-    size_t row = (size_t)s->W * es;
+    const int W = s->Wv[layer], H = s->Hv[layer];
+    size_t row = (size_t)W * es;
     size_t stride = row_stride_bytes ? (size_t)row_stride_bytes : row;
     if (stride < row) return fail(L3D_EINVAL, "row stride smaller than a row");
-    size_t need = row * s->H;
+    size_t need = row * H;
     if (s->staging_bytes < need) {
         if (s->staging) {
             cudaStreamSynchronize(s->stream);
@@ -625,24 +771,23 @@ int l3d_stereo_set_image(l3d_stereo* s, int32_t layer, int32_t dtype, const void
         L3D_CUDA(cudaMalloc(&s->staging, need), "staging allocation");
         s->staging_bytes = need;
     }
-    L3D_CUDA(cudaMemcpy2DAsync(s->staging, row, pixels, stride, row, s->H, cudaMemcpyHostToDevice,
+    L3D_CUDA(cudaMemcpy2DAsync(s->staging, row, pixels, stride, row, H, cudaMemcpyHostToDevice,
                                s->stream),
              "image upload");
     size_t out_es = dtype_size(s->opts.storage);
-    void* dst = (char*)s->images + (size_t)layer * s->P * out_es;
-    cudaError_t e = l3d_launch_convert(s->staging, dtype, (int64_t)row, s->W, s->H, dst,
+    void* dst = (char*)s->images + (size_t)s->offv[layer] * out_es;
+    cudaError_t e = l3d_launch_convert(s->staging, dtype, (int64_t)row, W, H, dst,
                                        s->opts.storage, s->stream);
     s->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "image conversion");
     if (!s->arrays.empty()) {
-        size_t rb = (size_t)s->W * out_es;
-        L3D_CUDA(cudaMemcpy2DToArrayAsync(s->arrays[layer], 0, 0, dst, rb, rb, s->H,
+        size_t rb = (size_t)W * out_es;
+        L3D_CUDA(cudaMemcpy2DToArrayAsync(s->arrays[layer], 0, 0, dst, rb, rb, H,
                                           cudaMemcpyDeviceToDevice, s->stream),
                  "image array copy");
     }
     if (s->pairs) {
-        e = l3d_launch_make_pairs(dst, s->opts.storage, s->W, s->H, s->pairs + (size_t)layer * s->P,
-                                  s->stream);
+        e = l3d_launch_make_pairs(dst, s->opts.storage, W, H, s->pairs + s->offv[layer], s->stream);
         s->launches++;
         if (e != cudaSuccess) return cuda_fail(e, "pair image");
     }
@@ -652,6 +797,7 @@ int l3d_stereo_set_image(l3d_stereo* s, int32_t layer, int32_t dtype, const void
 int l3d_stereo_solve(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o) {
     int rc = check_solve(s, ref, o);
     if (rc) return rc;
+    s->hyp_ref = ref;
     if (s->opts.form == L3D_FORM_FAST) return fast_solve(s, 1, &ref, o, false);
     return solve_one(s, ref, o, s->hyp, s->cost, s->prior);
 }
@@ -668,15 +814,15 @@ int l3d_stereo_solve_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
         for (int j = 0; j < i; j++)
             if (refs[i] == refs[j]) return fail(L3D_EINVAL, "reference layer %d appears twice", refs[i]);
     if (!s->hyp_all) {
-        L3D_CUDA(dalloc(&s->hyp_all, (size_t)s->V * s->P), "hyp_all allocation");
-        L3D_CUDA(dalloc(&s->cost_all, (size_t)s->V * s->P), "cost_all allocation");
-        L3D_CUDA(dalloc(&s->prior_all, (size_t)s->V * s->P), "prior_all allocation");
+        L3D_CUDA(dalloc(&s->hyp_all, (size_t)s->Ptot), "hyp_all allocation");
+        L3D_CUDA(dalloc(&s->cost_all, (size_t)s->Ptot), "cost_all allocation");
+        L3D_CUDA(dalloc(&s->prior_all, (size_t)s->Ptot), "prior_all allocation");
     }
     if (s->opts.form == L3D_FORM_FAST) return fast_solve(s, n_refs, refs, opts, true);
     for (int i = 0; i < n_refs; i++) {
         int r = refs[i];
-        int rc = solve_one(s, r, &opts[i], s->hyp_all + (size_t)r * s->P, s->cost_all + (size_t)r * s->P,
-                           s->prior_all + (size_t)r * s->P);
+        int rc = solve_one(s, r, &opts[i], s->hyp_all + s->offv[r], s->cost_all + s->offv[r],
+                           s->prior_all + s->offv[r]);
         if (rc) return rc;
     }
     return L3D_OK;
@@ -692,6 +838,7 @@ int l3d_stereo_dispatch(l3d_stereo* s, int32_t kernel, int32_t ref, const l3d_so
     if (kernel == L3D_KERNEL_INIT_COARSE && !s->opts.coarse)
         return fail(L3D_ESTATE, "init_coarse needs a coarse level");
     if (phase != 0 && phase != 1) return fail(L3D_EINVAL, "phase must be 0 or 1");
+    s->hyp_ref = ref;
     int n = std::min(o->n_sources, L3D_MAX_SOURCES);
     if (s->opts.form == L3D_FORM_FAST) {
         if (kernel == L3D_KERNEL_INIT_COARSE) return fail(L3D_EINVAL, "the fast form has no init_coarse");
@@ -705,7 +852,7 @@ int l3d_stereo_dispatch(l3d_stereo* s, int32_t kernel, int32_t ref, const l3d_so
     }
     L3dStereoDev d = dev_of(s);
     if (kernel == L3D_KERNEL_INIT && o->prior && !o->geometric) {
-        rc = upload_prior(s, o->prior, s->prior);
+        rc = upload_prior(s, ref, o->prior, s->prior);
         if (rc) return rc;
         d.prior = s->prior;
     }
@@ -725,6 +872,7 @@ int l3d_stereo_filter(l3d_stereo* s, int32_t ref, const int32_t* checks, int32_t
     /* DenseStereo.filter (dense-stereo.ts:296-309): range 0.01 - 100 m, no flags */
     L3dParams p = build_params(s, ref, checks, std::min(n, L3D_MAX_SOURCES), 0.01, 100.0, 0, 0, 0.0,
                                0, needed, 0, 0);
+    s->filtered_ref = ref;
     return launch(s, L3D_K_CONSISTENCY, p, dev_of(s));
 }
 
@@ -733,7 +881,7 @@ int l3d_stereo_filter_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs, co
     if (!s || n_refs < 0 || (n_refs > 0 && (!refs || !checks || !needed)))
         return fail(L3D_EINVAL, "bad arguments to filter_all");
     if (s->n_maps == 1 && s->V > 1) return fail(L3D_ESTATE, "handle was created without per-view depth maps");
-    if (!s->filtered_all) L3D_CUDA(dalloc(&s->filtered_all, (size_t)s->V * s->P), "filtered_all allocation");
+    if (!s->filtered_all) L3D_CUDA(dalloc(&s->filtered_all, (size_t)s->Ptot), "filtered_all allocation");
     for (int i = 0; i < n_refs; i++) {
         int r = refs[i];
         if (r < 0 || r >= s->V) return fail(L3D_EINVAL, "reference layer %d out of range", r);
@@ -745,7 +893,7 @@ int l3d_stereo_filter_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs, co
         if (rc) return rc;
         L3dParams p = build_params(s, r, src, n, 0.01, 100.0, 0, 0, 0.0, 0, needed[i], 0, 0);
         L3dStereoDev d = dev_of(s);
-        d.filtered = s->filtered_all + (size_t)r * s->P;
+        d.filtered = s->filtered_all + s->offv[r];
         rc = launch(s, L3D_K_CONSISTENCY, p, d);
         if (rc) return rc;
     }
@@ -760,29 +908,34 @@ static int read_dev(l3d_stereo* s, void* dst, const void* src, size_t bytes, con
 
 int l3d_stereo_read_filtered(l3d_stereo* s, uint32_t* out) {
     if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
-    return read_dev(s, out, s->filtered, s->P * 4, "read filtered");
+    const int r = s->filtered_ref;
+    return read_dev(s, out, s->filtered, (size_t)s->Wv[r] * s->Hv[r] * 4, "read filtered");
 }
 
 int l3d_stereo_read_filtered_layer(l3d_stereo* s, int32_t layer, uint32_t* out) {
     if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
     if (layer < 0 || layer >= s->V) return fail(L3D_EINVAL, "layer out of range");
     if (!s->filtered_all) return fail(L3D_ESTATE, "no filter_all has run");
-    return read_dev(s, out, s->filtered_all + (size_t)layer * s->P, s->P * 4, "read filtered layer");
+    return read_dev(s, out, s->filtered_all + s->offv[layer], (size_t)s->Wv[layer] * s->Hv[layer] * 4,
+                    "read filtered layer");
 }
 
 int l3d_stereo_read_depth(l3d_stereo* s, int32_t ref, uint32_t* out) {
     if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
     if (ref < 0 || ref >= s->n_maps) return fail(L3D_EINVAL, "depth map %d out of range", ref);
-    return read_dev(s, out, s->depths + (size_t)ref * s->P, s->P * 4, "read depth");
+    return read_dev(s, out, s->depths + (s->n_maps > 1 ? s->offv[ref] : 0),
+                    (size_t)s->Wv[ref] * s->Hv[ref] * 4, "read depth");
 }
 
 int l3d_stereo_read_hyp(l3d_stereo* s, float* hyp4, float* cost) {
     if (!s) return fail(L3D_EINVAL, "NULL handle");
     if (hyp4) {
-        int rc = read_dev(s, hyp4, s->hyp, s->P * 16, "read hypotheses");
+        int rc = read_dev(s, hyp4, s->hyp, (size_t)s->Wv[s->hyp_ref] * s->Hv[s->hyp_ref] * 16,
+                          "read hypotheses");
         if (rc) return rc;
     }
-    if (cost) return read_dev(s, cost, s->cost, s->P * 4, "read costs");
+    if (cost)
+        return read_dev(s, cost, s->cost, (size_t)s->Wv[s->hyp_ref] * s->Hv[s->hyp_ref] * 4, "read costs");
     return L3D_OK;
 }
 
@@ -791,24 +944,29 @@ int l3d_stereo_read_hyp_layer(l3d_stereo* s, int32_t layer, float* hyp4, float* 
     if (layer < 0 || layer >= s->V) return fail(L3D_EINVAL, "layer out of range");
     if (!s->hyp_all) return fail(L3D_ESTATE, "no solve_all has run");
     if (hyp4) {
-        int rc = read_dev(s, hyp4, s->hyp_all + (size_t)layer * s->P, s->P * 16, "read hypotheses");
+        int rc = read_dev(s, hyp4, s->hyp_all + s->offv[layer], (size_t)s->Wv[layer] * s->Hv[layer] * 16,
+                          "read hypotheses");
         if (rc) return rc;
     }
-    if (cost) return read_dev(s, cost, s->cost_all + (size_t)layer * s->P, s->P * 4, "read costs");
+    if (cost)
+        return read_dev(s, cost, s->cost_all + s->offv[layer], (size_t)s->Wv[layer] * s->Hv[layer] * 4,
+                        "read costs");
     return L3D_OK;
 }
 
 int l3d_stereo_write_hyp(l3d_stereo* s, const float* hyp4, const float* cost) {
     if (!s) return fail(L3D_EINVAL, "NULL handle");
-    if (hyp4) L3D_CUDA(cudaMemcpyAsync(s->hyp, hyp4, s->P * 16, cudaMemcpyHostToDevice, s->stream), "write hypotheses");
-    if (cost) L3D_CUDA(cudaMemcpyAsync(s->cost, cost, s->P * 4, cudaMemcpyHostToDevice, s->stream), "write costs");
+    const size_t n = (size_t)s->Wv[s->hyp_ref] * s->Hv[s->hyp_ref];
+    if (hyp4) L3D_CUDA(cudaMemcpyAsync(s->hyp, hyp4, n * 16, cudaMemcpyHostToDevice, s->stream), "write hypotheses");
+    if (cost) L3D_CUDA(cudaMemcpyAsync(s->cost, cost, n * 4, cudaMemcpyHostToDevice, s->stream), "write costs");
     return L3D_OK;
 }
 
 int l3d_stereo_write_depth(l3d_stereo* s, int32_t ref, const uint32_t* packed) {
     if (!s || !packed) return fail(L3D_EINVAL, "NULL argument");
     if (ref < 0 || ref >= s->n_maps) return fail(L3D_EINVAL, "depth map %d out of range", ref);
-    L3D_CUDA(cudaMemcpyAsync(s->depths + (size_t)ref * s->P, packed, s->P * 4, cudaMemcpyHostToDevice,
+    L3D_CUDA(cudaMemcpyAsync(s->depths + (s->n_maps > 1 ? s->offv[ref] : 0), packed,
+                             (size_t)s->Wv[ref] * s->Hv[ref] * 4, cudaMemcpyHostToDevice,
                              s->stream),
              "write depth");
     return L3D_OK;
@@ -823,7 +981,8 @@ int l3d_stereo_plane_cost(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o, c
         L3D_CUDA(dalloc(&s->planes, (size_t)s->P), "plane scratch");
         L3D_CUDA(dalloc(&s->plane_out, (size_t)s->P * (1 + L3D_MAX_SOURCES)), "plane scratch");
     }
-    L3D_CUDA(cudaMemcpyAsync(s->planes, planes, s->P * 16, cudaMemcpyHostToDevice, s->stream), "planes upload");
+    const size_t pn = (size_t)s->Wv[ref] * s->Hv[ref];
+    L3D_CUDA(cudaMemcpyAsync(s->planes, planes, pn * 16, cudaMemcpyHostToDevice, s->stream), "planes upload");
     if (s->opts.form == L3D_FORM_FAST) {
         if (view_costs) return fail(L3D_EINVAL, "the fast form reports the combined cost only");
         L3dFastDev fd;
@@ -833,7 +992,7 @@ int l3d_stereo_plane_cost(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o, c
         cudaError_t e = l3d_launch_fast_plane_cost(fd, s->planes, s->plane_out, s->variant, s->stream);
         s->launches++;
         if (e != cudaSuccess) return cuda_fail(e, "plane cost launch");
-        return read_dev(s, cost, s->plane_out, s->P * 4, "read plane cost");
+        return read_dev(s, cost, s->plane_out, pn * 4, "read plane cost");
     }
     int n = std::min(o->n_sources, L3D_MAX_SOURCES);
     L3dParams p = build_params(s, ref, o->sources, n, o->min_depth, o->max_depth, 0, 0, 1.0,
@@ -842,9 +1001,10 @@ int l3d_stereo_plane_cost(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o, c
                                           s->opts.window, s->opts.dilation, s->stream);
     s->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "plane cost launch");
-    rc = read_dev(s, cost, s->plane_out, s->P * 4, "read plane cost");
+    rc = read_dev(s, cost, s->plane_out, pn * 4, "read plane cost");
     if (rc) return rc;
-    if (view_costs) return read_dev(s, view_costs, s->plane_out + s->P, s->P * 4 * L3D_MAX_SOURCES, "read view costs");
+    if (view_costs)
+        return read_dev(s, view_costs, s->plane_out + s->P, pn * 4 * L3D_MAX_SOURCES, "read view costs");
     return L3D_OK;
 }
 
@@ -875,6 +1035,14 @@ int l3d_stereo_synchronize(l3d_stereo* s) {
 
 int64_t l3d_stereo_launches(const l3d_stereo* s) { return s ? s->launches : -1; }
 
+int l3d_stereo_view_size(const l3d_stereo* s, int32_t layer, int32_t* width, int32_t* height) {
+    if (!s || !width || !height) return fail(L3D_EINVAL, "NULL argument");
+    if (layer < 0 || layer >= s->V) return fail(L3D_EINVAL, "layer %d out of range", layer);
+    *width = s->Wv[layer];
+    *height = s->Hv[layer];
+    return L3D_OK;
+}
+
 int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant) {
     if (!s) return fail(L3D_EINVAL, "NULL handle");
     if (s->opts.form != L3D_FORM_FAST) return fail(L3D_ESTATE, "variants select fast-form kernels");
@@ -886,6 +1054,70 @@ int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant) {
 }
 
 int32_t l3d_stereo_variant(const l3d_stereo* s) { return s ? s->variant : -1; }
+
+int l3d_stereo_set_graphs(l3d_stereo* s, int32_t enable) {
+    if (!s) return fail(L3D_EINVAL, "NULL handle");
+    if (s->opts.form != L3D_FORM_FAST) return fail(L3D_ESTATE, "graph replay is a fast-form feature");
+    s->graphs = enable != 0;
+    if (!s->graphs) {
+        cudaStreamSynchronize(s->stream);
+        for (auto& g : s->graph_cache) free_graph(g);
+        s->graph_cache.clear();
+    }
+    return L3D_OK;
+}
+
+int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
+                        const l3d_solve_opts* opts, int32_t* best_variant, float* best_ms) {
+    if (!s) return fail(L3D_EINVAL, "NULL handle");
+    if (s->opts.form != L3D_FORM_FAST) return fail(L3D_ESTATE, "the autotuner picks fast-form variants");
+    if (s->opts.storage == L3D_DTYPE_BF16) {
+        if (best_variant) *best_variant = s->variant;
+        return L3D_OK;  /* one sampler only */
+    }
+    const int candidates[] = {6, 14, 4, 12};
+    std::vector<l3d_solve_opts> one(opts, opts + n_refs);
+    for (auto& q : one) {
+        q.iterations = 1;
+        q.prior = nullptr;
+        q.pack = 0;
+    }
+    cudaEvent_t a, b;
+    L3D_CUDA(cudaEventCreate(&a), "event");
+    L3D_CUDA(cudaEventCreate(&b), "event");
+    const bool graphs = s->graphs;
+    s->graphs = false;
+    int best = s->variant;
+    float best_t = 3.0e38f;
+    int rc = L3D_OK;
+    for (int v : candidates) {
+        s->variant = v;
+        for (int rep = 0; rep < 2 && rc == L3D_OK; rep++) {  /* the first run warms the caches */
+            cudaEventRecord(a, s->stream);
+            rc = l3d_stereo_solve_all(s, n_refs, refs, one.data());
+            cudaEventRecord(b, s->stream);
+        }
+        if (rc) break;
+        if (cudaEventSynchronize(b) != cudaSuccess) {
+            rc = cuda_fail(cudaGetLastError(), "autotune");
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best_t) {
+            best_t = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    s->graphs = graphs;
+    s->variant = best;
+    if (rc) return rc;
+    if (best_variant) *best_variant = best;
+    if (best_ms) *best_ms = best_t;
+    return L3D_OK;
+}
 
 void l3d_stereo_destroy(l3d_stereo* s) {
     if (!s) return;
@@ -903,6 +1135,7 @@ void l3d_stereo_destroy(l3d_stereo* s) {
     cudaFree(s->staging);
     cudaFree(s->planes);
     cudaFree(s->plane_out);
+    for (auto& g : s->graph_cache) free_graph(g);
     for (cudaTextureObject_t t : s->texs)
         if (t) cudaDestroyTextureObject(t);
     for (cudaArray_t a : s->arrays)
@@ -939,9 +1172,9 @@ struct l3d_tsdf {
     int view_cap = 0;
     const uint32_t** depth_ptrs = nullptr;  /* device, capacity view_cap */
     uint32_t* maps = nullptr;         /* uploaded host maps, map_cap * P */
-    int map_cap = 0;
+    long long map_cap = 0;
     float* priors = nullptr;          /* uploaded priors, prior_cap * P */
-    int prior_cap = 0;
+    long long prior_cap = 0;
     float4* normals = nullptr;        /* decoded normal per 12-bit normal code */
     L3dTsdfView* views_host = nullptr;      /* pinned staging for views */
     const uint32_t** ptrs_host = nullptr;   /* pinned staging for depth pointers */
@@ -1003,25 +1236,26 @@ int ensure_mask(l3d_tsdf* t, int n) {
     return L3D_OK;
 }
 
-int ensure_maps(l3d_tsdf* t, int n) {
-    if (t->map_cap >= n) return L3D_OK;
+/* Upload buffers, sized in elements (u32 maps / f32 priors). */
+int ensure_maps(l3d_tsdf* t, long long elems) {
+    if (t->map_cap >= elems) return L3D_OK;
     cudaStreamSynchronize(t->stream);
     cudaFree(t->maps);
     t->maps = nullptr;
     t->map_cap = 0;
-    L3D_CUDA(cudaMalloc(&t->maps, (size_t)n * t->g.W * t->g.H * 4), "depth map upload buffer");
-    t->map_cap = n;
+    L3D_CUDA(cudaMalloc(&t->maps, (size_t)elems * 4), "depth map upload buffer");
+    t->map_cap = elems;
     return L3D_OK;
 }
 
-int ensure_priors(l3d_tsdf* t, int n) {
-    if (t->prior_cap >= n) return L3D_OK;
+int ensure_priors(l3d_tsdf* t, long long elems) {
+    if (t->prior_cap >= elems) return L3D_OK;
     cudaStreamSynchronize(t->stream);
     cudaFree(t->priors);
     t->priors = nullptr;
     t->prior_cap = 0;
-    L3D_CUDA(cudaMalloc(&t->priors, (size_t)n * t->g.W * t->g.H * 4), "prior upload buffer");
-    t->prior_cap = n;
+    L3D_CUDA(cudaMalloc(&t->priors, (size_t)elems * 4), "prior upload buffer");
+    t->prior_cap = elems;
     return L3D_OK;
 }
 
@@ -1147,23 +1381,26 @@ int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packe
     if (rc) return rc;
     if ((src == nullptr) == (packed == nullptr))
         return fail(L3D_EINVAL, "give exactly one of a stereo handle or a packed map");
-    const long long P = (long long)t->g.W * t->g.H;
-    if (src && (src->W != t->g.W || src->H != t->g.H))
-        return fail(L3D_EINVAL, "stereo size %dx%d differs from the volume's %dx%d", src->W, src->H, t->g.W, t->g.H);
+    /* a stereo handle's filtered map has the size of the view it was filtered for */
+    const int mw = src ? src->Wv[src->filtered_ref] : t->g.W;
+    const int mh = src ? src->Hv[src->filtered_ref] : t->g.H;
+    const long long P = (long long)mw * mh;
     if ((rc = ensure_mask(t, 1))) return rc;
     L3dTsdfView v = make_view(*view);
+    v.W = mw;
+    v.H = mh;
     const uint32_t* depth;
     if (src) {
         if ((rc = after_stereo(t, src))) return rc;
         depth = src->filtered;
     } else {
-        if ((rc = ensure_maps(t, 1))) return rc;
+        if ((rc = ensure_maps(t, P))) return rc;
         L3D_CUDA(cudaMemcpyAsync(t->maps, packed, P * 4, cudaMemcpyHostToDevice, t->stream), "map upload");
         depth = t->maps;
     }
     const float* prior = nullptr;
     if (view->prior) {
-        if ((rc = ensure_priors(t, 1))) return rc;
+        if ((rc = ensure_priors(t, P))) return rc;
         L3D_CUDA(cudaMemcpyAsync(t->priors, view->prior, P * 4, cudaMemcpyHostToDevice, t->stream), "prior upload");
         prior = t->priors;
     }
@@ -1187,9 +1424,18 @@ int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* l
     if (src) {
         if (!layers) return fail(L3D_EINVAL, "layers is NULL");
         if (!src->filtered_all) return fail(L3D_ESTATE, "stereo handle has no filter_all output");
-        if (src->W != t->g.W || src->H != t->g.H) return fail(L3D_EINVAL, "stereo size differs from the volume's");
         for (int i = 0; i < n; i++)
             if (layers[i] < 0 || layers[i] >= src->V) return fail(L3D_EINVAL, "layer %d out of range", layers[i]);
+    }
+    /* map size and prior offset per view (maps from a stereo handle keep their view's size) */
+    std::vector<int> mw(n), mh(n);
+    std::vector<long long> poff(n);
+    long long ptotal = 0;
+    for (int i = 0; i < n; i++) {
+        mw[i] = src ? src->Wv[layers[i]] : t->g.W;
+        mh[i] = src ? src->Hv[layers[i]] : t->g.H;
+        poff[i] = ptotal;
+        ptotal += (long long)mw[i] * mh[i];
     }
     int rc;
     for (int i = 0; i < n; i++)
@@ -1200,20 +1446,24 @@ int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* l
     if (src) {
         if ((rc = after_stereo(t, src))) return rc;
     } else {
-        if ((rc = ensure_maps(t, n))) return rc;
+        if ((rc = ensure_maps(t, (long long)n * P))) return rc;
         L3D_CUDA(cudaMemcpyAsync(t->maps, packed, (size_t)n * P * 4, cudaMemcpyHostToDevice, t->stream), "map upload");
     }
     if (any_prior) {
-        if ((rc = ensure_priors(t, n))) return rc;
+        if ((rc = ensure_priors(t, ptotal))) return rc;
         for (int i = 0; i < n; i++)
             if (views[i].prior)
-                L3D_CUDA(cudaMemcpyAsync(t->priors + (size_t)i * P, views[i].prior, P * 4, cudaMemcpyHostToDevice, t->stream), "prior upload");
+                L3D_CUDA(cudaMemcpyAsync(t->priors + poff[i], views[i].prior, (size_t)mw[i] * mh[i] * 4,
+                                         cudaMemcpyHostToDevice, t->stream), "prior upload");
     }
     /* the pinned staging tables are reused: wait until the previous call's copies have run */
     L3D_CUDA(cudaEventSynchronize(t->staged), "staging wait");
     for (int i = 0; i < n; i++) {
         t->views_host[i] = make_view(views[i]);
-        t->ptrs_host[i] = src ? src->filtered_all + (size_t)layers[i] * P : t->maps + (size_t)i * P;
+        t->views_host[i].W = mw[i];
+        t->views_host[i].H = mh[i];
+        t->views_host[i].prior_off = poff[i];
+        t->ptrs_host[i] = src ? src->filtered_all + src->offv[layers[i]] : t->maps + (size_t)i * P;
     }
     L3D_CUDA(cudaMemcpyAsync(t->views, t->views_host, (size_t)n * sizeof(L3dTsdfView), cudaMemcpyHostToDevice, t->stream), "view upload");
     L3D_CUDA(cudaMemcpyAsync(t->depth_ptrs, t->ptrs_host, (size_t)n * sizeof(void*), cudaMemcpyHostToDevice, t->stream), "view upload");

@@ -48,6 +48,8 @@ struct L3dTsdfView {
     float t[3];
     float conf;
     int has_prior;
+    int W, H;                  /* this view's depth-map size */
+    long long prior_off;       /* element offset of this view's prior in the prior buffer */
     double kd[4];
     double Rd[9];
     double td[3];

@@ -133,6 +133,8 @@ extern "C" int l3d_tsdf_integrate_noalloc(const l3d_tsdf_desc* d, const int32_t*
     }
     v.conf = (float)view->confidence;
     v.has_prior = prior_dev != nullptr;
+    v.W = d->width;
+    v.H = d->height;
     v.max_depth = view->max_depth;
 
     void* flags = nullptr;

@@ -71,8 +71,8 @@ __device__ __forceinline__ bool observe(const L3dTsdfGrid& g, const L3dTsdfView&
     float iz = 1.0f / cam.z;
     float rx = rintf(fmaf(v.k[0] * cam.x, iz, v.k[2]));
     float ry = rintf(fmaf(v.k[1] * cam.y, iz, v.k[3]));
-    if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)g.W && ry < (float)g.H)) return false;
-    long long i = (long long)(int)ry * g.W + (int)rx;
+    if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)v.W && ry < (float)v.H)) return false;
+    long long i = (long long)(int)ry * v.W + (int)rx;
     uint32_t packed = __ldg(depth + i);
     float d = l3d_f16_to_f32(packed & 0xffffu);
     float w;
@@ -117,8 +117,8 @@ __device__ __forceinline__ bool observe_lut(const L3dTsdfGrid& g, const L3dTsdfV
     float iz = 1.0f / cam.z;
     float rx = rintf(fmaf(v.k[0] * cam.x, iz, v.k[2]));
     float ry = rintf(fmaf(v.k[1] * cam.y, iz, v.k[3]));
-    if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)g.W && ry < (float)g.H)) return false;
-    long long i = (long long)(int)ry * g.W + (int)rx;
+    if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)v.W && ry < (float)v.H)) return false;
+    long long i = (long long)(int)ry * v.W + (int)rx;
     uint32_t packed = __ldg(depth + i);
     float d = l3d_f16_to_f32(packed & 0xffffu);
     const bool stereo = d > 0.0f;
@@ -220,7 +220,7 @@ __device__ __forceinline__ uint8_t brick_visible(const L3dTsdfGrid& g, const L3d
     double z = p2;
     if (z < 0.02 - radius || z > v.max_depth + radius) return 0;
     double margin = (v.kd[0] * radius) / fmax(0.02, z);
-    if (u < -margin || w < -margin || u > g.W + margin || w > g.H + margin) return 0;
+    if (u < -margin || w < -margin || u > v.W + margin || w > v.H + margin) return 0;
     return 1;
 }
 
@@ -314,7 +314,6 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
     int gx, gy, gz;
     long long idx, brick;
     if (!quad_coords<VEC>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
-    const long long P = (long long)g.W * g.H;
     float t[VEC];
     float wf[VEC];
     uint32_t wq[VEC];
@@ -323,7 +322,7 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
         if (!mask[(long long)vi * g.bricks + brick]) continue;
         const L3dTsdfView& v = views[vi];
         const uint32_t* depth = depths[vi];
-        const float* prior = v.has_prior ? priors + (long long)vi * P : nullptr;
+        const float* prior = v.has_prior ? priors + v.prior_off : nullptr;
 #pragma unroll
         for (int j = 0; j < VEC; j++) {
             float obs, w;

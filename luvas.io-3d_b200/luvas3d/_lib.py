@@ -115,6 +115,9 @@ SIGNATURES = [
     ("l3d_last_error", C.c_size_t, [C.c_char_p, C.c_size_t]),
     ("l3d_stereo_opts_default", None, [C.POINTER(StereoOpts)]),
     ("l3d_stereo_create", C.c_int, [_I, _I, _I, C.POINTER(View), C.POINTER(StereoOpts), C.POINTER(_P)]),
+    ("l3d_stereo_create_sized", C.c_int, [_I, C.POINTER(View), C.POINTER(C.c_int32),
+                                          C.POINTER(StereoOpts), C.POINTER(_P)]),
+    ("l3d_stereo_view_size", C.c_int, [_P, _I, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("l3d_stereo_set_image", C.c_int, [_P, _I, _I, _P, C.c_int64]),
     ("l3d_stereo_solve", C.c_int, [_P, _I, C.POINTER(SolveOpts)]),
     ("l3d_stereo_solve_all", C.c_int, [_P, _I, C.POINTER(C.c_int32), C.POINTER(SolveOpts)]),
@@ -135,6 +138,9 @@ SIGNATURES = [
     ("l3d_stereo_launches", C.c_int64, [_P]),
     ("l3d_stereo_set_variant", C.c_int, [_P, _I]),
     ("l3d_stereo_variant", C.c_int32, [_P]),
+    ("l3d_stereo_autotune", C.c_int, [_P, _I, C.POINTER(C.c_int32), C.POINTER(SolveOpts),
+                                      C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
+    ("l3d_stereo_set_graphs", C.c_int, [_P, _I]),
     ("l3d_stereo_destroy", None, [_P]),
     ("l3d_tsdf_create", C.c_int, [C.POINTER(TsdfDesc), C.POINTER(_P)]),
     ("l3d_tsdf_integrate", C.c_int, [_P, _P, _P, C.POINTER(IntegrationView)]),

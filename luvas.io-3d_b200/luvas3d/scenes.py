@@ -153,10 +153,15 @@ class Workload:
     needed: list = field(default_factory=list)
     window: int = 6
     dilation: int = 2
+    sizes: list | None = None        # per-view (width, height) when the views differ in size
+    boxes: np.ndarray | None = None
 
     @property
     def pixels(self) -> int:
-        return self.width * self.height
+        """Pixels per step summed over the views (width * height each when uniform)."""
+        if self.sizes is not None:
+            return int(sum(w * h for w, h in self.sizes))
+        return self.width * self.height * len(self.views)
 
 
 def small(seed: int = 1, n_views: int = 8, width: int = 320, height: int = 240) -> Workload:
@@ -185,3 +190,46 @@ def scan(seed: int = 2, n_views: int = 48, width: int = 640, height: int = 480,
     return Workload("scan", width, height, views, true_views, imgs, truth, src,
                     [(0.15, 4.0)] * n_views, 5, (tsdf_dim,) * 3, vox, (-half, -half, -half), 0.02,
                     needed=[3] * n_views)
+
+
+ROOM_RESOLUTIONS = ((480, 360), (640, 480), (960, 720), (1280, 960))
+
+
+def room_boxes(seed: int, n: int = 20) -> np.ndarray:
+    """n axis-aligned cuboids standing on the floor of the 4 x 3 x 2.5 m room (lo.xyz, hi.xyz)."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros((n, 6))
+    for i in range(n):
+        size = rng.uniform([0.2, 0.2, 0.2], [0.7, 0.9, 0.7])
+        cx, cz = rng.uniform(-1.6, 1.6), rng.uniform(-1.2, 1.2)
+        lo = np.array([cx - size[0] / 2, -1.25, cz - size[2] / 2])
+        out[i, :3] = lo
+        out[i, 3:] = lo + size
+    return out
+
+
+def room(seed: int = 4, n_views: int = 96, tsdf_dim: int = 768) -> Workload:
+    """96 views of mixed resolutions inside a 4 x 3 x 2.5 m room with 20 textured cuboids, on an
+    ellipse around the room centre looking across it; 8 sources, 5 iterations; TSDF 768^3 at
+    8 mm.  The image sizes are drawn uniformly from ROOM_RESOLUTIONS."""
+    rng = np.random.default_rng(seed)
+    sizes = [ROOM_RESOLUTIONS[i] for i in rng.integers(0, len(ROOM_RESOLUTIONS), size=n_views)]
+    views = []
+    for i in range(n_views):
+        a = 2 * np.pi * i / n_views
+        c = np.array([1.5 * np.sin(a), 0.2 + 0.2 * np.sin(3 * a), 1.0 * np.cos(a)])
+        target = np.array([-0.5 * c[0], -0.6, -0.5 * c[2]])
+        W, H = sizes[i]
+        k = Intrinsics(0.875 * W, 0.875 * W, W / 2.0, H / 2.0)
+        views.append(StereoView(k, look_at(c, target)))
+    boxes = room_boxes(seed + 1)
+    imgs, truth = render_room(views, sizes, boxes, seed, sigma=0.01)
+    src = neighbour_sources(n_views, min(8, n_views - 1), circular=True)
+    vox = 0.008 * 768 / tsdf_dim
+    half = tsdf_dim * vox / 2
+    w = Workload("room", sizes[0][0], sizes[0][1], views, views, imgs, truth, src,
+                 [(0.2, 6.0)] * n_views, 5, (tsdf_dim,) * 3, vox, (-half, -half, -half), 4 * vox,
+                 needed=[3] * n_views)
+    w.sizes = sizes
+    w.boxes = boxes
+    return w

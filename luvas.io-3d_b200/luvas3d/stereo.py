@@ -82,12 +82,20 @@ class DenseStereo:
     """
 
     def __init__(self, width: int, height: int, views: Sequence[StereoView],
-                 options: StereoOptions | None = None):
+                 options: StereoOptions | None = None, sizes: Sequence[tuple[int, int]] | None = None):
+        """sizes: per-view (width, height) when the views differ in size (width/height are then
+        only a default); None gives every view width x height as in the reference."""
         self._lib = _lib.load()
         o = options or StereoOptions()
         self.width = int(width)
         self.height = int(height)
         self.views = list(views)
+        self.sizes = ([(int(w), int(h)) for w, h in sizes] if sizes is not None
+                      else [(self.width, self.height)] * len(self.views))
+        if len(self.sizes) != len(self.views):
+            raise ValueError("one size per view")
+        self._hyp_ref = 0
+        self._filtered_ref = 0
         self.options = o
         copts = _lib.StereoOpts()
         self._lib.l3d_stereo_opts_default(C.byref(copts))
@@ -101,13 +109,21 @@ class DenseStereo:
         self._coarse = o.coarse  # the coarse level must outlive this one
         h = C.c_void_p()
         cviews = _c_views(self.views)
-        _lib.check(self._lib.l3d_stereo_create(self.width, self.height, len(self.views), cviews,
-                                               C.byref(copts), C.byref(h)))
+        csizes = (C.c_int32 * (2 * len(self.views)))(*[v for wh in self.sizes for v in wh])
+        _lib.check(self._lib.l3d_stereo_create_sized(len(self.views), cviews, csizes,
+                                                     C.byref(copts), C.byref(h)))
         self._handle = h
 
     @property
     def pixels(self) -> int:
         return self.width * self.height
+
+    def shape(self, layer: int) -> tuple[int, int]:
+        """(height, width) of one view."""
+        if not 0 <= int(layer) < len(self.sizes):
+            raise _lib.L3dError(_lib.L3D_EINVAL, f"layer {layer} out of range [0, {len(self.sizes)})")
+        w, h = self.sizes[int(layer)]
+        return h, w
 
     def _h(self):
         if self._handle is None:
@@ -117,8 +133,9 @@ class DenseStereo:
     def set_image(self, layer: int, gray: np.ndarray) -> None:
         """setImage (dense-stereo.ts:221-228); u8 (r8unorm), float32, float16 or bfloat16 bits."""
         a = np.ascontiguousarray(gray)
-        if a.shape[-2:] != (self.height, self.width) and a.size != self.pixels:
-            raise ValueError(f"image shape {a.shape} does not match {self.height}x{self.width}")
+        h, w = self.shape(layer)
+        if a.shape[-2:] != (h, w) and a.size != h * w:
+            raise ValueError(f"image shape {a.shape} does not match {h}x{w}")
         dtype = {np.dtype(np.uint8): _lib.DTYPE_U8, np.dtype(np.float32): _lib.DTYPE_F32,
                  np.dtype(np.float16): _lib.DTYPE_F16}.get(a.dtype)
         if dtype is None:
@@ -132,14 +149,16 @@ class DenseStereo:
 
     def solve(self, ref: int, options: SolveOptions) -> None:
         """solve (dense-stereo.ts:231-285): init, red/black iterations, pack."""
-        args = _SolveArgs(options, self.pixels)
+        h, w = self.shape(ref)
+        args = _SolveArgs(options, h * w)
         _lib.check(self._lib.l3d_stereo_solve(self._h(), int(ref), C.byref(args.c)))
+        self._hyp_ref = int(ref)
         if args.prior is not None:
             self.synchronize()  # the prior may be pinned; keep it alive until copied
 
     def solve_all(self, refs: Sequence[int], options: Sequence[SolveOptions]) -> None:
         """The photometric stage for many reference views in one call."""
-        args = [_SolveArgs(o, self.pixels) for o in options]
+        args = [_SolveArgs(o, int(np.prod(self.shape(r)))) for r, o in zip(refs, options)]
         arr = (_lib.SolveOpts * len(args))(*[a.c for a in args])
         crefs = (C.c_int32 * len(refs))(*[int(r) for r in refs])
         _lib.check(self._lib.l3d_stereo_solve_all(self._h(), len(refs), crefs, arr))
@@ -149,28 +168,31 @@ class DenseStereo:
     def dispatch(self, kernel: int, ref: int, options: SolveOptions, iteration: int = 0,
                  phase: int = 0) -> None:
         """One kernel over the whole image (the unit DenseStereo.sliced submits)."""
-        args = _SolveArgs(options, self.pixels)
+        args = _SolveArgs(options, int(np.prod(self.shape(ref))))
         _lib.check(self._lib.l3d_stereo_dispatch(self._h(), int(kernel), int(ref), C.byref(args.c),
                                                  int(iteration), int(phase)))
+        self._hyp_ref = int(ref)
         if args.prior is not None:
             self.synchronize()
 
     @property
     def hypotheses(self) -> np.ndarray:
         """The current per-pixel planes (dense-stereo.ts:288-290), read back: (H, W, 4)."""
-        hyp = np.empty((self.height, self.width, 4), dtype=np.float32)
+        hyp = np.empty(self.shape(self._hyp_ref) + (4,), dtype=np.float32)
         _lib.check(self._lib.l3d_stereo_read_hyp(self._h(), _lib.ptr(hyp), None))
         return hyp
 
     def read_hypotheses(self) -> tuple[np.ndarray, np.ndarray]:
-        hyp = np.empty((self.height, self.width, 4), dtype=np.float32)
-        cost = np.empty((self.height, self.width), dtype=np.float32)
+        shape = self.shape(self._hyp_ref)
+        hyp = np.empty(shape + (4,), dtype=np.float32)
+        cost = np.empty(shape, dtype=np.float32)
         _lib.check(self._lib.l3d_stereo_read_hyp(self._h(), _lib.ptr(hyp), _lib.ptr(cost)))
         return hyp, cost
 
     def read_hypotheses_layer(self, layer: int) -> tuple[np.ndarray, np.ndarray]:
-        hyp = np.empty((self.height, self.width, 4), dtype=np.float32)
-        cost = np.empty((self.height, self.width), dtype=np.float32)
+        shape = self.shape(layer)
+        hyp = np.empty(shape + (4,), dtype=np.float32)
+        cost = np.empty(shape, dtype=np.float32)
         _lib.check(self._lib.l3d_stereo_read_hyp_layer(self._h(), int(layer), _lib.ptr(hyp),
                                                        _lib.ptr(cost)))
         return hyp, cost
@@ -190,6 +212,7 @@ class DenseStereo:
         """filter (dense-stereo.ts:296-309): consistency check of depths[ref] into `filtered`."""
         src = (C.c_int32 * max(1, len(sources)))(*[int(s) for s in sources])
         _lib.check(self._lib.l3d_stereo_filter(self._h(), int(ref), src, len(sources), int(needed)))
+        self._filtered_ref = int(ref)
 
     def filter_all(self, refs: Sequence[int], checks: Sequence[Sequence[int]],
                    needed: Sequence[int]) -> None:
@@ -211,28 +234,29 @@ class DenseStereo:
         return self.read_filtered()
 
     def read_filtered(self) -> np.ndarray:
-        out = np.empty((self.height, self.width), dtype=np.uint32)
+        out = np.empty(self.shape(self._filtered_ref), dtype=np.uint32)
         _lib.check(self._lib.l3d_stereo_read_filtered(self._h(), _lib.ptr(out)))
         return out
 
     def read_filtered_layer(self, layer: int) -> np.ndarray:
-        out = np.empty((self.height, self.width), dtype=np.uint32)
+        out = np.empty(self.shape(layer), dtype=np.uint32)
         _lib.check(self._lib.l3d_stereo_read_filtered_layer(self._h(), int(layer), _lib.ptr(out)))
         return out
 
     def depth_map(self, ref: int) -> np.ndarray:
         """depthMap (dense-stereo.ts:355-358): raw packed map of one view, (H, W) u32."""
-        out = np.empty((self.height, self.width), dtype=np.uint32)
+        out = np.empty(self.shape(ref), dtype=np.uint32)
         _lib.check(self._lib.l3d_stereo_read_depth(self._h(), int(ref), _lib.ptr(out)))
         return out
 
     def plane_cost(self, ref: int, options: SolveOptions, planes: np.ndarray,
                    view_costs: bool = False):
         """hypothesis_cost of given planes (H, W, 4) at every pixel of view `ref`."""
-        args = _SolveArgs(options, self.pixels)
+        shape = self.shape(ref)
+        args = _SolveArgs(options, shape[0] * shape[1])
         pl = np.ascontiguousarray(planes, dtype=np.float32)
-        cost = np.empty((self.height, self.width), dtype=np.float32)
-        vc = np.empty((self.height, self.width, MAX_SOURCES), dtype=np.float32) if view_costs else None
+        cost = np.empty(shape, dtype=np.float32)
+        vc = np.empty(shape + (MAX_SOURCES,), dtype=np.float32) if view_costs else None
         _lib.check(self._lib.l3d_stereo_plane_cost(self._h(), int(ref), C.byref(args.c),
                                                    _lib.ptr(pl), _lib.ptr(cost), _lib.ptr(vc)))
         return (cost, vc) if view_costs else cost
@@ -260,6 +284,20 @@ class DenseStereo:
     @variant.setter
     def variant(self, v: int) -> None:
         _lib.check(self._lib.l3d_stereo_set_variant(self._h(), int(v)))
+
+    def autotune(self, refs: Sequence[int], options: Sequence[SolveOptions]) -> tuple[int, float]:
+        """Times each fast-form variant on one iteration of this batch; keeps the fastest."""
+        args = [_SolveArgs(o, int(np.prod(self.shape(r)))) for r, o in zip(refs, options)]
+        arr = (_lib.SolveOpts * len(args))(*[a.c for a in args])
+        crefs = (C.c_int32 * len(refs))(*[int(r) for r in refs])
+        best, ms = C.c_int32(), C.c_float()
+        _lib.check(self._lib.l3d_stereo_autotune(self._h(), len(refs), crefs, arr, C.byref(best),
+                                                 C.byref(ms)))
+        return best.value, ms.value
+
+    def set_graphs(self, enable: bool) -> None:
+        """Replay batched solves from CUDA graphs (fast form)."""
+        _lib.check(self._lib.l3d_stereo_set_graphs(self._h(), int(bool(enable))))
 
     def synchronize(self) -> None:
         _lib.check(self._lib.l3d_stereo_synchronize(self._h()))

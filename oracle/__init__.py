@@ -31,6 +31,7 @@ class StereoArgs(C.Structure):
         ("from_coarse", C.c_int32), ("coarse_hyp", C.c_void_p),
         ("coarse_w", C.c_int32), ("coarse_h", C.c_int32),
         ("needed", C.c_int32), ("threads", C.c_int32),
+        ("sizes", C.c_void_p),
     ]
 
 
@@ -103,30 +104,74 @@ def _views_array(views) -> np.ndarray:
 
 
 class Stereo:
-    """Oracle state for one image set: images (V, H, W) float32, packed depths (V, H, W) and the
-    hypothesis buffers of one reference view, in FP32 (`precision=32`) or FP64."""
+    """Oracle state for one image set: images, packed depth maps of every view and the hypothesis
+    buffers of one reference view, in FP32 (`precision=32`) or FP64.
+
+    Views may differ in size (images of different shapes): images and depth maps are then kept
+    concatenated, `depths` is a list of per-view arrays and `hyp`/`cost` take the shape of the
+    reference view of the last call."""
 
     def __init__(self, width, height, views, images, precision: int = 32, window: int = 6,
                  dilation: int = 2, threads: int = 0):
-        self.W, self.H = int(width), int(height)
         self.V = len(views)
         self.views = _views_array(views)
-        self.images = np.ascontiguousarray(np.stack([np.asarray(i, dtype=np.float32) for i in images]))
-        assert self.images.shape == (self.V, self.H, self.W)
+        imgs = [np.ascontiguousarray(i, dtype=np.float32) for i in images]
+        self.shapes = [im.shape for im in imgs]
+        self.uniform = all(sh == (int(height), int(width)) for sh in self.shapes)
+        self.W, self.H = int(width), int(height)
+        self.sizes = np.ascontiguousarray([[sh[1], sh[0]] for sh in self.shapes], dtype=np.int32)
+        self.offsets = np.concatenate([[0], np.cumsum([sh[0] * sh[1] for sh in self.shapes])])
+        self.images = np.ascontiguousarray(np.concatenate([im.reshape(-1) for im in imgs]))
         self.dt = np.float32 if precision == 32 else np.float64
         self.pre = "orc32" if precision == 32 else "orc64"
-        self.hyp = np.zeros((self.H, self.W, 4), dtype=self.dt)
-        self.cost = np.zeros((self.H, self.W), dtype=self.dt)
-        self.depths = np.zeros((self.V, self.H, self.W), dtype=np.uint32)
-        self.filtered = np.zeros((self.H, self.W), dtype=np.uint32)
+        pmax = max(sh[0] * sh[1] for sh in self.shapes)
+        self._hyp = np.zeros(pmax * 4, dtype=self.dt)
+        self._cost = np.zeros(pmax, dtype=self.dt)
+        self._filtered = np.zeros(pmax, dtype=np.uint32)
+        self._depths = np.zeros(int(self.offsets[-1]), dtype=np.uint32)
+        self._ref_shape = self.shapes[0]
         self.window, self.dilation, self.threads = window, dilation, threads
         self.coarse = None  # (hyp (h, w, 4) in this precision)
+
+    @property
+    def hyp(self):
+        h, w = self._ref_shape
+        return self._hyp[:h * w * 4].reshape(h, w, 4)
+
+    @hyp.setter
+    def hyp(self, value):
+        h, w = self._ref_shape
+        self._hyp[:h * w * 4] = np.asarray(value, dtype=self.dt).reshape(-1)
+
+    @property
+    def cost(self):
+        h, w = self._ref_shape
+        return self._cost[:h * w].reshape(h, w)
+
+    @cost.setter
+    def cost(self, value):
+        h, w = self._ref_shape
+        self._cost[:h * w] = np.asarray(value, dtype=self.dt).reshape(-1)
+
+    @property
+    def filtered(self):
+        h, w = self._ref_shape
+        return self._filtered[:h * w].reshape(h, w)
+
+    @property
+    def depths(self):
+        if self.uniform:
+            return self._depths.reshape(self.V, self.H, self.W)
+        return [self._depths[self.offsets[i]:self.offsets[i + 1]].reshape(self.shapes[i])
+                for i in range(self.V)]
 
     def _args(self, ref, sources, min_depth=0.5, max_depth=3.0, prior=None, geometric=False,
               iterations=3, pack=True, from_coarse=False, needed=0):
         keep = []
         a = StereoArgs()
         a.width, a.height, a.n_views = self.W, self.H, self.V
+        a.sizes = None if self.uniform else self.sizes.ctypes.data
+        self._ref_shape = self.shapes[int(ref)]
         a.views = self.views.ctypes.data
         a.images = self.images.ctypes.data
         a.ref = int(ref)
@@ -155,16 +200,16 @@ class Stereo:
 
     def solve(self, ref, sources, **kw) -> None:
         a, keep = self._args(ref, sources, **kw)
-        rc = getattr(load(), self.pre + "_solve")(C.byref(a), self.hyp.ctypes.data,
-                                                  self.cost.ctypes.data, self.depths.ctypes.data)
+        rc = getattr(load(), self.pre + "_solve")(C.byref(a), self._hyp.ctypes.data,
+                                                  self._cost.ctypes.data, self._depths.ctypes.data)
         assert rc == 0, "oracle rejected the arguments"
 
     def kernel(self, kernel, ref, sources, iteration=0, phase=0, **kw) -> None:
         a, keep = self._args(ref, sources, **kw)
         rc = getattr(load(), self.pre + "_kernel")(C.byref(a), int(kernel), int(iteration),
-                                                   int(phase), self.hyp.ctypes.data,
-                                                   self.cost.ctypes.data, self.depths.ctypes.data,
-                                                   self.filtered.ctypes.data)
+                                                   int(phase), self._hyp.ctypes.data,
+                                                   self._cost.ctypes.data, self._depths.ctypes.data,
+                                                   self._filtered.ctypes.data)
         assert rc == 0, "oracle rejected the arguments"
 
     def filter(self, ref, checks, needed) -> np.ndarray:
@@ -174,8 +219,9 @@ class Stereo:
     def plane_cost(self, ref, sources, planes, **kw):
         a, keep = self._args(ref, sources, **kw)
         pl = np.ascontiguousarray(planes, dtype=self.dt)
-        cost = np.zeros((self.H, self.W), dtype=self.dt)
-        vc = np.zeros((self.H, self.W, 8), dtype=self.dt)
+        h, w = self._ref_shape
+        cost = np.zeros((h, w), dtype=self.dt)
+        vc = np.zeros((h, w, 8), dtype=self.dt)
         rc = getattr(load(), self.pre + "_plane_cost")(C.byref(a), pl.ctypes.data, cost.ctypes.data,
                                                        vc.ctypes.data)
         assert rc == 0

@@ -96,6 +96,8 @@ template <typename T> struct Src {
     T B[9];
     T kt[3];
     int layer;
+    int W, H;                   /* source image size */
+    size_t off;                 /* offset of the source's image and depth map */
 };
 
 /* Params of patchmatch.wgsl.ts:12-26 as built by DenseStereo.params (dense-stereo.ts:360-401). */
@@ -108,8 +110,19 @@ template <typename T> struct Params {
     T ck[4];
     int cW, cH;
     int win_n, win_dil;
+    size_t ref_off;             /* offset of the reference image and depth map */
     Src<T> src[MAX_SOURCES];
 };
+
+/* Size and offset of view i in the concatenated image / depth-map arrays. */
+inline void view_size(const orc_stereo_args* a, int i, int* W, int* H, size_t* off) {
+    size_t o = 0;
+    for (int j = 0; j < i; j++)
+        o += a->sizes ? (size_t)a->sizes[2 * j] * a->sizes[2 * j + 1] : (size_t)a->width * a->height;
+    *W = a->sizes ? a->sizes[2 * i] : a->width;
+    *H = a->sizes ? a->sizes[2 * i + 1] : a->height;
+    *off = o;
+}
 
 /* relativePose (camera.ts:73-77) in FP64 with the reference's summation order. */
 void relative_pose(const double* a, const double* b, double* R, double* t) {
@@ -144,8 +157,7 @@ Params<T> build_params(const orc_stereo_args* a, int iteration, int phase, doubl
     p.kinv[1] = T(1) / p.k[1];
     p.kinv[2] = (-p.k[2]) / p.k[0];
     p.kinv[3] = (-p.k[3]) / p.k[1];
-    p.W = a->width;
-    p.H = a->height;
+    view_size(a, a->ref, &p.W, &p.H, &p.ref_off);
     p.ref = a->ref;
     p.n = std::min(a->n_sources, MAX_SOURCES);
     p.range[0] = (T)(1.0 / min_depth);
@@ -159,7 +171,7 @@ Params<T> build_params(const orc_stereo_args* a, int iteration, int phase, doubl
     p.needed = (uint32_t)needed;
     if (a->coarse_w > 0 && a->coarse_h > 0) {
         /* scaleIntrinsics (camera.ts:28-36) */
-        double sx = (double)a->coarse_w / a->width, sy = (double)a->coarse_h / a->height;
+        double sx = (double)a->coarse_w / p.W, sy = (double)a->coarse_h / p.H;
         p.ck[0] = (T)(ref[0] * sx);
         p.ck[1] = (T)(ref[1] * sy);
         p.ck[2] = (T)((ref[2] + 0.5) * sx - 0.5);
@@ -195,6 +207,7 @@ Params<T> build_params(const orc_stereo_args* a, int iteration, int phase, doubl
         o.kt[1] = (T)(v[1] * t[1] + v[3] * t[2]);
         o.kt[2] = (T)t[2];
         o.layer = a->sources[s];
+        view_size(a, o.layer, &o.W, &o.H, &o.off);
     }
     return p;
 }
@@ -265,8 +278,8 @@ template <typename T> struct Kernel {
         }
     }
 
-    T image(int layer, int x, int y) const {
-        return (T)images[((size_t)layer * p.H + y) * p.W + x];
+    T image(size_t off, int W, int x, int y) const {
+        return (T)images[off + (size_t)y * W + x];
     }
 
     V3<T> ray_of(T x, T y) const {
@@ -291,7 +304,7 @@ template <typename T> struct Kernel {
     T ref_pixel(int x, int y) const {
         x = std::min(std::max(x, 0), p.W - 1);
         y = std::min(std::max(y, 0), p.H - 1);
-        return image(p.ref, x, y);
+        return image(p.ref_off, p.W, x, y);
     }
 
     /* prepare_window (patchmatch.wgsl.ts:90-110) */
@@ -315,13 +328,13 @@ template <typename T> struct Kernel {
         s.rvar = maxT(Mth<T>::fma(-s.rmean, s.rmean, srr / sw), T(0));
     }
 
-    T bilinear(int layer, T u, T v) const {
+    T bilinear(const Src<T>& src, T u, T v) const {
         T x0 = Mth<T>::floor(u), y0 = Mth<T>::floor(v);
         T fx = u - x0, fy = v - y0;
         int ix0 = (int)x0, iy0 = (int)y0;
-        int ix1 = std::min(ix0 + 1, p.W - 1), iy1 = std::min(iy0 + 1, p.H - 1);
-        T a = image(layer, ix0, iy0), b = image(layer, ix1, iy0);
-        T c = image(layer, ix0, iy1), d = image(layer, ix1, iy1);
+        int ix1 = std::min(ix0 + 1, src.W - 1), iy1 = std::min(iy0 + 1, src.H - 1);
+        T a = image(src.off, src.W, ix0, iy0), b = image(src.off, src.W, ix1, iy0);
+        T c = image(src.off, src.W, ix0, iy1), d = image(src.off, src.W, ix1, iy1);
         T top = Mth<T>::fma(fx, b - a, a);
         T bot = Mth<T>::fma(fx, d - c, c);
         return Mth<T>::fma(fy, bot - top, top);
@@ -332,7 +345,7 @@ template <typename T> struct Kernel {
         T h[9];
         for (int r = 0; r < 3; r++)
             for (int c = 0; c < 3; c++) h[r * 3 + c] = Mth<T>::fma(src.kt[r], u[c], src.B[r * 3 + c]);
-        const T wmax = (T)(p.W - 1), hmax = (T)(p.H - 1);
+        const T wmax = (T)(src.W - 1), hmax = (T)(src.H - 1);
         T ss = 0, sss = 0, srs = 0;
         for (int i = 0; i < S; i++) {
             T x = s.px + (T)off[i][0];
@@ -344,7 +357,7 @@ template <typename T> struct Kernel {
             T iz = T(1) / qz;
             T uu = qx * iz, vv = qy * iz;
             if (!(uu >= T(0) && vv >= T(0) && uu <= wmax && vv <= hmax)) return T(2);
-            T val = bilinear(src.layer, uu, vv);
+            T val = bilinear(src, uu, vv);
             T w = s.rw[i];
             ss = Mth<T>::fma(w, val, ss);
             T wv = w * val;
@@ -373,9 +386,9 @@ template <typename T> struct Kernel {
         T iz = T(1) / xs.z;
         T rx = Mth<T>::rint(Mth<T>::fma(v.k[0] * xs.x, iz, v.k[2]));
         T ry = Mth<T>::rint(Mth<T>::fma(v.k[1] * xs.y, iz, v.k[3]));
-        if (!(rx >= T(0) && ry >= T(0) && rx < (T)p.W && ry < (T)p.H)) return bad;
+        if (!(rx >= T(0) && ry >= T(0) && rx < (T)v.W && ry < (T)v.H)) return bad;
         int ix = (int)rx, iy = (int)ry;
-        uint32_t packed = depths[((size_t)v.layer * p.H + iy) * p.W + ix];
+        uint32_t packed = depths[v.off + (size_t)iy * v.W + ix];
         T ds_ = unpack_depth<T>(packed);
         if (!(ds_ > T(0)) || unpack_cost(packed) > FILTER_COST) return bad;
         V3<T> bs = {((rx - v.k[2]) / v.k[0]) * ds_, ((ry - v.k[3]) / v.k[1]) * ds_, ds_};
@@ -469,7 +482,7 @@ template <typename T> struct Kernel {
         V3<T> n = random_normal(s);
         T d = random_depth(s);
         if (p.flags & 1u) {
-            uint32_t packed = depths[(size_t)p.ref * p.W * p.H + index];
+            uint32_t packed = depths[p.ref_off + index];
             if (unpack_depth<T>(packed) > T(0)) {
                 d = unpack_depth<T>(packed);
                 n = unpack_normal<T>(packed);
@@ -618,7 +631,7 @@ template <typename T> struct Kernel {
     /* consistency (patchmatch.wgsl.ts:436-469) */
     uint32_t consistency(int x, int y) const {
         size_t index = (size_t)y * p.W + x;
-        uint32_t packed = depths[(size_t)p.ref * p.W * p.H + index];
+        uint32_t packed = depths[p.ref_off + index];
         T d = unpack_depth<T>(packed);
         if (!(d > T(0)) || unpack_cost(packed) > FILTER_COST) return 0u;
         T px = (T)x, py = (T)y;
@@ -650,7 +663,7 @@ void run_kernel(const orc_stereo_args* a, const Params<T>& p, int kernel, T* hyp
 #endif
     if (kernel == ORC_PACK) {
         size_t total = (size_t)W * H;
-        uint32_t* out = depths + (size_t)p.ref * total;
+        uint32_t* out = depths + p.ref_off;
         for (size_t i = 0; i < total; i++) {
             V3<T> n = {hyp[i * 4], hyp[i * 4 + 1], hyp[i * 4 + 2]};
             out[i] = pack_sample<T>(hyp[i * 4 + 3], n, cost[i]);
@@ -674,8 +687,11 @@ void run_kernel(const orc_stereo_args* a, const Params<T>& p, int kernel, T* hyp
 }
 
 bool valid_args(const orc_stereo_args* a) {
-    if (!a || a->width <= 0 || a->height <= 0 || a->n_views <= 0 || !a->views || !a->images)
-        return false;
+    if (!a || a->n_views <= 0 || !a->views || !a->images) return false;
+    if (!a->sizes && (a->width <= 0 || a->height <= 0)) return false;
+    if (a->sizes)
+        for (int i = 0; i < a->n_views; i++)
+            if (a->sizes[2 * i] <= 0 || a->sizes[2 * i + 1] <= 0) return false;
     if (a->ref < 0 || a->ref >= a->n_views || a->n_sources < 0) return false;
     for (int s = 0; s < std::min(a->n_sources, MAX_SOURCES); s++)
         if (a->sources[s] < 0 || a->sources[s] >= a->n_views) return false;

@@ -27,7 +27,7 @@ enum { ORC_INIT = 0, ORC_INIT_COARSE = 1, ORC_PROPAGATE = 2, ORC_PACK = 3, ORC_C
 typedef struct {
     int32_t width, height, n_views;
     const double* views;       /* n_views * 16 */
-    const float* images;       /* n_views * height * width, values in [0, 1] */
+    const float* images;       /* every view's image, concatenated, values in [0, 1] */
     int32_t ref;
     const int32_t* sources;    /* n_sources layer indices (at most 8 are used) */
     int32_t n_sources;
@@ -43,6 +43,8 @@ typedef struct {
     int32_t coarse_w, coarse_h;
     int32_t needed;            /* consistency: views that must agree */
     int32_t threads;           /* OpenMP threads, <= 0 for the default */
+    const int32_t* sizes;      /* n_views (width, height) pairs, or NULL: every view is
+                                  width x height.  Images and depth maps are concatenated per view */
 } orc_stereo_args;
 
 /* Full schedule of DenseStereo.solve (dense-stereo.ts:231-285) for one reference view. */

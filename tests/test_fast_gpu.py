@@ -167,3 +167,34 @@ def test_fast_form_rejections(arc):
     s = make(views, [im[:48, :64] for im in imgs], 64, 48)
     with pytest.raises(L3dError):
         s.solve_all([0, 0], [SolveOptions([1], 0.5, 5.0)] * 2)
+
+
+def test_graph_replay_equals_direct_launches(arc):
+    views, imgs, truth, srcs = arc
+    W, H = 256, 192
+    a = make(views, imgs, W, H)
+    b = make(views, imgs, W, H)
+    b.set_graphs(True)
+    opts = [SolveOptions(srcs[r], 0.5, 5.0, iterations=3) for r in range(5)]
+    a.solve_all(list(range(5)), opts)
+    for _ in range(3):  # capture, then replays
+        b.solve_all(list(range(5)), opts)
+    for r in range(5):
+        assert_bit_equal(b.read_hypotheses_layer(r)[0], a.read_hypotheses_layer(r)[0], f"view {r}")
+        assert_bit_equal(b.depth_map(r), a.depth_map(r), f"packed {r}")
+    # a different request is captured separately
+    opts2 = [SolveOptions(srcs[r], 0.5, 5.0, iterations=2) for r in range(5)]
+    a.solve_all(list(range(5)), opts2)
+    b.solve_all(list(range(5)), opts2)
+    assert_bit_equal(b.read_hypotheses_layer(1)[0], a.read_hypotheses_layer(1)[0], "second graph")
+    b.set_graphs(False)
+    with pytest.raises(L3dError):
+        make(views, imgs, W, H, form=FORM_PLAIN, storage=DTYPE_F32).set_graphs(True)
+
+
+def test_autotune_picks_a_valid_variant(arc):
+    views, imgs, truth, srcs = arc
+    s = make(views, imgs, 256, 192)
+    opts = [SolveOptions(srcs[r], 0.5, 5.0, iterations=3) for r in range(5)]
+    best, ms = s.autotune(list(range(5)), opts)
+    assert best in (6, 14, 4, 12) and s.variant == best and ms > 0
