@@ -285,6 +285,54 @@ int64_t l3d_tsdf_launches(const l3d_tsdf* t);
 /* TsdfVolume.destroy() (tsdf-volume.ts:484-495). */
 void l3d_tsdf_destroy(l3d_tsdf* t);
 
+/* ---- Differentiation (no reference counterpart) ----
+ *
+ * The reference has no gradients: its WGSL kernels only evaluate costs.  These entry points give
+ * the adjoints that gradient-based plane and pose polishing after PatchMatch needs.  All
+ * pointers are device pointers; work goes on `stream` (a cudaStream_t; NULL = the handle's
+ * stream; cudaStreamLegacy for the legacy default stream), ordered after the handle's queued
+ * work and before its later work.
+ *
+ * NCC objective of a reference view: per pixel, the sum over the sources of view_cost
+ * (mvs/patchmatch.wgsl.ts:130-159, the bilateral-weighted 1 - NCC over the handle's window,
+ * exact bilinear samples of the stored images; 2 for a source the window leaves, 1 for a window
+ * without texture).  Parameters:
+ *   planes       width * height * 3 f32 of the reference view: z-depth d and normal angles
+ *                (a, b), n = (sin a cos b, sin b, -cos a cos b); a plane with d <= 0 or
+ *                n . ray >= -1e-3 costs 2 per source.
+ *   pose_deltas  n_views * 6 f32 se(3) increments (v, w) or NULL (all zero): view i's world ->
+ *                camera map becomes X -> Exp(w) (R_i X + t_i) + v.  The handle's poses stay the
+ *                FP64 base; the relative poses are composed in FP64 on the device. */
+int l3d_ncc_forward(l3d_stereo* s, int32_t ref, const int32_t* sources, int32_t n_sources,
+                    const float* planes, const float* pose_deltas, float* cost, void* stream);
+/* Adjoint of l3d_ncc_forward: with grad_cost (width * height, NULL = all ones) the gradient of
+ * sum(grad_cost * cost), written per pixel into grad_planes (width * height * 3, may be NULL)
+ * and ADDED into grad_deltas (n_views * 6 doubles, may be NULL; zero it before the first
+ * reference view of a step).  cost (may be NULL) receives the forward values.  The warped
+ * samples are recomputed, not stored. */
+int l3d_ncc_backward(l3d_stereo* s, int32_t ref, const int32_t* sources, int32_t n_sources,
+                     const float* planes, const float* pose_deltas, const float* grad_cost,
+                     float* cost, float* grad_planes, double* grad_deltas, void* stream);
+
+/* TSDF integration of one view with its depths taken from an FP32 map (depth_dev), out of place:
+ * (tsdf_in, weight_in) -> (tsdf_out, weight_out), every voxel written (in place when the
+ * pointers are equal).  packed_dev (width * height) still gives each pixel's validity, normal and
+ * cost; with depth_dev equal to the packed depths the result equals l3d_tsdf_integrate bit for
+ * bit.  The handle supplies the grid, weight type and brick mask; its own volume is untouched. */
+int l3d_tsdf_forward_depth(l3d_tsdf* t, const l3d_integration_view* view, int32_t width,
+                           int32_t height, const uint32_t* packed_dev, const float* depth_dev,
+                           const float* prior_dev, const float* tsdf_in, const void* weight_in,
+                           float* tsdf_out, void* weight_out, void* stream);
+/* Adjoint of l3d_tsdf_forward_depth at (depth_dev, tsdf_in, weight_in): given the gradients with
+ * respect to tsdf_out and weight_out (f32 weights; NULL = zero), ADDS the depth gradient into
+ * grad_depth (width * height) and writes grad_tsdf_in / grad_weight_in (voxel count, f32); any
+ * of the three outputs may be NULL.  Q8.8 weights are integers, so their gradients are zero. */
+int l3d_tsdf_backward(l3d_tsdf* t, const l3d_integration_view* view, int32_t width, int32_t height,
+                      const uint32_t* packed_dev, const float* depth_dev, const float* prior_dev,
+                      const float* tsdf_in, const void* weight_in, const float* grad_tsdf_out,
+                      const float* grad_weight_out, float* grad_depth, float* grad_tsdf_in,
+                      float* grad_weight_in, void* stream);
+
 /* Largest volume, in 8^3 bricks, that l3d_tsdf_integrate_noalloc accepts (a dense grid has
  * ceil(X/8) * ceil(Y/8) * ceil(Z/8) bricks; 2^20 covers 768^3). */
 #define L3D_NOALLOC_MAX_BRICKS (1 << 20)

@@ -122,6 +122,10 @@ struct l3d_stereo {
     };
     bool graphs = false;
     std::vector<Graph> graph_cache;
+    /* differentiable NCC: FP64 view table and per-call pair scratch, allocated on first use */
+    L3dGradView* grad_views = nullptr;
+    L3dGradPair* grad_pairs = nullptr;
+    double* grad_sums = nullptr;
 };
 
 namespace {
@@ -1008,6 +1012,97 @@ int l3d_stereo_plane_cost(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o, c
     return L3D_OK;
 }
 
+/* Shared body of l3d_ncc_forward / l3d_ncc_backward. */
+static int ncc_run(l3d_stereo* s, int32_t ref, const int32_t* sources, int32_t n, const float* planes,
+                   const float* deltas, const float* grad_cost, float* cost, float* grad_planes,
+                   double* grad_deltas, void* stream) {
+    if (!s) return fail(L3D_EINVAL, "stereo handle is NULL");
+    if (ref < 0 || ref >= s->V) return fail(L3D_EINVAL, "reference layer %d out of range [0, %d)", ref, s->V);
+    if (n <= 0 || n > L3D_MAX_SOURCES)
+        return fail(L3D_EINVAL, "source count %d outside [1, %d]", n, L3D_MAX_SOURCES);
+    int rc = check_sources(s, sources, n);
+    if (rc) return rc;
+    for (int k = 0; k < n; k++)
+        if (sources[k] == ref) return fail(L3D_EINVAL, "the reference layer %d is listed as a source", ref);
+    if (!planes) return fail(L3D_EINVAL, "planes is NULL");
+    if (!s->grad_views) {
+        std::vector<L3dGradView> table(s->V);
+        for (int v = 0; v < s->V; v++) {
+            const l3d_view& sv = s->views[v];
+            L3dGradView& g = table[v];
+            std::memset(&g, 0, sizeof(g));
+            g.k[0] = sv.intrinsics.fx;
+            g.k[1] = sv.intrinsics.fy;
+            g.k[2] = sv.intrinsics.cx;
+            g.k[3] = sv.intrinsics.cy;
+            for (int i = 0; i < 9; i++) g.R[i] = sv.pose.R[i];
+            for (int i = 0; i < 3; i++) g.t[i] = sv.pose.t[i];
+            g.W = s->Wv[v];
+            g.H = s->Hv[v];
+            g.img_off = s->offv[v];
+        }
+        L3D_CUDA(dalloc(&s->grad_pairs, L3D_MAX_SOURCES), "gradient scratch");
+        L3D_CUDA(dalloc(&s->grad_sums, 6 * L3D_MAX_SOURCES), "gradient scratch");
+        L3D_CUDA(dalloc(&s->grad_views, (size_t)s->V), "gradient view table");
+        L3D_CUDA(cudaMemcpy(s->grad_views, table.data(), table.size() * sizeof(L3dGradView),
+                            cudaMemcpyHostToDevice),
+                 "gradient view table upload");
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    const bool other = st != s->stream;
+    if (other) {
+        /* after the handle's queued work (image uploads) */
+        L3D_CUDA(cudaEventRecord(s->done, s->stream), "event record");
+        L3D_CUDA(cudaStreamWaitEvent(st, s->done, 0), "stream wait");
+    }
+    L3dGradDev d;
+    std::memset(&d, 0, sizeof(d));
+    d.images = s->images;
+    d.storage = s->opts.storage;
+    d.elem = (int)dtype_size(s->opts.storage);
+    d.window = s->opts.window;
+    d.dilation = s->opts.dilation;
+    d.W = s->Wv[ref];
+    d.H = s->Hv[ref];
+    d.ref_img_off = s->offv[ref];
+    const l3d_intrinsics& ki = s->views[ref].intrinsics;
+    const float k[4] = {(float)ki.fx, (float)ki.fy, (float)ki.cx, (float)ki.cy};
+    d.kinv[0] = 1.0f / k[0];
+    d.kinv[1] = 1.0f / k[1];
+    d.kinv[2] = (-k[2]) / k[0];
+    d.kinv[3] = (-k[3]) / k[1];
+    L3dGradJob job;
+    std::memset(&job, 0, sizeof(job));
+    job.ref = ref;
+    job.n = n;
+    for (int i = 0; i < n; i++) job.src[i] = sources[i];
+    cudaError_t e = l3d_launch_ncc_grad(d, s->grad_views, deltas, job, s->grad_pairs, s->grad_sums,
+                                        planes, grad_cost, cost, grad_planes, grad_deltas, st);
+    s->launches += grad_deltas ? 3 : 2;
+    if (e != cudaSuccess) return cuda_fail(e, "NCC gradient launch");
+    if (other) {
+        /* later handle work (image uploads) waits for these reads */
+        L3D_CUDA(cudaEventRecord(s->done, st), "event record");
+        L3D_CUDA(cudaStreamWaitEvent(s->stream, s->done, 0), "stream wait");
+    }
+    return L3D_OK;
+}
+
+int l3d_ncc_forward(l3d_stereo* s, int32_t ref, const int32_t* sources, int32_t n_sources,
+                    const float* planes, const float* pose_deltas, float* cost, void* stream) {
+    if (!cost) return fail(L3D_EINVAL, "cost is NULL");
+    return ncc_run(s, ref, sources, n_sources, planes, pose_deltas, nullptr, cost, nullptr, nullptr,
+                   stream);
+}
+
+int l3d_ncc_backward(l3d_stereo* s, int32_t ref, const int32_t* sources, int32_t n_sources,
+                     const float* planes, const float* pose_deltas, const float* grad_cost,
+                     float* cost, float* grad_planes, double* grad_deltas, void* stream) {
+    if (!grad_planes && !grad_deltas) return fail(L3D_EINVAL, "no gradient output requested");
+    return ncc_run(s, ref, sources, n_sources, planes, pose_deltas, grad_cost, cost, grad_planes,
+                   grad_deltas, stream);
+}
+
 int l3d_stereo_buffers_get(const l3d_stereo* s, l3d_stereo_buffers* out) {
     if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
     out->images = s->images;
@@ -1141,6 +1236,9 @@ void l3d_stereo_destroy(l3d_stereo* s) {
     for (cudaArray_t a : s->arrays)
         if (a) cudaFreeArray(a);
     cudaFree(s->pairs);
+    cudaFree(s->grad_views);
+    cudaFree(s->grad_pairs);
+    cudaFree(s->grad_sums);
     cudaFree(s->fviews_dev);
     cudaFree(s->tile_start_dev);
     cudaFreeHost(s->fviews_host);
@@ -1477,6 +1575,67 @@ int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* l
     if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
     if (src && (rc = before_stereo(t, src))) return rc;
     return L3D_OK;
+}
+
+/* Shared body of l3d_tsdf_forward_depth / l3d_tsdf_backward. */
+static int tsdf_depth_run(l3d_tsdf* t, const l3d_integration_view* view, int32_t width,
+                          int32_t height, const uint32_t* packed, const float* depth,
+                          const float* prior, const float* tsdf_in, const void* weight_in,
+                          float* tsdf_out, void* weight_out, const float* grad_tsdf_out,
+                          const float* grad_weight_out, float* grad_depth, float* grad_tsdf_in,
+                          float* grad_weight_in, void* stream) {
+    if (!t) return fail(L3D_EINVAL, "NULL handle");
+    int rc = check_view(view);
+    if (rc) return rc;
+    if (width <= 0 || height <= 0) return fail(L3D_EINVAL, "depth map size must be positive");
+    if (!packed || !depth || !tsdf_in || !weight_in)
+        return fail(L3D_EINVAL, "NULL packed map, depth map or input volume");
+    if ((rc = ensure_mask(t, 1))) return rc;
+    L3dTsdfView v = make_view(*view);
+    v.has_prior = prior != nullptr;
+    v.W = width;
+    v.H = height;
+    cudaStream_t st = stream ? (cudaStream_t)stream : t->stream;
+    const bool other = st != t->stream;
+    if (other) {
+        L3D_CUDA(cudaEventRecord(t->done, t->stream), "event record");
+        L3D_CUDA(cudaStreamWaitEvent(st, t->done, 0), "stream wait");
+    }
+    cudaError_t e = l3d_launch_tsdf_depth(t->g, v, t->coords, t->mask, packed, depth, prior, tsdf_in,
+                                          weight_in, tsdf_out, weight_out, grad_tsdf_out,
+                                          grad_weight_out, grad_depth, grad_tsdf_in, grad_weight_in,
+                                          t->q8, st);
+    t->launches += 2;
+    if (e != cudaSuccess) return cuda_fail(e, "differentiable integrate launch");
+    if (other) {
+        /* the brick mask is shared with the handle's own integrations */
+        L3D_CUDA(cudaEventRecord(t->done, st), "event record");
+        L3D_CUDA(cudaStreamWaitEvent(t->stream, t->done, 0), "stream wait");
+    }
+    return L3D_OK;
+}
+
+int l3d_tsdf_forward_depth(l3d_tsdf* t, const l3d_integration_view* view, int32_t width,
+                           int32_t height, const uint32_t* packed_dev, const float* depth_dev,
+                           const float* prior_dev, const float* tsdf_in, const void* weight_in,
+                           float* tsdf_out, void* weight_out, void* stream) {
+    if (!tsdf_out || !weight_out) return fail(L3D_EINVAL, "NULL output volume");
+    return tsdf_depth_run(t, view, width, height, packed_dev, depth_dev, prior_dev, tsdf_in,
+                          weight_in, tsdf_out, weight_out, nullptr, nullptr, nullptr, nullptr,
+                          nullptr, stream);
+}
+
+int l3d_tsdf_backward(l3d_tsdf* t, const l3d_integration_view* view, int32_t width, int32_t height,
+                      const uint32_t* packed_dev, const float* depth_dev, const float* prior_dev,
+                      const float* tsdf_in, const void* weight_in, const float* grad_tsdf_out,
+                      const float* grad_weight_out, float* grad_depth, float* grad_tsdf_in,
+                      float* grad_weight_in, void* stream) {
+    if (!grad_tsdf_out) return fail(L3D_EINVAL, "grad_tsdf_out is NULL");
+    if (!grad_depth && !grad_tsdf_in && !grad_weight_in)
+        return fail(L3D_EINVAL, "no gradient output requested");
+    return tsdf_depth_run(t, view, width, height, packed_dev, depth_dev, prior_dev, tsdf_in,
+                          weight_in, nullptr, nullptr, grad_tsdf_out, grad_weight_out, grad_depth,
+                          grad_tsdf_in, grad_weight_in, stream);
 }
 
 int l3d_tsdf_read(l3d_tsdf* t, float* tsdf, void* weight) {

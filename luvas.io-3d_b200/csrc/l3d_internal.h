@@ -176,6 +176,62 @@ cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_
 cudaError_t l3d_launch_tsdf_fill(float* tsdf, void* weight, long long voxels, int q8,
                                  cudaStream_t stream);
 
+/* ---- differentiable NCC (grad.cu) ---- */
+
+/* FP64 base pose and intrinsics of one view, uploaded once per stereo handle. */
+struct L3dGradView {
+    double k[4];
+    double R[9];
+    double t[3];
+    int W, H;
+    long long img_off;         /* element offset of the view's image in the storage */
+};
+
+/* One (reference, source) pair, composed on the device from the poses and increments. */
+struct L3dGradPair {
+    float B[9];
+    float kt[3];
+    float ks[4];               /* source intrinsics fx, fy, cx, cy */
+    int W, H;
+    long long img_off;
+};
+
+struct L3dGradJob {
+    int ref, n;
+    int src[L3D_MAX_SOURCES];
+};
+
+struct L3dGradDev {
+    const void* images;        /* the handle's image storage */
+    int storage;               /* L3D_DTYPE_* of the storage */
+    int elem;                  /* bytes per texel */
+    int window, dilation;      /* 6/2 or 11/1 */
+    int W, H;                  /* reference view size */
+    long long ref_img_off;
+    float kinv[4];             /* 1/fx, 1/fy, -cx/fx, -cy/fy of the reference, f32 */
+};
+
+/* Cost per reference pixel (sum over the job's sources) into cost (may be NULL) and, when
+ * grad_planes / grad_deltas are given, the gradients: per-pixel (depth, a, b) written into
+ * grad_planes, per-view se(3) gradients added into grad_deltas (FP64, 6 per view).  pairs_dev
+ * (L3D_MAX_SOURCES entries) and pair_sums (6 * L3D_MAX_SOURCES doubles) are scratch. */
+cudaError_t l3d_launch_ncc_grad(const L3dGradDev& d, const L3dGradView* views_dev,
+                                const float* deltas, const L3dGradJob& job, L3dGradPair* pairs_dev,
+                                double* pair_sums, const float* planes, const float* grad_cost,
+                                float* cost, float* grad_planes, double* grad_deltas,
+                                cudaStream_t stream);
+
+/* Differentiable TSDF integration of one view with its depth taken from an FP32 map (tsdf.cu):
+ * visibility into mask, then either the out-of-place forward (grad_tsdf_out == NULL) or its
+ * adjoint.  Two launches. */
+cudaError_t l3d_launch_tsdf_depth(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,
+                                  uint8_t* mask, const uint32_t* depth, const float* depthf,
+                                  const float* prior, const float* tsdf_in, const void* weight_in,
+                                  float* tsdf_out, void* weight_out, const float* grad_tsdf_out,
+                                  const float* grad_weight_out, float* grad_depth,
+                                  float* grad_tsdf_in, float* grad_weight_in, int q8,
+                                  cudaStream_t stream);
+
 /* Sets the calling thread's l3d_last_error() message (capi.cu). */
 void l3d_set_error(const char* msg);
 

@@ -355,6 +355,161 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
     }
 }
 
+/* ---- differentiable integration: depth from an FP32 map ---- */
+
+/* observe() with the stereo depth read from an FP32 map (validity, normal and cost still come
+ * from the packed map), plus the derivatives of the observation and of its weight with respect
+ * to that depth.  *pix is the map index whose depth was used, or -1 for a prior observation
+ * (which does not depend on the map).  With depthf[i] == unpack_depth(packed[i]) the results
+ * equal observe()'s bit for bit. */
+__device__ __forceinline__ bool observe_diff(const L3dTsdfGrid& g, const L3dTsdfView& v,
+                                             const uint32_t* __restrict__ depth,
+                                             const float* __restrict__ depthf,
+                                             const float* __restrict__ prior, int gx, int gy,
+                                             int gz, float* obs, float* wout, long long* pix,
+                                             float* dobs, float* dw) {
+    float wx = fmaf((float)gx + 0.5f, g.voxel, g.origin[0]);
+    float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
+    float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
+    const float* R = v.R;
+    float3 cam = make_float3(fmaf(R[2], wz, fmaf(R[1], wy, fmaf(R[0], wx, v.t[0]))),
+                             fmaf(R[5], wz, fmaf(R[4], wy, fmaf(R[3], wx, v.t[1]))),
+                             fmaf(R[8], wz, fmaf(R[7], wy, fmaf(R[6], wx, v.t[2]))));
+    if (!(cam.z > 0.01f)) return false;
+    float iz = 1.0f / cam.z;
+    float rx = rintf(fmaf(v.k[0] * cam.x, iz, v.k[2]));
+    float ry = rintf(fmaf(v.k[1] * cam.y, iz, v.k[3]));
+    if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)v.W && ry < (float)v.H)) return false;
+    long long i = (long long)(int)ry * v.W + (int)rx;
+    uint32_t packed = __ldg(depth + i);
+    float d = l3d_f16_to_f32(packed & 0xffffu);
+    float w, dwdd = 0.0f;
+    if (d > 0.0f) {
+        d = __ldg(depthf + i);
+        float3 n = unpack_normal(packed);
+        float3 cn = normalize3f(cam);
+        w = maxw(0.2f, fabsf(dot3f(n, cn)));
+        if (v.conf > 0.0f) {
+            float c = (float)(packed >> 28) / 8.0f;
+            float q = v.conf / d;
+            float r = clampw(q, 0.5f, 2.0f);
+            float m = maxw(0.15f, (1.0f - c) * (1.0f - c));
+            /* w m r^2 with r = conf / d inside the clamp: dr/dd = -conf / d^2 = -r / d */
+            if (q > 0.5f && q < 2.0f) dwdd = w * m * 2.0f * r * (-q / d);
+            w = w * ((m * r) * r);
+        }
+        *pix = i;
+    } else {
+        d = prior ? __ldg(prior + i) : 0.0f;
+        w = g.prior_weight;
+        *pix = -1;
+    }
+    if (!(d > 0.0f)) return false;
+    float sdf = d - cam.z;
+    if (sdf < -g.mu) return false;
+    float ratio = sdf / g.mu;
+    *obs = minw(1.0f, ratio);
+    *dobs = (1.0f < ratio) ? 0.0f : 1.0f / g.mu;
+    *wout = w;
+    *dw = dwdd;
+    return true;
+}
+
+/* Out-of-place integration of one view: (tsdf_in, weight_in) -> (tsdf_out, weight_out), every
+ * voxel written (in place when the pointers are equal).  Same culling and arithmetic as
+ * k_integrate. */
+template <bool Q8>
+__global__ void __launch_bounds__(256) k_integrate_depth(const L3dTsdfGrid g, const L3dTsdfView v,
+                                                         const int32_t* __restrict__ coords,
+                                                         const uint8_t* __restrict__ mask,
+                                                         const uint32_t* __restrict__ depth,
+                                                         const float* __restrict__ depthf,
+                                                         const float* __restrict__ prior,
+                                                         const float* tsdf_in, const void* weight_in,
+                                                         float* tsdf_out, void* weight_out,
+                                                         long long voxels) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= voxels) return;
+    int gx, gy, gz;
+    long long idx, brick;
+    if (!quad_coords<1>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
+    float t = tsdf_in[idx];
+    float ww = 0.0f;
+    uint32_t wq = 0;
+    if (Q8) wq = ((const uint16_t*)weight_in)[idx];
+    else ww = ((const float*)weight_in)[idx];
+    float obs, w, dobs, dw;
+    long long pix;
+    if (mask[brick] &&
+        observe_diff(g, v, depth, depthf, v.has_prior ? prior : nullptr, gx, gy, gz, &obs, &w, &pix,
+                     &dobs, &dw)) {
+        if (Q8) apply_q8(t, wq, obs, w, g.max_q);
+        else apply_f32(t, ww, obs, w, g.max_weight);
+    }
+    tsdf_out[idx] = t;
+    if (Q8) ((uint16_t*)weight_out)[idx] = (uint16_t)wq;
+    else ((float*)weight_out)[idx] = ww;
+}
+
+/* Adjoint of k_integrate_depth.  Per voxel, with the state (T0, W0) before the update and the
+ * observation o(d) with weight w(d):
+ *   T1 = (T0 W0 + o w) / (W0 + w),  W1 = min(W0 + w, max)
+ *   dT1/dT0 = W0 / (W0 + w),  dT1/dW0 = (T0 - T1) / (W0 + w)
+ *   dT1/dd  = (w do/dd + (o - T1) dw/dd) / (W0 + w),  dW1/dd = dw/dd, dW1/dW0 = 1 (below max)
+ * gT, gW are the loss gradients with respect to T1 and W1 (gW may be NULL).  The depth gradient
+ * is added into grad_depth with atomics (many voxels see one pixel); grad_tsdf_in and
+ * grad_weight_in (either may be NULL) are written for every voxel.  Q8.8 weights are integers:
+ * dw/dd and the weight gradients are zero there. */
+template <bool Q8>
+__global__ void __launch_bounds__(256) k_integrate_depth_grad(
+        const L3dTsdfGrid g, const L3dTsdfView v, const int32_t* __restrict__ coords,
+        const uint8_t* __restrict__ mask, const uint32_t* __restrict__ depth,
+        const float* __restrict__ depthf, const float* __restrict__ prior,
+        const float* __restrict__ tsdf_in, const void* __restrict__ weight_in,
+        const float* __restrict__ gT, const float* __restrict__ gW, float* __restrict__ grad_depth,
+        float* __restrict__ grad_tsdf_in, float* __restrict__ grad_weight_in, long long voxels) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= voxels) return;
+    int gx, gy, gz;
+    long long idx, brick;
+    if (!quad_coords<1>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
+    const float gt = gT[idx];
+    const float gw = (!Q8 && gW) ? gW[idx] : 0.0f;
+    float g_t0 = gt, g_w0 = gw;
+    float obs, w, dobs, dw;
+    long long pix;
+    if (mask[brick] &&
+        observe_diff(g, v, depth, depthf, v.has_prior ? prior : nullptr, gx, gy, gz, &obs, &w, &pix,
+                     &dobs, &dw)) {
+        const float t0 = tsdf_in[idx];
+        float w0, wu;
+        bool updated = true;
+        if (Q8) {
+            uint32_t wi = (uint32_t)rintf(w * 256.0f);
+            updated = wi != 0u;
+            w0 = (float)((const uint16_t*)weight_in)[idx] * 0.00390625f;
+            wu = (float)wi * 0.00390625f;
+            dw = 0.0f;
+        } else {
+            w0 = ((const float*)weight_in)[idx];
+            wu = w;
+        }
+        if (updated) {
+            const float den = w0 + wu;
+            const float t1 = fmaf(t0, w0, obs * wu) / den;
+            const float below = (!Q8 && (w0 + wu < g.max_weight)) ? 1.0f : 0.0f;
+            g_t0 = gt * (w0 / den);
+            g_w0 = Q8 ? 0.0f : fmaf(gt, (t0 - t1) / den, gw * below);
+            if (pix >= 0 && grad_depth) {
+                float gd = gt * (fmaf(wu, dobs, (obs - t1) * dw) / den) + gw * below * dw;
+                if (gd != 0.0f) atomicAdd(grad_depth + pix, gd);
+            }
+        }
+    }
+    if (grad_tsdf_in) grad_tsdf_in[idx] = g_t0;
+    if (grad_weight_in) grad_weight_in[idx] = Q8 ? 0.0f : g_w0;
+}
+
 __global__ void k_fill(float* tsdf, void* weight, long long voxels, int q8) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= voxels) return;
@@ -419,6 +574,28 @@ cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_
     } else {
         if (q8) k_integrate_many<1, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
         else k_integrate_many<1, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_tsdf_depth(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,
+                                  uint8_t* mask, const uint32_t* depth, const float* depthf,
+                                  const float* prior, const float* tsdf_in, const void* weight_in,
+                                  float* tsdf_out, void* weight_out, const float* grad_tsdf_out,
+                                  const float* grad_weight_out, float* grad_depth,
+                                  float* grad_tsdf_in, float* grad_weight_in, int q8,
+                                  cudaStream_t stream) {
+    if (g.bricks == 0) return cudaSuccess;
+    k_visible_one<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, v, coords, mask);
+    const long long voxels = quad_count(g, 1);
+    if (voxels == 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((voxels + 255) / 256);
+    if (grad_tsdf_out) {
+        if (q8) k_integrate_depth_grad<true><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, depthf, prior, tsdf_in, weight_in, grad_tsdf_out, grad_weight_out, grad_depth, grad_tsdf_in, grad_weight_in, voxels);
+        else k_integrate_depth_grad<false><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, depthf, prior, tsdf_in, weight_in, grad_tsdf_out, grad_weight_out, grad_depth, grad_tsdf_in, grad_weight_in, voxels);
+    } else {
+        if (q8) k_integrate_depth<true><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, depthf, prior, tsdf_in, weight_in, tsdf_out, weight_out, voxels);
+        else k_integrate_depth<false><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, depthf, prior, tsdf_in, weight_in, tsdf_out, weight_out, voxels);
     }
     return cudaGetLastError();
 }

@@ -155,6 +155,12 @@ SIGNATURES = [
     ("l3d_tsdf_destroy", None, [_P]),
     ("l3d_tsdf_integrate_noalloc", C.c_int, [C.POINTER(TsdfDesc), _P, _P, _P,
                                              C.POINTER(IntegrationView), _P, _P, _P]),
+    ("l3d_ncc_forward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P]),
+    ("l3d_ncc_backward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P, _P, _P, _P]),
+    ("l3d_tsdf_forward_depth", C.c_int, [_P, C.POINTER(IntegrationView), _I, _I, _P, _P, _P, _P, _P,
+                                         _P, _P, _P]),
+    ("l3d_tsdf_backward", C.c_int, [_P, C.POINTER(IntegrationView), _I, _I, _P, _P, _P, _P, _P, _P,
+                                    _P, _P, _P, _P, _P]),
 ]
 
 _lib = None

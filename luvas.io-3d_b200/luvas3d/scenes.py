@@ -192,6 +192,43 @@ def scan(seed: int = 2, n_views: int = 48, width: int = 640, height: int = 480,
                     needed=[3] * n_views)
 
 
+def polish(seed: int = 6, n_views: int = 24, width: int = 640, height: int = 480,
+           trans: float = 0.005, rot_deg: float = 0.3) -> Workload:
+    """The small workload's sphere scene with 24 views of 640x480 on its circle (radius 1.5 m,
+    fx = fy = 560): images rendered with the true poses, poses handed to the solver perturbed by
+    5 mm / 0.3 deg (seeded); 4 sources, 5 iterations, depths 0.3-3 m.  The starting point of
+    gradient-based plane and pose polishing."""
+    f = 280.0 * width / 320.0
+    true_views = circle_views(n_views, width, height, 1.5, f)
+    imgs, truth = render_sphere(true_views, [(width, height)] * n_views, seed, sigma=0.01)
+    views = perturb(true_views, seed + 1000, trans, rot_deg)
+    src = neighbour_sources(n_views, min(4, n_views - 1), circular=True)
+    dims = (256, 256, 256)
+    return Workload("polish", width, height, views, true_views, imgs, truth, src,
+                    [(0.3, 3.0)] * n_views, 5, dims, 0.01, (-1.28, -1.28, -1.28), 0.04,
+                    needed=[2] * n_views)
+
+
+def relative_pose_errors(views, true_views, anchor: int = 0):
+    """Per view, the rotation (degrees) and translation (metres) error of its pose relative to
+    the anchor view's, against the same relative pose of the true views (the anchor itself
+    excluded)."""
+    rot, trans = [], []
+    Ra, ta = np.asarray(views[anchor].pose.R), np.asarray(views[anchor].pose.t)
+    Qa, qa = np.asarray(true_views[anchor].pose.R), np.asarray(true_views[anchor].pose.t)
+    for i, (v, tv) in enumerate(zip(views, true_views)):
+        if i == anchor:
+            continue
+        R = np.asarray(v.pose.R) @ Ra.T
+        t = np.asarray(v.pose.t) - R @ ta
+        Q = np.asarray(tv.pose.R) @ Qa.T
+        q = np.asarray(tv.pose.t) - Q @ qa
+        c = np.clip((np.trace(R @ Q.T) - 1) / 2, -1.0, 1.0)
+        rot.append(np.degrees(np.arccos(c)))
+        trans.append(float(np.linalg.norm(t - q)))
+    return np.asarray(rot), np.asarray(trans)
+
+
 ROOM_RESOLUTIONS = ((480, 360), (640, 480), (960, 720), (1280, 960))
 
 

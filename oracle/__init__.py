@@ -73,6 +73,8 @@ def load():
             getattr(lib, pre + "_tsdf_integrate").argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView),
                                                               P, P, P, C.c_int32]
         lib.orc_tsdf_visible.argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView), P]
+        lib.orc64_ncc_grad.argtypes = [C.POINTER(StereoArgs), P, P, P, P, P, P, P, P]
+        lib.orc64_tsdf_depth.argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView)] + [P] * 11 + [C.c_int32]
         lib.orc_pack_sample.restype = C.c_uint32
         lib.orc_pack_sample.argtypes = [C.c_float] * 5
         lib.orc_unpack_depth.restype = C.c_float
@@ -226,6 +228,80 @@ class Stereo:
                                                        vc.ctypes.data)
         assert rc == 0
         return cost, vc
+
+
+class NccGrad:
+    """FP64 summed-NCC objective of one reference view and its forward-mode (dual-number)
+    gradients with respect to per-pixel planes (depth, angle a, angle b) and per-view se(3)
+    increments (oracle/grad.cpp)."""
+
+    def __init__(self, views, images, window: int = 6, dilation: int = 2, threads: int = 0):
+        self.st = Stereo(images[0].shape[1], images[0].shape[0], views, images, precision=64,
+                         window=window, dilation=dilation, threads=threads)
+
+    def __call__(self, ref, sources, planes, deltas=None, weights=None, grad_planes=False,
+                 grad_deltas=False):
+        """Returns (cost (H, W), grad_planes (H, W, 3) or None, grad_deltas (V, 6) or None) for
+        the objective sum(weights * cost) (weights None = ones)."""
+        a, keep = self.st._args(ref, sources)
+        h, w = self.st._ref_shape
+        pl = np.ascontiguousarray(planes, dtype=np.float64).reshape(h, w, 3)
+        de = None if deltas is None else np.ascontiguousarray(deltas, dtype=np.float64).reshape(-1, 6)
+        wt = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64).reshape(h, w)
+        cost = np.zeros((h, w), dtype=np.float64)
+        gp = np.zeros((h, w, 3), dtype=np.float64) if grad_planes else None
+        gd = np.zeros((self.st.V, 6), dtype=np.float64) if grad_deltas else None
+        ptr = lambda x: None if x is None else x.ctypes.data  # noqa: E731
+        rc = load().orc64_ncc_grad(C.byref(a), pl.ctypes.data, ptr(de), ptr(wt), cost.ctypes.data,
+                                   ptr(gp), ptr(gd), None, None)
+        assert rc == 0
+        return cost, gp, gd
+
+    def structure(self, ref, sources, planes, deltas=None):
+        """(cost, margin, cells) per pixel: margin is the smallest distance (texels) from a
+        window sample to a source's border (-1 where a source's cost is the constant 2 or 1),
+        cells a hash of the texel cells the samples fall in; the cost is smooth in a parameter
+        while a pixel's hash stays the same."""
+        a, keep = self.st._args(ref, sources)
+        h, w = self.st._ref_shape
+        pl = np.ascontiguousarray(planes, dtype=np.float64).reshape(h, w, 3)
+        de = None if deltas is None else np.ascontiguousarray(deltas, dtype=np.float64).reshape(-1, 6)
+        margin = np.zeros((h, w), dtype=np.float64)
+        cells = np.zeros((h, w), dtype=np.uint64)
+        cost = np.zeros((h, w), dtype=np.float64)
+        rc = load().orc64_ncc_grad(C.byref(a), pl.ctypes.data, None if de is None else de.ctypes.data,
+                                   None, cost.ctypes.data, None, None, margin.ctypes.data,
+                                   cells.ctypes.data)
+        assert rc == 0
+        return cost, margin, cells
+
+
+def tsdf_depth(desc, view_kw: dict, packed, depth, tsdf_in, weight_in, grad_tsdf=None,
+               grad_weight=None, threads=0):
+    """FP64 differentiable TSDF integration of one view (oracle/grad.cpp).  weight_in is in units
+    (Q8.8 volumes: value / 256).  Returns (tsdf_out, weight_out, grad_depth, grad_tsdf_in,
+    grad_weight_in); the gradients are None without grad_tsdf."""
+    v, keep = tsdf_view(**view_kw)
+    pk = np.ascontiguousarray(packed, dtype=np.uint32).reshape(-1)
+    dp = np.ascontiguousarray(depth, dtype=np.float64).reshape(-1)
+    t0 = np.ascontiguousarray(tsdf_in, dtype=np.float64).reshape(-1)
+    w0 = np.ascontiguousarray(weight_in, dtype=np.float64).reshape(-1)
+    t1 = np.empty_like(t0)
+    w1 = np.empty_like(w0)
+    gd = gt0 = gw0 = None
+    gT = gW = None
+    if grad_tsdf is not None:
+        gT = np.ascontiguousarray(grad_tsdf, dtype=np.float64).reshape(-1)
+        gW = None if grad_weight is None else np.ascontiguousarray(grad_weight, dtype=np.float64).reshape(-1)
+        gd = np.zeros_like(dp)
+        gt0 = np.empty_like(t0)
+        gw0 = np.empty_like(w0)
+    ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+    rc = load().orc64_tsdf_depth(C.byref(desc), C.byref(v), ptr(pk), ptr(dp), ptr(t0), ptr(w0),
+                                 ptr(t1), ptr(w1), ptr(gT), ptr(gW), ptr(gd), ptr(gt0), ptr(gw0),
+                                 int(threads))
+    assert rc == 0
+    return t1, w1, gd, gt0, gw0
 
 
 def tsdf_desc(width, height, voxel, origin, truncation, dense=None, coords=None,

@@ -95,6 +95,33 @@ int orc64_tsdf_integrate(const orc_tsdf_desc* d, const orc_tsdf_view* v, const u
 /* Brick visibility of tsdf-volume.ts:425-439 (FP64); out: count (or dense brick count) bytes. */
 int orc_tsdf_visible(const orc_tsdf_desc* d, const orc_tsdf_view* v, uint8_t* out);
 
+/* ---- gradients (grad.cpp): forward-mode dual numbers over FP64 restatements ---- */
+
+/* Summed NCC cost of reference a->ref over a->sources (a->n_sources <= 8) per pixel, for planes
+ * (P * 3: z-depth, angles a, b with n = (sin a cos b, sin b, -cos a cos b)) and per-view se(3)
+ * increments deltas (n_views * 6: v, w; NULL = zero): cost (P, may be NULL) and the gradient of
+ * sum(weights * cost) (weights P, NULL = ones) per pixel in grad_planes (P * 3, may be NULL) and
+ * for the poses ADDED into grad_deltas (n_views * 6, may be NULL).  Computed with the cost only
+ * (grad_planes NULL): margin (P, may be NULL) receives each pixel's smallest distance in texels
+ * from a window sample to a source image's border, -1 where a source costs the constant 2 or 1,
+ * and cells (P, may be NULL) a hash of the texel cells its samples fall in (the objective is
+ * smooth in a parameter as long as the pixel's hash stays the same).
+ * Uses a->views, images, sizes, width, height, win_n, win_dil, threads. */
+int orc64_ncc_grad(const orc_stereo_args* a, const double* planes, const double* deltas,
+                   const double* weights, double* cost, double* grad_planes, double* grad_deltas,
+                   double* margin, uint64_t* cells);
+
+/* TSDF integration of one view with the depth of each valid pixel (packed map says valid) taken
+ * from depth (width * height), out of place, and its adjoint: tsdf_out / weight_out (may be
+ * NULL); with grad_tsdf_out / grad_weight_out (NULL = zero) the gradient ADDED into grad_depth
+ * and written into grad_tsdf_in / grad_weight_in (any may be NULL).  Weights are in units
+ * (Q8.8 volumes: value / 256). */
+int orc64_tsdf_depth(const orc_tsdf_desc* d, const orc_tsdf_view* v, const uint32_t* packed,
+                     const double* depth, const double* tsdf_in, const double* weight_in,
+                     double* tsdf_out, double* weight_out, const double* grad_tsdf_out,
+                     const double* grad_weight_out, double* grad_depth, double* grad_tsdf_in,
+                     double* grad_weight_in, int32_t threads);
+
 /* Packing helpers (depth-packing.wgsl.ts:3-33) and primitives for unit tests. */
 uint32_t orc_pack_sample(float depth, float nx, float ny, float nz, float cost);
 float orc_unpack_depth(uint32_t packed);
