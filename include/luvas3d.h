@@ -285,6 +285,44 @@ int64_t l3d_tsdf_launches(const l3d_tsdf* t);
 /* TsdfVolume.destroy() (tsdf-volume.ts:484-495). */
 void l3d_tsdf_destroy(l3d_tsdf* t);
 
+/* ---- Dense point cloud: PointAccumulator (fusion/point-accumulator.ts:16-147) fed by
+ * addDepthMap (fusion/depth-fusion.ts:42-74) ----
+ *
+ * Points are averaged per cell of a grid in a device hash table: position, normal and colour
+ * sums in FP64 (the reference keeps f32 sums), a sample count per cell.  Cells must lie within
+ * 2^20 cells of the origin on every axis. */
+typedef struct l3d_cloud l3d_cloud;
+
+/* new PointAccumulator(cell) (point-accumulator.ts:23); work runs on `stream` (a cudaStream_t,
+ * NULL = a stream of its own). */
+int l3d_cloud_create(double cell, void* stream, l3d_cloud** out);
+/* addDepthMap (depth-fusion.ts:42-74): every valid sample of a packed depth map becomes a world
+ * point (FP64), a world normal and the colour of the nearest thumbnail pixel (thumb_rgb: host,
+ * thumb_w * thumb_h * 3 bytes), added to its cell.  Give exactly one of `src` (its last
+ * l3d_stereo_filter result stays on the device; width and height are ignored) or `packed`
+ * (host, width * height).  `view` is the depth map's camera. */
+int l3d_cloud_add(l3d_cloud* c, const l3d_stereo* src, const uint32_t* packed, int32_t width,
+                  int32_t height, const l3d_view* view, const uint8_t* thumb_rgb, int32_t thumb_w,
+                  int32_t thumb_h);
+/* PointAccumulator.add (:29-56) of n samples, host, 9 doubles each: x y z nx ny nz r g b. */
+int l3d_cloud_add_points(l3d_cloud* c, int64_t n, const double* samples);
+/* coarsen(factor) (:85-87): the cell grows by `factor`; every cell is re-binned by its mean
+ * position and cells that fall together merge. */
+int l3d_cloud_coarsen(l3d_cloud* c, double factor);
+/* size (:25-27): occupied cells (synchronises). */
+int l3d_cloud_size(l3d_cloud* c, int64_t* size);
+int l3d_cloud_cell(const l3d_cloud* c, double* cell);
+/* cloud(minSupport) (:114-143): the averaged points of the cells with at least min_support
+ * samples, ordered by cell (z, then y, then x; the reference's order is its hash-slot order).
+ * *count receives the number of points; with every output NULL only the count is computed.
+ * Outputs (host, `capacity` points): positions and normals 3 floats, colors 3 bytes, support
+ * min(samples, 65535), cells 3 int32 (the integer cell of each point; any may be NULL). */
+int l3d_cloud_read(l3d_cloud* c, int32_t min_support, int64_t capacity, int64_t* count,
+                   float* positions, float* normals, uint8_t* colors, uint16_t* support,
+                   int32_t* cells);
+int64_t l3d_cloud_launches(const l3d_cloud* c);
+void l3d_cloud_destroy(l3d_cloud* c);
+
 /* ---- Differentiation (no reference counterpart) ----
  *
  * The reference has no gradients: its WGSL kernels only evaluate costs.  These entry points give

@@ -1691,3 +1691,331 @@ void l3d_tsdf_destroy(l3d_tsdf* t) {
 }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------ dense point cloud ------ */
+
+struct l3d_cloud {
+    double cell = 0.0;
+    L3dCloudTable t{};
+    unsigned* counters = nullptr;     /* [0] used slots, [1] emitted points */
+    int* err = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t done = nullptr;
+    uint8_t* thumb = nullptr;         /* uploaded thumbnail */
+    size_t thumb_cap = 0;
+    uint32_t* map = nullptr;          /* uploaded packed map */
+    size_t map_cap = 0;
+    double* pts = nullptr;            /* uploaded samples */
+    size_t pts_cap = 0;
+    long long launches = 0;
+};
+
+namespace {
+
+void free_table(L3dCloudTable& t) {
+    cudaFree(t.keys);
+    cudaFree(t.sums);
+    cudaFree(t.counts);
+    t = L3dCloudTable{};
+}
+
+int alloc_table(l3d_cloud* c, int capacity, L3dCloudTable* out) {
+    L3dCloudTable t{};
+    t.capacity = capacity;
+    cudaError_t e;
+    if ((e = cudaMalloc(&t.keys, (size_t)capacity * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&t.sums, (size_t)capacity * 9 * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&t.counts, (size_t)capacity * 4)) != cudaSuccess) {
+        free_table(t);
+        return cuda_fail(e, "point table allocation");
+    }
+    if ((e = l3d_launch_cloud_clear(t, c->stream)) != cudaSuccess) {
+        free_table(t);
+        return cuda_fail(e, "point table clear");
+    }
+    c->launches++;
+    *out = t;
+    return L3D_OK;
+}
+
+/* Waits for the queued work and reports a device-side error of the table. */
+int cloud_state(l3d_cloud* c, unsigned* used) {
+    unsigned h[2];
+    int err = 0;
+    L3D_CUDA(cudaMemcpyAsync(h, c->counters, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "read counters");
+    L3D_CUDA(cudaMemcpyAsync(&err, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "read error flag");
+    L3D_CUDA(cudaStreamSynchronize(c->stream), "synchronize");
+    if (err & L3D_CLOUD_ERR_RANGE)
+        return fail(L3D_EINVAL, "a point lies more than 2^20 cells from the origin (cell %g m)", c->cell);
+    if (err & L3D_CLOUD_ERR_FULL) return fail(L3D_ECUDA, "point table overflow");
+    if (used) *used = h[0];
+    return L3D_OK;
+}
+
+/* rebuild (point-accumulator.ts:89-111) into a table of `capacity` slots with cell `cell`. */
+int cloud_rebuild(l3d_cloud* c, int capacity, double cell) {
+    L3dCloudTable nt;
+    int rc = alloc_table(c, capacity, &nt);
+    if (rc) return rc;
+    L3D_CUDA(cudaMemsetAsync(c->counters, 0, sizeof(unsigned), c->stream), "reset counter");
+    cudaError_t e = l3d_launch_cloud_rebin(c->t, nt, cell, c->counters, c->err, c->stream);
+    c->launches++;
+    if (e != cudaSuccess) {
+        free_table(nt);
+        return cuda_fail(e, "rebin launch");
+    }
+    L3D_CUDA(cudaStreamSynchronize(c->stream), "synchronize");
+    free_table(c->t);
+    c->t = nt;
+    c->cell = cell;
+    return L3D_OK;
+}
+
+/* Grows the table (grow(), point-accumulator.ts:77-79) until `extra` new cells keep the load
+ * at or under 60 %. */
+int cloud_reserve(l3d_cloud* c, long long extra) {
+    unsigned used = 0;
+    int rc = cloud_state(c, &used);
+    if (rc) return rc;
+    long long cap = c->t.capacity;
+    while (((long long)used + extra) * 10 > cap * 6) cap *= 2;
+    if (cap > (1ll << 30)) return fail(L3D_ENOMEM, "point table would exceed 2^30 slots");
+    if (cap == c->t.capacity) return L3D_OK;
+    return cloud_rebuild(c, (int)cap, c->cell);
+}
+
+template <typename T>
+int ensure_upload(T** p, size_t* cap, size_t n, cudaStream_t stream, const char* what) {
+    if (*cap >= n) return L3D_OK;
+    cudaStreamSynchronize(stream);
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    L3D_CUDA(cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)), what);
+    *cap = n;
+    return L3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int l3d_cloud_create(double cell, void* stream, l3d_cloud** out) {
+    if (!out) return fail(L3D_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!(cell > 0.0)) return fail(L3D_EINVAL, "cell must be positive");
+    l3d_cloud* c = new (std::nothrow) l3d_cloud();
+    if (!c) return fail(L3D_ENOMEM, "host allocation failed");
+    c->cell = cell;
+    auto cleanup = [&](int rc) {
+        l3d_cloud_destroy(c);
+        return rc;
+    };
+    cudaError_t e;
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "stream creation"));
+        c->own_stream = true;
+    }
+    if ((e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "event creation"));
+    if ((e = cudaMalloc(&c->counters, 2 * sizeof(unsigned))) != cudaSuccess ||
+        (e = cudaMalloc(&c->err, sizeof(int))) != cudaSuccess)
+        return cleanup(cuda_fail(e, "counter allocation"));
+    if ((e = cudaMemsetAsync(c->counters, 0, 2 * sizeof(unsigned), c->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->err, 0, sizeof(int), c->stream)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "counter clear"));
+    int rc = alloc_table(c, 1 << 16, &c->t);
+    if (rc) return cleanup(rc);
+    *out = c;
+    return L3D_OK;
+}
+
+int l3d_cloud_add(l3d_cloud* c, const l3d_stereo* src, const uint32_t* packed, int32_t width,
+                  int32_t height, const l3d_view* view, const uint8_t* thumb_rgb, int32_t thumb_w,
+                  int32_t thumb_h) {
+    if (!c || !view || !thumb_rgb) return fail(L3D_EINVAL, "NULL handle, view or thumbnail");
+    if ((src == nullptr) == (packed == nullptr))
+        return fail(L3D_EINVAL, "give exactly one of a stereo handle or a packed map");
+    if (thumb_w <= 0 || thumb_h <= 0) return fail(L3D_EINVAL, "thumbnail size must be positive");
+    if (!(view->intrinsics.fx != 0.0) || !(view->intrinsics.fy != 0.0))
+        return fail(L3D_EINVAL, "zero focal length");
+    /* a stereo handle's filtered map has the size of the view it was filtered for */
+    const int W = src ? src->Wv[src->filtered_ref] : width;
+    const int H = src ? src->Hv[src->filtered_ref] : height;
+    if (W <= 0 || H <= 0) return fail(L3D_EINVAL, "depth map size must be positive");
+    int rc = cloud_reserve(c, (long long)W * H);
+    if (rc) return rc;
+    const size_t tb = (size_t)thumb_w * thumb_h * 3;
+    if ((rc = ensure_upload(&c->thumb, &c->thumb_cap, tb, c->stream, "thumbnail buffer"))) return rc;
+    L3D_CUDA(cudaMemcpyAsync(c->thumb, thumb_rgb, tb, cudaMemcpyHostToDevice, c->stream), "thumbnail upload");
+    const uint32_t* map;
+    if (src) {
+        L3D_CUDA(cudaEventRecord(src->done, src->stream), "event record");
+        L3D_CUDA(cudaStreamWaitEvent(c->stream, src->done, 0), "stream wait");
+        map = src->filtered;
+    } else {
+        if ((rc = ensure_upload(&c->map, &c->map_cap, (size_t)W * H, c->stream, "map buffer"))) return rc;
+        L3D_CUDA(cudaMemcpyAsync(c->map, packed, (size_t)W * H * 4, cudaMemcpyHostToDevice, c->stream),
+                 "map upload");
+        map = c->map;
+    }
+    L3dCloudView v;
+    std::memset(&v, 0, sizeof(v));
+    v.k[0] = view->intrinsics.fx;
+    v.k[1] = view->intrinsics.fy;
+    v.k[2] = view->intrinsics.cx;
+    v.k[3] = view->intrinsics.cy;
+    for (int i = 0; i < 9; i++) v.R[i] = view->pose.R[i];
+    for (int i = 0; i < 3; i++) v.t[i] = view->pose.t[i];
+    v.tw = thumb_w;
+    v.th = thumb_h;
+    cudaError_t e = l3d_launch_cloud_add_map(c->t, c->cell, map, W, H, v, c->thumb, c->counters,
+                                             c->err, c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "point add launch");
+    if (src) {
+        /* the stereo handle's later work (the next filter) waits for this read */
+        L3D_CUDA(cudaEventRecord(c->done, c->stream), "event record");
+        L3D_CUDA(cudaStreamWaitEvent(src->stream, c->done, 0), "stream wait");
+    }
+    return L3D_OK;
+}
+
+int l3d_cloud_add_points(l3d_cloud* c, int64_t n, const double* samples) {
+    if (!c) return fail(L3D_EINVAL, "NULL handle");
+    if (n < 0 || (n > 0 && !samples)) return fail(L3D_EINVAL, "bad sample list");
+    if (n == 0) return L3D_OK;
+    int rc = cloud_reserve(c, n);
+    if (rc) return rc;
+    if ((rc = ensure_upload(&c->pts, &c->pts_cap, (size_t)n * 9, c->stream, "sample buffer"))) return rc;
+    L3D_CUDA(cudaMemcpyAsync(c->pts, samples, (size_t)n * 9 * 8, cudaMemcpyHostToDevice, c->stream),
+             "sample upload");
+    cudaError_t e = l3d_launch_cloud_add_points(c->t, c->cell, c->pts, n, c->counters, c->err, c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "point add launch");
+    return L3D_OK;
+}
+
+int l3d_cloud_coarsen(l3d_cloud* c, double factor) {
+    if (!c) return fail(L3D_EINVAL, "NULL handle");
+    if (!(factor > 0.0)) return fail(L3D_EINVAL, "factor must be positive");
+    int rc = cloud_state(c, nullptr);
+    if (rc) return rc;
+    return cloud_rebuild(c, c->t.capacity, c->cell * factor);
+}
+
+int l3d_cloud_size(l3d_cloud* c, int64_t* size) {
+    if (!c || !size) return fail(L3D_EINVAL, "NULL argument");
+    unsigned used = 0;
+    int rc = cloud_state(c, &used);
+    if (rc) return rc;
+    *size = used;
+    return L3D_OK;
+}
+
+int l3d_cloud_cell(const l3d_cloud* c, double* cell) {
+    if (!c || !cell) return fail(L3D_EINVAL, "NULL argument");
+    *cell = c->cell;
+    return L3D_OK;
+}
+
+int l3d_cloud_read(l3d_cloud* c, int32_t min_support, int64_t capacity, int64_t* count,
+                   float* positions, float* normals, uint8_t* colors, uint16_t* support,
+                   int32_t* cells) {
+    if (!c || !count) return fail(L3D_EINVAL, "NULL handle or count");
+    unsigned used = 0;
+    int rc = cloud_state(c, &used);
+    if (rc) return rc;
+    const size_t n = std::max<unsigned>(used, 1u);
+    float* dpos = nullptr;
+    float* dnrm = nullptr;
+    uint8_t* dcol = nullptr;
+    uint16_t* dsup = nullptr;
+    unsigned long long* dkey = nullptr;
+    cudaError_t e;
+    auto cleanup = [&]() {
+        cudaFree(dpos);
+        cudaFree(dnrm);
+        cudaFree(dcol);
+        cudaFree(dsup);
+        cudaFree(dkey);
+    };
+    if ((e = cudaMalloc(&dpos, n * 12)) != cudaSuccess || (e = cudaMalloc(&dnrm, n * 12)) != cudaSuccess ||
+        (e = cudaMalloc(&dcol, n * 3)) != cudaSuccess || (e = cudaMalloc(&dsup, n * 2)) != cudaSuccess ||
+        (e = cudaMalloc(&dkey, n * 8)) != cudaSuccess) {
+        cleanup();
+        return cuda_fail(e, "read buffers");
+    }
+    unsigned total = 0;
+    if ((e = cudaMemsetAsync(c->counters + 1, 0, sizeof(unsigned), c->stream)) != cudaSuccess ||
+        (e = l3d_launch_cloud_emit(c->t, (unsigned)std::max(min_support, 0), c->counters + 1, dpos,
+                                   dnrm, dcol, dsup, dkey, c->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&total, c->counters + 1, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             c->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
+        cleanup();
+        return cuda_fail(e, "point read");
+    }
+    c->launches++;
+    *count = total;
+    if (!positions && !normals && !colors && !support && !cells) {
+        cleanup();
+        return L3D_OK;
+    }
+    if (capacity < (int64_t)total) {
+        cleanup();
+        return fail(L3D_EINVAL, "output holds %lld points, the cloud has %u", (long long)capacity, total);
+    }
+    std::vector<float> hp(total * 3), hn(total * 3);
+    std::vector<uint8_t> hc(total * 3);
+    std::vector<uint16_t> hs(total);
+    std::vector<unsigned long long> hk(total);
+    if (total &&
+        ((e = cudaMemcpy(hp.data(), dpos, total * 12, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+         (e = cudaMemcpy(hn.data(), dnrm, total * 12, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+         (e = cudaMemcpy(hc.data(), dcol, total * 3, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+         (e = cudaMemcpy(hs.data(), dsup, total * 2, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+         (e = cudaMemcpy(hk.data(), dkey, total * 8, cudaMemcpyDeviceToHost)) != cudaSuccess)) {
+        cleanup();
+        return cuda_fail(e, "point download");
+    }
+    cleanup();
+    /* cells in ascending packed order: z, then y, then x */
+    std::vector<uint32_t> order(total);
+    for (uint32_t i = 0; i < total; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return hk[a] < hk[b]; });
+    const long long bias = 1 << 20;
+    for (uint32_t j = 0; j < total; j++) {
+        const uint32_t i = order[j];
+        for (int q = 0; q < 3; q++) {
+            if (positions) positions[j * 3 + q] = hp[i * 3 + q];
+            if (normals) normals[j * 3 + q] = hn[i * 3 + q];
+            if (colors) colors[j * 3 + q] = hc[i * 3 + q];
+            if (cells) cells[j * 3 + q] = (int32_t)((long long)((hk[i] >> (21 * q)) & 0x1FFFFFull) - bias);
+        }
+        if (support) support[j] = hs[i];
+    }
+    return L3D_OK;
+}
+
+int64_t l3d_cloud_launches(const l3d_cloud* c) { return c ? c->launches : -1; }
+
+void l3d_cloud_destroy(l3d_cloud* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_table(c->t);
+    cudaFree(c->counters);
+    cudaFree(c->err);
+    cudaFree(c->thumb);
+    cudaFree(c->map);
+    cudaFree(c->pts);
+    if (c->done) cudaEventDestroy(c->done);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+}  // extern "C"

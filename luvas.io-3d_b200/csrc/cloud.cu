@@ -1,0 +1,232 @@
+/*
+ * Dense point cloud: packed depth maps fused into cell-averaged points on the device.
+ *
+ * frontend/src/app/vision/fusion/depth-fusion.ts:42-74 decodes every valid sample of a filtered
+ * depth map into a world point, a world normal and a thumbnail colour, and
+ * frontend/src/app/vision/fusion/point-accumulator.ts:16-147 averages them per cell of a grid
+ * (open-addressing hash on the integer cell, growth at 60 % load, coarsening that re-bins cell
+ * means into a larger cell).  Here one thread decodes one pixel and adds it to a device hash
+ * table with atomics:
+ *   - keys: the integer cell packed into 63 bits (21 bits per axis, biased by 2^20), claimed with
+ *     atomicCAS on linear probes from the reference's hash; cells beyond +-2^20 set an error flag;
+ *   - sums: nine FP64 sums per slot (position, normal, colour), added with FP64 atomics (the
+ *     reference keeps f32 sums; FP64 makes the result independent of the order of the adds up
+ *     to rounding at the last bit);
+ *   - counts: u32 per slot; `used`: the number of claimed slots.
+ * Decoding and the world transform run in FP64 in the reference's operation order.  Probing is
+ * bounded by the table size (the host keeps the load under 60 %, so a free slot always exists);
+ * a probe that runs out sets an error flag instead of looping.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "l3d_fmath.h"
+#include "l3d_internal.h"
+
+namespace {
+
+constexpr unsigned long long kEmpty = ~0ull;
+constexpr int kBias = 1 << 20;
+
+__device__ __forceinline__ uint32_t cell_hash(int x, int y, int z) {
+    return ((uint32_t)x * 73856093u) ^ ((uint32_t)y * 19349663u) ^ ((uint32_t)z * 83492791u);
+}
+
+__device__ __forceinline__ bool pack_key(double fx, double fy, double fz, unsigned long long* key,
+                                         int* ix, int* iy, int* iz) {
+    if (!(fabs(fx) < (double)kBias && fabs(fy) < (double)kBias && fabs(fz) < (double)kBias))
+        return false;
+    *ix = (int)fx;
+    *iy = (int)fy;
+    *iz = (int)fz;
+    *key = (unsigned long long)(*ix + kBias) | ((unsigned long long)(*iy + kBias) << 21) |
+           ((unsigned long long)(*iz + kBias) << 42);
+    return true;
+}
+
+/* Slot of the cell (claimed when new), or -1 after setting an error flag. */
+__device__ int claim(const L3dCloudTable& t, double cx, double cy, double cz, unsigned* used,
+                     int* err) {
+    unsigned long long key;
+    int ix, iy, iz;
+    if (!pack_key(floor(cx), floor(cy), floor(cz), &key, &ix, &iy, &iz)) {
+        atomicOr(err, L3D_CLOUD_ERR_RANGE);
+        return -1;
+    }
+    const unsigned mask = (unsigned)t.capacity - 1u;
+    unsigned slot = cell_hash(ix, iy, iz) & mask;
+    for (int probe = 0; probe < t.capacity; probe++) {
+        const unsigned long long k = __ldcg(t.keys + slot);
+        if (k == key) return (int)slot;
+        if (k == kEmpty) {
+            const unsigned long long prev = atomicCAS(t.keys + slot, kEmpty, key);
+            if (prev == kEmpty) {
+                atomicAdd(used, 1u);
+                return (int)slot;
+            }
+            if (prev == key) return (int)slot;
+        }
+        slot = (slot + 1u) & mask;
+    }
+    atomicOr(err, L3D_CLOUD_ERR_FULL);
+    return -1;
+}
+
+__device__ __forceinline__ void accumulate(const L3dCloudTable& t, int slot, const double* v,
+                                           unsigned n) {
+    double* s = t.sums + (size_t)slot * 9;
+#pragma unroll
+    for (int i = 0; i < 9; i++) atomicAdd(s + i, v[i]);
+    atomicAdd(t.counts + slot, n);
+}
+
+/* addDepthMap (depth-fusion.ts:42-74) for one pixel; unpackDepthSample (depth-maps.ts:66-85). */
+__global__ void k_cloud_add_map(const L3dCloudTable t, double cell, const uint32_t* __restrict__ packed,
+                                int W, int H, const L3dCloudView v, const uint8_t* __restrict__ rgb,
+                                unsigned* used, int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * H) return;
+    const uint32_t value = __ldg(packed + i);
+    if (value == 0u) return;
+    const double d = (double)l3d_f16_to_f32(value & 0xffffu);
+    if (!(d > 0.0)) return;
+    const int x = i % W, y = i / W;
+    const double ex = ((double)((value >> 16) & 63u) / 63.0) * 2.0 - 1.0;
+    const double ey = ((double)((value >> 22) & 63u) / 63.0) * 2.0 - 1.0;
+    double nx = ex, ny = ey;
+    const double nz = 1.0 - fabs(ex) - fabs(ey);
+    if (nz < 0.0) {
+        nx = (1.0 - fabs(ey)) * (ex >= 0.0 ? 1.0 : -1.0);
+        ny = (1.0 - fabs(ex)) * (ey >= 0.0 ? 1.0 : -1.0);
+    }
+    double len = sqrt(nx * nx + ny * ny + nz * nz);
+    if (!(len != 0.0)) len = 1.0;
+    nx /= len;
+    ny /= len;
+    const double nzn = nz / len;
+    /* fromCamera (camera.ts:57-59): R^T (x_cam - t) */
+    const double* R = v.R;
+    const double a0 = ((x - v.k[2]) / v.k[0]) * d - v.t[0];
+    const double a1 = ((y - v.k[3]) / v.k[1]) * d - v.t[1];
+    const double a2 = d - v.t[2];
+    double p[9];
+    p[0] = R[0] * a0 + R[3] * a1 + R[6] * a2;
+    p[1] = R[1] * a0 + R[4] * a1 + R[7] * a2;
+    p[2] = R[2] * a0 + R[5] * a1 + R[8] * a2;
+    p[3] = R[0] * nx + R[3] * ny + R[6] * nzn;
+    p[4] = R[1] * nx + R[4] * ny + R[7] * nzn;
+    p[5] = R[2] * nx + R[5] * ny + R[8] * nzn;
+    const double sx = (double)v.tw / W, sy = (double)v.th / H;
+    const int tx = min(v.tw - 1, (int)floor((x + 0.5) * sx));
+    const int ty = min(v.th - 1, (int)floor((y + 0.5) * sy));
+    const uint8_t* c = rgb + ((size_t)ty * v.tw + tx) * 3;
+    p[6] = c[0];
+    p[7] = c[1];
+    p[8] = c[2];
+    const int slot = claim(t, p[0] / cell, p[1] / cell, p[2] / cell, used, err);
+    if (slot >= 0) accumulate(t, slot, p, 1u);
+}
+
+/* PointAccumulator.add (point-accumulator.ts:29-56) of n samples of 9 doubles. */
+__global__ void k_cloud_add_points(const L3dCloudTable t, double cell, const double* __restrict__ pts,
+                                   long long n, unsigned* used, int* err) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double p[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) p[j] = pts[i * 9 + j];
+    const int slot = claim(t, p[0] / cell, p[1] / cell, p[2] / cell, used, err);
+    if (slot >= 0) accumulate(t, slot, p, 1u);
+}
+
+/* rebuild (point-accumulator.ts:89-111): every occupied slot re-binned by its mean position
+ * into the table `to` with cell size `cell`. */
+__global__ void k_cloud_rebin(const L3dCloudTable from, const L3dCloudTable to, double cell,
+                              unsigned* used, int* err) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= from.capacity || from.keys[s] == kEmpty) return;
+    const unsigned n = from.counts[s];
+    const double* src = from.sums + (size_t)s * 9;
+    double p[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) p[j] = src[j];
+    const double dn = (double)n;
+    const int slot = claim(to, p[0] / dn / cell, p[1] / dn / cell, p[2] / dn / cell, used, err);
+    if (slot >= 0) accumulate(to, slot, p, n);
+}
+
+/* cloud(minSupport) (point-accumulator.ts:114-143): averaged points of the slots with enough
+ * support, in arbitrary order, with their cell keys (the host orders them). */
+__global__ void k_cloud_emit(const L3dCloudTable t, unsigned min_support, unsigned* count,
+                             float* pos, float* nrm, uint8_t* col, uint16_t* support,
+                             unsigned long long* keys) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= t.capacity) return;
+    const unsigned long long key = t.keys[s];
+    const unsigned n = t.counts[s];
+    if (key == kEmpty || n < min_support) return;
+    const unsigned o = atomicAdd(count, 1u);
+    const double* sm = t.sums + (size_t)s * 9;
+    const double dn = (double)n;
+    for (int j = 0; j < 3; j++) pos[o * 3 + j] = (float)(sm[j] / dn);
+    double len = sqrt(sm[3] * sm[3] + sm[4] * sm[4] + sm[5] * sm[5]);
+    if (!(len != 0.0)) len = 1.0;
+    for (int j = 0; j < 3; j++) nrm[o * 3 + j] = (float)(sm[3 + j] / len);
+    for (int j = 0; j < 3; j++) {
+        /* Uint8Array store: truncation, then modulo 256 */
+        double c = trunc(sm[6 + j] / dn);
+        c = c - 256.0 * floor(c / 256.0);
+        col[o * 3 + j] = (uint8_t)c;
+    }
+    support[o] = (uint16_t)min(n, 65535u);
+    keys[o] = key;
+}
+
+__global__ void k_cloud_clear(L3dCloudTable t) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= t.capacity) return;
+    t.keys[s] = kEmpty;
+    t.counts[s] = 0u;
+    double* sm = t.sums + (size_t)s * 9;
+#pragma unroll
+    for (int j = 0; j < 9; j++) sm[j] = 0.0;
+}
+
+inline unsigned blocks_for(long long n) { return (unsigned)((n + 255) / 256); }
+
+}  // namespace
+
+cudaError_t l3d_launch_cloud_clear(const L3dCloudTable& t, cudaStream_t stream) {
+    k_cloud_clear<<<blocks_for(t.capacity), 256, 0, stream>>>(t);
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_cloud_add_map(const L3dCloudTable& t, double cell, const uint32_t* packed,
+                                     int W, int H, const L3dCloudView& v, const uint8_t* rgb,
+                                     unsigned* used, int* err, cudaStream_t stream) {
+    if ((long long)W * H == 0) return cudaSuccess;
+    k_cloud_add_map<<<blocks_for((long long)W * H), 256, 0, stream>>>(t, cell, packed, W, H, v, rgb,
+                                                                      used, err);
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_cloud_add_points(const L3dCloudTable& t, double cell, const double* pts,
+                                        long long n, unsigned* used, int* err, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    k_cloud_add_points<<<blocks_for(n), 256, 0, stream>>>(t, cell, pts, n, used, err);
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_cloud_rebin(const L3dCloudTable& from, const L3dCloudTable& to, double cell,
+                                   unsigned* used, int* err, cudaStream_t stream) {
+    k_cloud_rebin<<<blocks_for(from.capacity), 256, 0, stream>>>(from, to, cell, used, err);
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_cloud_emit(const L3dCloudTable& t, unsigned min_support, unsigned* count,
+                                  float* pos, float* nrm, uint8_t* col, uint16_t* support,
+                                  unsigned long long* keys, cudaStream_t stream) {
+    k_cloud_emit<<<blocks_for(t.capacity), 256, 0, stream>>>(t, min_support, count, pos, nrm, col,
+                                                             support, keys);
+    return cudaGetLastError();
+}

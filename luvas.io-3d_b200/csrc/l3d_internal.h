@@ -232,6 +232,37 @@ cudaError_t l3d_launch_tsdf_depth(const L3dTsdfGrid& g, const L3dTsdfView& v, co
                                   float* grad_tsdf_in, float* grad_weight_in, int q8,
                                   cudaStream_t stream);
 
+/* ---- dense point cloud (cloud.cu) ---- */
+
+struct L3dCloudTable {
+    unsigned long long* keys;  /* capacity packed cells, ~0 = empty */
+    double* sums;              /* capacity x 9: position, normal, colour sums */
+    unsigned* counts;          /* capacity */
+    int capacity;              /* power of two */
+};
+
+/* One view of addDepthMap in FP64: fx fy cx cy, R (world -> camera), t, thumbnail size. */
+struct L3dCloudView {
+    double k[4];
+    double R[9];
+    double t[3];
+    int tw, th;
+};
+
+enum { L3D_CLOUD_ERR_RANGE = 1, L3D_CLOUD_ERR_FULL = 2 };
+
+cudaError_t l3d_launch_cloud_clear(const L3dCloudTable& t, cudaStream_t stream);
+cudaError_t l3d_launch_cloud_add_map(const L3dCloudTable& t, double cell, const uint32_t* packed,
+                                     int W, int H, const L3dCloudView& v, const uint8_t* rgb,
+                                     unsigned* used, int* err, cudaStream_t stream);
+cudaError_t l3d_launch_cloud_add_points(const L3dCloudTable& t, double cell, const double* pts,
+                                        long long n, unsigned* used, int* err, cudaStream_t stream);
+cudaError_t l3d_launch_cloud_rebin(const L3dCloudTable& from, const L3dCloudTable& to, double cell,
+                                   unsigned* used, int* err, cudaStream_t stream);
+cudaError_t l3d_launch_cloud_emit(const L3dCloudTable& t, unsigned min_support, unsigned* count,
+                                  float* pos, float* nrm, uint8_t* col, uint16_t* support,
+                                  unsigned long long* keys, cudaStream_t stream);
+
 /* Sets the calling thread's l3d_last_error() message (capi.cu). */
 void l3d_set_error(const char* msg);
 

@@ -155,6 +155,15 @@ SIGNATURES = [
     ("l3d_tsdf_destroy", None, [_P]),
     ("l3d_tsdf_integrate_noalloc", C.c_int, [C.POINTER(TsdfDesc), _P, _P, _P,
                                              C.POINTER(IntegrationView), _P, _P, _P]),
+    ("l3d_cloud_create", C.c_int, [C.c_double, _P, C.POINTER(_P)]),
+    ("l3d_cloud_add", C.c_int, [_P, _P, _P, _I, _I, C.POINTER(View), _P, _I, _I]),
+    ("l3d_cloud_add_points", C.c_int, [_P, C.c_int64, _P]),
+    ("l3d_cloud_coarsen", C.c_int, [_P, C.c_double]),
+    ("l3d_cloud_size", C.c_int, [_P, C.POINTER(C.c_int64)]),
+    ("l3d_cloud_cell", C.c_int, [_P, C.POINTER(C.c_double)]),
+    ("l3d_cloud_read", C.c_int, [_P, _I, C.c_int64, C.POINTER(C.c_int64), _P, _P, _P, _P, _P]),
+    ("l3d_cloud_launches", C.c_int64, [_P]),
+    ("l3d_cloud_destroy", None, [_P]),
     ("l3d_ncc_forward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P]),
     ("l3d_ncc_backward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P, _P, _P, _P]),
     ("l3d_tsdf_forward_depth", C.c_int, [_P, C.POINTER(IntegrationView), _I, _I, _P, _P, _P, _P, _P,

@@ -73,6 +73,18 @@ def load():
             getattr(lib, pre + "_tsdf_integrate").argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView),
                                                               P, P, P, C.c_int32]
         lib.orc_tsdf_visible.argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView), P]
+        lib.orc_cloud_create.restype = P
+        lib.orc_cloud_create.argtypes = [C.c_double]
+        lib.orc_cloud_destroy.argtypes = [P]
+        lib.orc_cloud_add_point.argtypes = [P, P]
+        lib.orc_cloud_add_map.argtypes = [P, P, C.c_int32, C.c_int32, P, P, C.c_int32, C.c_int32]
+        lib.orc_cloud_coarsen.argtypes = [P, C.c_double]
+        lib.orc_cloud_size.restype = C.c_int32
+        lib.orc_cloud_size.argtypes = [P]
+        lib.orc_cloud_cell.restype = C.c_double
+        lib.orc_cloud_cell.argtypes = [P]
+        lib.orc_cloud_read.restype = C.c_int32
+        lib.orc_cloud_read.argtypes = [P, C.c_int32, P, P, P, P, P]
         lib.orc64_ncc_grad.argtypes = [C.POINTER(StereoArgs), P, P, P, P, P, P, P, P]
         lib.orc64_tsdf_depth.argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView)] + [P] * 11 + [C.c_int32]
         lib.orc_pack_sample.restype = C.c_uint32
@@ -274,6 +286,52 @@ class NccGrad:
                                    cells.ctypes.data)
         assert rc == 0
         return cost, margin, cells
+
+
+class Cloud:
+    """PointAccumulator + addDepthMap restated (oracle/cloud.cpp)."""
+
+    def __init__(self, cell: float):
+        self._c = load().orc_cloud_create(float(cell))
+
+    def __del__(self):
+        if getattr(self, "_c", None):
+            load().orc_cloud_destroy(self._c)
+            self._c = None
+
+    def add(self, x, y, z, nx, ny, nz, r, g, b) -> None:
+        p = np.array([x, y, z, nx, ny, nz, r, g, b], dtype=np.float64)
+        load().orc_cloud_add_point(self._c, p.ctypes.data)
+
+    def add_map(self, packed, view, thumb) -> None:
+        """packed (H, W) u32; view a StereoView; thumb (th, tw, 3) uint8."""
+        pk = np.ascontiguousarray(packed, dtype=np.uint32)
+        v = _views_array([view])[0].copy()
+        rgb = np.ascontiguousarray(thumb, dtype=np.uint8)
+        load().orc_cloud_add_map(self._c, pk.ctypes.data, pk.shape[1], pk.shape[0], v.ctypes.data,
+                                 rgb.ctypes.data, rgb.shape[1], rgb.shape[0])
+
+    def coarsen(self, factor: float = 1.4) -> None:
+        load().orc_cloud_coarsen(self._c, float(factor))
+
+    @property
+    def size(self) -> int:
+        return int(load().orc_cloud_size(self._c))
+
+    @property
+    def cell(self) -> float:
+        return float(load().orc_cloud_cell(self._c))
+
+    def cloud(self, min_support: int = 1) -> dict:
+        lib = load()
+        n = lib.orc_cloud_read(self._c, int(min_support), None, None, None, None, None)
+        out = {"positions": np.zeros((n, 3), np.float32), "normals": np.zeros((n, 3), np.float32),
+               "colors": np.zeros((n, 3), np.uint8), "support": np.zeros(n, np.uint16),
+               "cells": np.zeros((n, 3), np.int32)}
+        lib.orc_cloud_read(self._c, int(min_support), out["positions"].ctypes.data,
+                           out["normals"].ctypes.data, out["colors"].ctypes.data,
+                           out["support"].ctypes.data, out["cells"].ctypes.data)
+        return out
 
 
 def tsdf_depth(desc, view_kw: dict, packed, depth, tsdf_in, weight_in, grad_tsdf=None,

@@ -122,6 +122,24 @@ int orc64_tsdf_depth(const orc_tsdf_desc* d, const orc_tsdf_view* v, const uint3
                      const double* grad_weight_out, double* grad_depth, double* grad_tsdf_in,
                      double* grad_weight_in, int32_t threads);
 
+/* ---- dense point cloud (cloud.cpp): depth-fusion.ts addDepthMap + PointAccumulator ---- */
+typedef struct orc_cloud orc_cloud;
+orc_cloud* orc_cloud_create(double cell);
+void orc_cloud_destroy(orc_cloud* c);
+/* PointAccumulator.add of one sample: x y z nx ny nz r g b */
+void orc_cloud_add_point(orc_cloud* c, const double* p9);
+/* addDepthMap: packed width * height map, view = 16 doubles (fx fy cx cy | R | t), thumbnail
+ * rgb (tw * th * 3 bytes) */
+void orc_cloud_add_map(orc_cloud* c, const uint32_t* packed, int32_t width, int32_t height,
+                       const double* view, const uint8_t* rgb, int32_t tw, int32_t th);
+void orc_cloud_coarsen(orc_cloud* c, double factor);
+int32_t orc_cloud_size(const orc_cloud* c);
+double orc_cloud_cell(const orc_cloud* c);
+/* cloud(minSupport) in slot order; returns the point count, fills the outputs (and each point's
+ * integer cell, 3 int32) when pos is not NULL */
+int32_t orc_cloud_read(const orc_cloud* c, int32_t min_support, float* pos, float* nrm,
+                       uint8_t* col, uint16_t* support, int32_t* cells);
+
 /* Packing helpers (depth-packing.wgsl.ts:3-33) and primitives for unit tests. */
 uint32_t orc_pack_sample(float depth, float nx, float ny, float nz, float cost);
 float orc_unpack_depth(uint32_t packed);
