@@ -323,6 +323,48 @@ int l3d_cloud_read(l3d_cloud* c, int32_t min_support, int64_t capacity, int64_t*
 int64_t l3d_cloud_launches(const l3d_cloud* c);
 void l3d_cloud_destroy(l3d_cloud* c);
 
+/* ---- Surface extraction: extractSurface (fusion/surface-nets.ts:47-174), computeNormals and
+ * removeSmallComponents (fusion/mesh.ts:9-87), BrickGrid (fusion/tsdf-volume.ts:13-65) ----
+ *
+ * The mesh equals the reference's: vertices in its append order (one per sign-changing cell in
+ * brick, voxel order), triangles in (brick, voxel, axis) order, positions computed in FP64 and
+ * rounded to f32, normals summed in f32 in face order.  Vector lengths use sqrt(x^2+y^2+z^2)
+ * where the reference calls Math.hypot. */
+typedef struct l3d_mesh l3d_mesh;
+
+/* SdfBricks (surface-nets.ts:4-12), host arrays: lookup over dims[0]*dims[1]*dims[2] grid
+ * cells (pool brick or -1), tsdf and weight of `bricks` pool bricks, voxel b*512 + x + 8y + 64z. */
+typedef struct {
+    double origin[3];
+    double voxel;
+    int32_t dims[3];
+    const int32_t* lookup;
+    const float* tsdf;
+    const float* weight;
+    int64_t bricks;
+} l3d_sdf_bricks;
+
+/* extractSurface(volume, minWeight) of a host volume. */
+int l3d_extract_surface(const l3d_sdf_bricks* volume, double min_weight, l3d_mesh** out);
+/* extractSurface of a TSDF handle's volume in place (brick pool: the grid spans the pool's
+ * brick coordinates; dense grid: bricks in dense brick order, voxels outside dims missing). */
+int l3d_tsdf_extract_surface(l3d_tsdf* t, double min_weight, l3d_mesh** out);
+int l3d_mesh_counts(const l3d_mesh* m, int64_t* vertices, int64_t* indices);
+/* Host copies: positions and normals 3 floats per vertex, indices 3 per triangle (any NULL). */
+int l3d_mesh_read(const l3d_mesh* m, float* positions, float* normals, uint32_t* indices);
+/* removeSmallComponents (mesh.ts:37-87): a new mesh without the connected components of fewer
+ * than max(min_faces, faces * fraction) faces, vertices renumbered in order of first use. */
+int l3d_mesh_remove_small_components(const l3d_mesh* m, double fraction, int32_t min_faces,
+                                     l3d_mesh** out);
+int64_t l3d_mesh_launches(const l3d_mesh* m);
+void l3d_mesh_destroy(l3d_mesh* m);
+/* new BrickGrid(origin, voxel, extent), mark(point, radius) for n host points (3 floats each),
+ * build(): dims, the brick count, coords (4 int32 per brick, grid order) and lookup (one per grid
+ * cell); with coords and lookup NULL only dims and count are returned. */
+int l3d_brick_grid_build(const double origin[3], double voxel, const double extent[3],
+                         const float* points, int64_t n, double radius, int32_t dims[3],
+                         int32_t* count, int32_t* coords, int32_t* lookup);
+
 /* ---- Differentiation (no reference counterpart) ----
  *
  * The reference has no gradients: its WGSL kernels only evaluate costs.  These entry points give

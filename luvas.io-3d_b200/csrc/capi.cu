@@ -2019,3 +2019,368 @@ void l3d_cloud_destroy(l3d_cloud* c) {
 }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------ surface extraction ----- */
+
+struct l3d_mesh {
+    float* pos = nullptr;
+    float* nrm = nullptr;
+    uint32_t* idx = nullptr;
+    long long nv = 0, ni = 0;
+    long long launches = 0;
+};
+
+namespace {
+
+/* Device buffers freed when the holder goes out of scope. */
+struct DevBufs {
+    std::vector<void*> ptrs;
+    ~DevBufs() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    cudaError_t get(T** p, size_t count) {
+        *p = nullptr;
+        cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) ptrs.push_back(*p);
+        return e;
+    }
+};
+
+int read_u32(const uint32_t* dev, uint32_t* host, cudaStream_t s) {
+    L3D_CUDA(cudaMemcpyAsync(host, dev, 4, cudaMemcpyDeviceToHost, s), "read count");
+    L3D_CUDA(cudaStreamSynchronize(s), "synchronize");
+    return L3D_OK;
+}
+
+void mesh_free(l3d_mesh* m) {
+    if (!m) return;
+    cudaFree(m->pos);
+    cudaFree(m->nrm);
+    cudaFree(m->idx);
+    delete m;
+}
+
+/* extractSurface (surface-nets.ts:47-174) + computeNormals (mesh.ts:9-31) of a volume view with
+ * `bricks` bricks. */
+int extract_mesh(const L3dSdfView& v, long long bricks, cudaStream_t s, l3d_mesh** out) {
+    const long long cells = bricks * 512;
+    if (cells >= (1ll << 31)) return fail(L3D_EINVAL, "volume too large for surface extraction");
+    DevBufs tmp;
+    uint32_t *flag, *base, *qcount, *qbase, *scratch, *total;
+    int32_t* cell_vertex;
+    L3D_CUDA(tmp.get(&flag, cells), "surface buffers");
+    L3D_CUDA(tmp.get(&base, cells), "surface buffers");
+    L3D_CUDA(tmp.get(&qcount, cells), "surface buffers");
+    L3D_CUDA(tmp.get(&qbase, cells), "surface buffers");
+    L3D_CUDA(tmp.get(&cell_vertex, cells), "surface buffers");
+    L3D_CUDA(tmp.get(&scratch, l3d_scan_scratch(std::max(cells, 1ll)) / 4 + 1), "scan scratch");
+    L3D_CUDA(tmp.get(&total, 2), "scan total");
+    l3d_mesh* m = new (std::nothrow) l3d_mesh();
+    if (!m) return fail(L3D_ENOMEM, "host allocation failed");
+    auto bail = [&](int rc) {
+        mesh_free(m);
+        return rc;
+    };
+    cudaError_t e;
+    uint32_t nv = 0, nq = 0;
+    if ((e = l3d_launch_sn_flag(v, cells, flag, s)) != cudaSuccess ||
+        (e = l3d_scan_exclusive(flag, base, cells, scratch, total, s)) != cudaSuccess)
+        return bail(cuda_fail(e, "surface vertices"));
+    int rc = read_u32(total, &nv, s);
+    if (rc) return bail(rc);
+    double* pos_d;
+    if ((e = tmp.get(&pos_d, (size_t)nv * 3)) != cudaSuccess ||
+        (e = cudaMalloc(&m->pos, std::max<size_t>(nv, 1) * 12)) != cudaSuccess ||
+        (e = cudaMalloc(&m->nrm, std::max<size_t>(nv, 1) * 12)) != cudaSuccess)
+        return bail(cuda_fail(e, "vertex buffers"));
+    if ((e = l3d_launch_sn_vertex(v, cells, flag, base, cell_vertex, pos_d, m->pos, s)) != cudaSuccess ||
+        (e = l3d_launch_sn_count(v, cells, cell_vertex, qcount, s)) != cudaSuccess ||
+        (e = l3d_scan_exclusive(qcount, qbase, cells, scratch, total, s)) != cudaSuccess)
+        return bail(cuda_fail(e, "surface quads"));
+    if ((rc = read_u32(total, &nq, s))) return bail(rc);
+    const long long faces = 2ll * nq;
+    if ((e = cudaMalloc(&m->idx, std::max<long long>(faces * 3, 1) * 4)) != cudaSuccess)
+        return bail(cuda_fail(e, "index buffer"));
+    if ((e = l3d_launch_sn_emit(v, cells, cell_vertex, qcount, qbase, pos_d, m->idx, s)) != cudaSuccess)
+        return bail(cuda_fail(e, "surface triangles"));
+    /* normals: faces gathered per vertex in face order */
+    double* fn;
+    uint32_t *degree, *start, *cursor, *lists;
+    if ((e = tmp.get(&fn, (size_t)faces * 3)) != cudaSuccess || (e = tmp.get(&degree, nv)) != cudaSuccess ||
+        (e = tmp.get(&start, nv)) != cudaSuccess || (e = tmp.get(&cursor, nv)) != cudaSuccess ||
+        (e = tmp.get(&lists, (size_t)faces * 3)) != cudaSuccess)
+        return bail(cuda_fail(e, "normal buffers"));
+    uint32_t* nscratch;
+    if ((e = tmp.get(&nscratch, l3d_scan_scratch(std::max<long long>(nv, 1)) / 4 + 1)) != cudaSuccess)
+        return bail(cuda_fail(e, "scan scratch"));
+    if ((e = cudaMemsetAsync(degree, 0, std::max<size_t>(nv, 1) * 4, s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(cursor, 0, std::max<size_t>(nv, 1) * 4, s)) != cudaSuccess ||
+        (e = l3d_launch_face_normals(m->pos, m->idx, faces, fn, degree, s)) != cudaSuccess ||
+        (e = l3d_scan_exclusive(degree, start, nv, nscratch, nullptr, s)) != cudaSuccess ||
+        (e = l3d_launch_face_lists(m->idx, faces, start, cursor, lists, s)) != cudaSuccess ||
+        (e = l3d_launch_vertex_normals(nv, start, degree, lists, fn, m->nrm, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return bail(cuda_fail(e, "vertex normals"));
+    m->nv = nv;
+    m->ni = faces * 3;
+    m->launches = 13;
+    *out = m;
+    return L3D_OK;
+}
+
+/* Grid dims and lookup of a brick pool from its coords (host). */
+void pool_lookup(const int32_t* coords, long long count, int dims[3], std::vector<int32_t>& lookup) {
+    dims[0] = dims[1] = dims[2] = 1;
+    for (long long b = 0; b < count; b++)
+        for (int k = 0; k < 3; k++) dims[k] = std::max(dims[k], coords[b * 4 + k] + 1);
+    lookup.assign((size_t)dims[0] * dims[1] * dims[2], -1);
+    for (long long b = 0; b < count; b++)
+        lookup[((size_t)coords[b * 4 + 2] * dims[1] + coords[b * 4 + 1]) * dims[0] + coords[b * 4]] = (int32_t)b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int l3d_tsdf_extract_surface(l3d_tsdf* t, double min_weight, l3d_mesh** out) {
+    if (!t || !out) return fail(L3D_EINVAL, "NULL handle or out");
+    *out = nullptr;
+    L3dSdfView v;
+    std::memset(&v, 0, sizeof(v));
+    v.tsdf = t->tsdf;
+    v.weight = t->weight;
+    v.q8 = t->q8;
+    for (int i = 0; i < 3; i++) v.origin[i] = t->g.origin_d[i];
+    v.voxel = t->g.voxel_d;
+    v.min_weight = min_weight;
+    DevBufs tmp;
+    long long bricks;
+    if (t->g.dense) {
+        v.dense = 1;
+        for (int i = 0; i < 3; i++) {
+            v.dims[i] = t->g.nb[i];
+            v.vdims[i] = t->g.dims[i];
+        }
+        bricks = (long long)v.dims[0] * v.dims[1] * v.dims[2];
+    } else {
+        bricks = t->g.bricks;
+        std::vector<int32_t> coords((size_t)bricks * 4), lookup;
+        L3D_CUDA(cudaMemcpyAsync(coords.data(), t->coords, coords.size() * 4, cudaMemcpyDeviceToHost,
+                                 t->stream), "read coords");
+        L3D_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+        pool_lookup(coords.data(), bricks, v.dims, lookup);
+        int32_t* dl;
+        L3D_CUDA(tmp.get(&dl, lookup.size()), "lookup buffer");
+        L3D_CUDA(cudaMemcpyAsync(dl, lookup.data(), lookup.size() * 4, cudaMemcpyHostToDevice, t->stream),
+                 "lookup upload");
+        v.lookup = dl;
+        v.coords = t->coords;
+        for (int i = 0; i < 3; i++) v.vdims[i] = v.dims[i] * 8;
+    }
+    int rc = extract_mesh(v, bricks, t->stream, out);
+    if (!rc) t->launches += (*out)->launches;
+    return rc;
+}
+
+int l3d_extract_surface(const l3d_sdf_bricks* vol, double min_weight, l3d_mesh** out) {
+    if (!vol || !out || !vol->lookup || !vol->tsdf || !vol->weight)
+        return fail(L3D_EINVAL, "NULL volume, array or out");
+    *out = nullptr;
+    if (vol->bricks < 0 || vol->dims[0] <= 0 || vol->dims[1] <= 0 || vol->dims[2] <= 0)
+        return fail(L3D_EINVAL, "bad volume dimensions");
+    const size_t cells = (size_t)vol->dims[0] * vol->dims[1] * vol->dims[2];
+    std::vector<int32_t> coords((size_t)std::max<int64_t>(vol->bricks, 1) * 4, 0);
+    for (size_t i = 0; i < cells; i++) {
+        const int32_t b = vol->lookup[i];
+        if (b < 0) continue;
+        if (b >= vol->bricks) return fail(L3D_EINVAL, "lookup entry %d beyond %lld bricks", b, (long long)vol->bricks);
+        coords[(size_t)b * 4] = (int32_t)(i % vol->dims[0]);
+        coords[(size_t)b * 4 + 1] = (int32_t)((i / vol->dims[0]) % vol->dims[1]);
+        coords[(size_t)b * 4 + 2] = (int32_t)(i / ((size_t)vol->dims[0] * vol->dims[1]));
+    }
+    cudaStream_t s;
+    L3D_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream creation");
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    } guard{s};
+    DevBufs tmp;
+    int32_t *dl, *dc;
+    float *dt, *dw;
+    const size_t voxels = (size_t)vol->bricks * 512;
+    L3D_CUDA(tmp.get(&dl, cells), "volume upload");
+    L3D_CUDA(tmp.get(&dc, coords.size()), "volume upload");
+    L3D_CUDA(tmp.get(&dt, voxels), "volume upload");
+    L3D_CUDA(tmp.get(&dw, voxels), "volume upload");
+    L3D_CUDA(cudaMemcpyAsync(dl, vol->lookup, cells * 4, cudaMemcpyHostToDevice, s), "volume upload");
+    L3D_CUDA(cudaMemcpyAsync(dc, coords.data(), coords.size() * 4, cudaMemcpyHostToDevice, s), "volume upload");
+    L3D_CUDA(cudaMemcpyAsync(dt, vol->tsdf, voxels * 4, cudaMemcpyHostToDevice, s), "volume upload");
+    L3D_CUDA(cudaMemcpyAsync(dw, vol->weight, voxels * 4, cudaMemcpyHostToDevice, s), "volume upload");
+    L3dSdfView v;
+    std::memset(&v, 0, sizeof(v));
+    v.tsdf = dt;
+    v.weight = dw;
+    v.lookup = dl;
+    v.coords = dc;
+    for (int i = 0; i < 3; i++) {
+        v.dims[i] = vol->dims[i];
+        v.vdims[i] = vol->dims[i] * 8;
+        v.origin[i] = vol->origin[i];
+    }
+    v.voxel = vol->voxel;
+    v.min_weight = min_weight;
+    return extract_mesh(v, vol->bricks, s, out);
+}
+
+int l3d_mesh_counts(const l3d_mesh* m, int64_t* vertices, int64_t* indices) {
+    if (!m) return fail(L3D_EINVAL, "NULL mesh");
+    if (vertices) *vertices = m->nv;
+    if (indices) *indices = m->ni;
+    return L3D_OK;
+}
+
+int l3d_mesh_read(const l3d_mesh* m, float* positions, float* normals, uint32_t* indices) {
+    if (!m) return fail(L3D_EINVAL, "NULL mesh");
+    if (positions && m->nv) L3D_CUDA(cudaMemcpy(positions, m->pos, m->nv * 12, cudaMemcpyDeviceToHost), "read positions");
+    if (normals && m->nv) L3D_CUDA(cudaMemcpy(normals, m->nrm, m->nv * 12, cudaMemcpyDeviceToHost), "read normals");
+    if (indices && m->ni) L3D_CUDA(cudaMemcpy(indices, m->idx, m->ni * 4, cudaMemcpyDeviceToHost), "read indices");
+    return L3D_OK;
+}
+
+int l3d_mesh_remove_small_components(const l3d_mesh* m, double fraction, int32_t min_faces,
+                                     l3d_mesh** out) {
+    if (!m || !out) return fail(L3D_EINVAL, "NULL mesh or out");
+    *out = nullptr;
+    const long long nv = m->nv, faces = m->ni / 3;
+    cudaStream_t s;
+    L3D_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream creation");
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    } guard{s};
+    DevBufs tmp;
+    uint32_t *label, *comp, *kept, *first, *face_base, *marks, *rank, *scratch, *total;
+    int* changed;
+    L3D_CUDA(tmp.get(&label, nv), "component buffers");
+    L3D_CUDA(tmp.get(&comp, nv), "component buffers");
+    L3D_CUDA(tmp.get(&kept, faces), "component buffers");
+    L3D_CUDA(tmp.get(&first, nv), "component buffers");
+    L3D_CUDA(tmp.get(&face_base, faces), "component buffers");
+    L3D_CUDA(tmp.get(&marks, faces * 3), "component buffers");
+    L3D_CUDA(tmp.get(&rank, faces * 3), "component buffers");
+    L3D_CUDA(tmp.get(&scratch, l3d_scan_scratch(std::max(faces * 3, 1ll)) / 4 + 1), "scan scratch");
+    L3D_CUDA(tmp.get(&total, 2), "scan total");
+    L3D_CUDA(tmp.get(&changed, 1), "flag");
+    L3D_CUDA(l3d_launch_cc_init(nv, label, s), "component labels");
+    int rounds = 0;
+    for (;; rounds++) {
+        if (rounds >= 256) return fail(L3D_ECUDA, "connected components did not settle in 256 rounds");
+        int h = 0;
+        L3D_CUDA(cudaMemsetAsync(changed, 0, sizeof(int), s), "flag clear");
+        L3D_CUDA(l3d_launch_cc_round(m->idx, faces, nv, label, changed, s), "component round");
+        L3D_CUDA(cudaMemcpyAsync(&h, changed, sizeof(int), cudaMemcpyDeviceToHost, s), "flag read");
+        L3D_CUDA(cudaStreamSynchronize(s), "synchronize");
+        if (!h) break;
+    }
+    const double limit = std::max((double)min_faces, (double)faces * fraction);
+    uint32_t kf = 0, kv = 0;
+    L3D_CUDA(cudaMemsetAsync(comp, 0, std::max<size_t>(nv, 1) * 4, s), "clear");
+    L3D_CUDA(cudaMemsetAsync(first, 0xff, std::max<size_t>(nv, 1) * 4, s), "clear");
+    L3D_CUDA(cudaMemsetAsync(marks, 0, std::max<size_t>(faces * 3, 1) * 4, s), "clear");
+    L3D_CUDA(l3d_launch_cc_count(m->idx, faces, label, comp, s), "component sizes");
+    L3D_CUDA(l3d_launch_cc_keep(m->idx, faces, label, comp, limit, kept, first, s), "kept faces");
+    L3D_CUDA(l3d_scan_exclusive(kept, face_base, faces, scratch, total, s), "face scan");
+    int rc = read_u32(total, &kf, s);
+    if (rc) return rc;
+    L3D_CUDA(l3d_launch_cc_first_marks(nv, first, marks, s), "vertex order");
+    L3D_CUDA(l3d_scan_exclusive(marks, rank, faces * 3, scratch, total, s), "vertex scan");
+    if ((rc = read_u32(total, &kv, s))) return rc;
+    l3d_mesh* r = new (std::nothrow) l3d_mesh();
+    if (!r) return fail(L3D_ENOMEM, "host allocation failed");
+    cudaError_t e;
+    if ((e = cudaMalloc(&r->pos, std::max<size_t>(kv, 1) * 12)) != cudaSuccess ||
+        (e = cudaMalloc(&r->nrm, std::max<size_t>(kv, 1) * 12)) != cudaSuccess ||
+        (e = cudaMalloc(&r->idx, std::max<size_t>(kf, 1) * 12)) != cudaSuccess ||
+        (e = l3d_launch_cc_emit(m->idx, faces, kept, face_base, first, rank, m->pos, m->nrm, r->idx,
+                                r->pos, r->nrm, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        mesh_free(r);
+        return cuda_fail(e, "component output");
+    }
+    r->nv = kv;
+    r->ni = 3ll * kf;
+    r->launches = 2ll * rounds + 9;
+    *out = r;
+    return L3D_OK;
+}
+
+int64_t l3d_mesh_launches(const l3d_mesh* m) { return m ? m->launches : -1; }
+
+void l3d_mesh_destroy(l3d_mesh* m) { mesh_free(m); }
+
+int l3d_brick_grid_build(const double origin[3], double voxel, const double extent[3],
+                         const float* points, int64_t n, double radius, int32_t dims[3],
+                         int32_t* count, int32_t* coords, int32_t* lookup) {
+    if (!origin || !extent || !dims || !count) return fail(L3D_EINVAL, "NULL argument");
+    if (!(voxel > 0.0)) return fail(L3D_EINVAL, "voxel must be positive");
+    if (n < 0 || (n > 0 && !points)) return fail(L3D_EINVAL, "bad point list");
+    /* BrickGrid constructor (tsdf-volume.ts:17-29) */
+    const double side = voxel * 8.0;
+    L3dBrickGrid g;
+    long long cells = 1;
+    for (int i = 0; i < 3; i++) {
+        const double d = std::ceil(extent[i] / side);
+        if (!(d < 1e6)) return fail(L3D_EINVAL, "grid too large");
+        g.dims[i] = std::max(1, (int)d);
+        g.origin[i] = origin[i];
+        dims[i] = g.dims[i];
+        cells *= g.dims[i];
+    }
+    g.voxel = voxel;
+    if (cells >= (1ll << 31)) return fail(L3D_EINVAL, "grid of %lld bricks too large", cells);
+    cudaStream_t s;
+    L3D_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream creation");
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    } guard{s};
+    DevBufs tmp;
+    uint8_t* marks;
+    float* pts;
+    uint32_t *flags, *base, *scratch, *total;
+    int32_t *dlook, *dcoords;
+    L3D_CUDA(tmp.get(&marks, cells), "grid buffers");
+    L3D_CUDA(tmp.get(&pts, (size_t)n * 3), "grid buffers");
+    L3D_CUDA(tmp.get(&flags, cells), "grid buffers");
+    L3D_CUDA(tmp.get(&base, cells), "grid buffers");
+    L3D_CUDA(tmp.get(&dlook, cells), "grid buffers");
+    L3D_CUDA(tmp.get(&scratch, l3d_scan_scratch(cells) / 4 + 1), "scan scratch");
+    L3D_CUDA(tmp.get(&total, 1), "scan total");
+    L3D_CUDA(cudaMemsetAsync(marks, 0, cells, s), "clear marks");
+    if (n) L3D_CUDA(cudaMemcpyAsync(pts, points, (size_t)n * 12, cudaMemcpyHostToDevice, s), "point upload");
+    L3D_CUDA(l3d_launch_grid_mark(pts, n, g, radius, marks, s), "mark");
+    L3D_CUDA(l3d_launch_grid_widen(marks, cells, flags, s), "mark");
+    L3D_CUDA(l3d_scan_exclusive(flags, base, cells, scratch, total, s), "brick scan");
+    uint32_t c = 0;
+    int rc = read_u32(total, &c, s);
+    if (rc) return rc;
+    *count = (int32_t)c;
+    L3D_CUDA(tmp.get(&dcoords, (size_t)c * 4), "coords buffer");
+    L3D_CUDA(l3d_launch_grid_build(flags, base, cells, g, dlook, dcoords, s), "build");
+    if (lookup) L3D_CUDA(cudaMemcpyAsync(lookup, dlook, cells * 4, cudaMemcpyDeviceToHost, s), "read lookup");
+    if (coords && c) L3D_CUDA(cudaMemcpyAsync(coords, dcoords, (size_t)c * 16, cudaMemcpyDeviceToHost, s), "read coords");
+    L3D_CUDA(cudaStreamSynchronize(s), "synchronize");
+    return L3D_OK;
+}
+
+}  // extern "C"

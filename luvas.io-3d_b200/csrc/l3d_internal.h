@@ -263,6 +263,73 @@ cudaError_t l3d_launch_cloud_emit(const L3dCloudTable& t, unsigned min_support, 
                                   float* pos, float* nrm, uint8_t* col, uint16_t* support,
                                   unsigned long long* keys, cudaStream_t stream);
 
+/* ---- prefix sums (scan.cu) ---- */
+
+/* Bytes of scratch l3d_scan_exclusive needs for n elements. */
+size_t l3d_scan_scratch(long long n);
+/* out[i] = in[0] + ... + in[i-1] (in == out allowed); *total (device, may be NULL) = the sum. */
+cudaError_t l3d_scan_exclusive(const uint32_t* in, uint32_t* out, long long n, uint32_t* scratch,
+                               uint32_t* total, cudaStream_t stream);
+
+/* ---- surface extraction (mesh.cu) ---- */
+
+/* A TSDF volume as surface extraction reads it: a brick pool (lookup over the grid of dims
+ * bricks, coords per pool brick) or a dense grid (bricks in dense brick order). */
+struct L3dSdfView {
+    const float* tsdf;
+    const void* weight;        /* f32, or u16 Q8.8 when q8 */
+    const int32_t* lookup;     /* pool: grid cell -> pool brick or -1 */
+    const int32_t* coords;     /* pool: 4 int32 per brick */
+    int dims[3];               /* grid size in bricks */
+    int vdims[3];              /* voxels per axis (dense dims, or dims x 8) */
+    int dense;
+    int q8;
+    double origin[3];
+    double voxel;
+    double min_weight;
+};
+
+struct L3dBrickGrid {
+    double origin[3];
+    double voxel;
+    int dims[3];
+};
+
+cudaError_t l3d_launch_sn_flag(const L3dSdfView& v, long long cells, uint32_t* flag, cudaStream_t s);
+cudaError_t l3d_launch_sn_vertex(const L3dSdfView& v, long long cells, const uint32_t* flag,
+                                 const uint32_t* base, int32_t* cell_vertex, double* pos_d,
+                                 float* pos_f, cudaStream_t s);
+cudaError_t l3d_launch_sn_count(const L3dSdfView& v, long long cells, const int32_t* cell_vertex,
+                                uint32_t* qcount, cudaStream_t s);
+cudaError_t l3d_launch_sn_emit(const L3dSdfView& v, long long cells, const int32_t* cell_vertex,
+                               const uint32_t* qcount, const uint32_t* qbase, const double* pos_d,
+                               uint32_t* indices, cudaStream_t s);
+cudaError_t l3d_launch_face_normals(const float* pos, const uint32_t* idx, long long faces, double* fn,
+                                    uint32_t* degree, cudaStream_t s);
+cudaError_t l3d_launch_face_lists(const uint32_t* idx, long long faces, const uint32_t* start,
+                                  uint32_t* cursor, uint32_t* lists, cudaStream_t s);
+cudaError_t l3d_launch_vertex_normals(long long vertices, const uint32_t* start, const uint32_t* degree,
+                                      uint32_t* lists, const double* fn, float* nrm, cudaStream_t s);
+cudaError_t l3d_launch_cc_init(long long vertices, uint32_t* label, cudaStream_t s);
+cudaError_t l3d_launch_cc_round(const uint32_t* idx, long long faces, long long vertices, uint32_t* label,
+                                int* changed, cudaStream_t s);
+cudaError_t l3d_launch_cc_count(const uint32_t* idx, long long faces, const uint32_t* label,
+                                uint32_t* comp_faces, cudaStream_t s);
+cudaError_t l3d_launch_cc_keep(const uint32_t* idx, long long faces, const uint32_t* label,
+                               const uint32_t* comp_faces, double limit, uint32_t* kept,
+                               uint32_t* first, cudaStream_t s);
+cudaError_t l3d_launch_cc_first_marks(long long vertices, const uint32_t* first, uint32_t* marks,
+                                      cudaStream_t s);
+cudaError_t l3d_launch_cc_emit(const uint32_t* idx, long long faces, const uint32_t* kept,
+                               const uint32_t* face_base, const uint32_t* first, const uint32_t* rank,
+                               const float* pos, const float* nrm, uint32_t* out_idx, float* out_pos,
+                               float* out_nrm, cudaStream_t s);
+cudaError_t l3d_launch_grid_mark(const float* pts, long long n, const L3dBrickGrid& g, double radius,
+                                 uint8_t* marks, cudaStream_t s);
+cudaError_t l3d_launch_grid_widen(const uint8_t* marks, long long cells, uint32_t* flags, cudaStream_t s);
+cudaError_t l3d_launch_grid_build(const uint32_t* flags, const uint32_t* base, long long cells,
+                                  const L3dBrickGrid& g, int32_t* lookup, int32_t* coords, cudaStream_t s);
+
 /* Sets the calling thread's l3d_last_error() message (capi.cu). */
 void l3d_set_error(const char* msg);
 

@@ -98,6 +98,18 @@ class TsdfDesc(C.Structure):
     ]
 
 
+class SdfBricks(C.Structure):
+    _fields_ = [
+        ("origin", C.c_double * 3),
+        ("voxel", C.c_double),
+        ("dims", C.c_int32 * 3),
+        ("lookup", C.c_void_p),
+        ("tsdf", C.c_void_p),
+        ("weight", C.c_void_p),
+        ("bricks", C.c_int64),
+    ]
+
+
 class IntegrationView(C.Structure):
     _fields_ = [
         ("intrinsics", Intrinsics),
@@ -164,6 +176,14 @@ SIGNATURES = [
     ("l3d_cloud_read", C.c_int, [_P, _I, C.c_int64, C.POINTER(C.c_int64), _P, _P, _P, _P, _P]),
     ("l3d_cloud_launches", C.c_int64, [_P]),
     ("l3d_cloud_destroy", None, [_P]),
+    ("l3d_extract_surface", C.c_int, [C.POINTER(SdfBricks), C.c_double, C.POINTER(_P)]),
+    ("l3d_tsdf_extract_surface", C.c_int, [_P, C.c_double, C.POINTER(_P)]),
+    ("l3d_mesh_counts", C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    ("l3d_mesh_read", C.c_int, [_P, _P, _P, _P]),
+    ("l3d_mesh_remove_small_components", C.c_int, [_P, C.c_double, _I, C.POINTER(_P)]),
+    ("l3d_mesh_launches", C.c_int64, [_P]),
+    ("l3d_mesh_destroy", None, [_P]),
+    ("l3d_brick_grid_build", C.c_int, [_P, C.c_double, _P, _P, C.c_int64, C.c_double, _P, _P, _P, _P]),
     ("l3d_ncc_forward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P]),
     ("l3d_ncc_backward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P, _P, _P, _P]),
     ("l3d_tsdf_forward_depth", C.c_int, [_P, C.POINTER(IntegrationView), _I, _I, _P, _P, _P, _P, _P,

@@ -44,6 +44,13 @@ class TsdfDesc(C.Structure):
     ]
 
 
+class SdfBricks(C.Structure):
+    _fields_ = [
+        ("origin", C.c_double * 3), ("voxel", C.c_double), ("dims", C.c_int32 * 3),
+        ("lookup", C.c_void_p), ("tsdf", C.c_void_p), ("weight", C.c_void_p), ("bricks", C.c_int64),
+    ]
+
+
 class TsdfView(C.Structure):
     _fields_ = [
         ("k", C.c_double * 4), ("R", C.c_double * 9), ("t", C.c_double * 3),
@@ -85,6 +92,13 @@ def load():
         lib.orc_cloud_cell.argtypes = [P]
         lib.orc_cloud_read.restype = C.c_int32
         lib.orc_cloud_read.argtypes = [P, C.c_int32, P, P, P, P, P]
+        lib.orc_extract_surface.argtypes = [C.POINTER(SdfBricks), C.c_double, P, P, P, P, P]
+        lib.orc_remove_small_components.argtypes = [C.c_int64, C.c_int64, P, P, P, C.c_double,
+                                                     C.c_int32, P, P, P, P, P]
+        lib.orc_brick_grid_dims.argtypes = [C.c_double, P, P]
+        lib.orc_brick_grid_mark.argtypes = [P, C.c_double, P, P, P, C.c_int64, C.c_double]
+        lib.orc_brick_grid_build.restype = C.c_int32
+        lib.orc_brick_grid_build.argtypes = [P, P, P, P]
         lib.orc64_ncc_grad.argtypes = [C.POINTER(StereoArgs), P, P, P, P, P, P, P, P]
         lib.orc64_tsdf_depth.argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView)] + [P] * 11 + [C.c_int32]
         lib.orc_pack_sample.restype = C.c_uint32
@@ -286,6 +300,61 @@ class NccGrad:
                                    cells.ctypes.data)
         assert rc == 0
         return cost, margin, cells
+
+
+def extract_surface(origin, voxel, dims, lookup, tsdf, weight, min_weight):
+    """extractSurface + computeNormals -> (positions (V, 3) f32, normals (V, 3) f32,
+    indices (I,) u32)."""
+    lk = np.ascontiguousarray(lookup, dtype=np.int32)
+    ts = np.ascontiguousarray(tsdf, dtype=np.float32)
+    wt = np.ascontiguousarray(weight, dtype=np.float32)
+    v = SdfBricks()
+    v.origin[:] = [float(o) for o in origin]
+    v.voxel = float(voxel)
+    v.dims[:] = [int(d) for d in dims]
+    v.lookup, v.tsdf, v.weight = lk.ctypes.data, ts.ctypes.data, wt.ctypes.data
+    v.bricks = ts.size // 512
+    nv, ni = C.c_int64(), C.c_int64()
+    lib = load()
+    lib.orc_extract_surface(C.byref(v), float(min_weight), C.byref(nv), C.byref(ni), None, None, None)
+    pos = np.zeros((nv.value, 3), np.float32)
+    nrm = np.zeros((nv.value, 3), np.float32)
+    idx = np.zeros(ni.value, np.uint32)
+    lib.orc_extract_surface(C.byref(v), float(min_weight), C.byref(nv), C.byref(ni),
+                            pos.ctypes.data, nrm.ctypes.data, idx.ctypes.data)
+    return pos, nrm, idx
+
+
+def remove_small_components(pos, nrm, idx, fraction, min_faces):
+    p = np.ascontiguousarray(pos, np.float32)
+    n = np.ascontiguousarray(nrm, np.float32)
+    i = np.ascontiguousarray(idx, np.uint32)
+    op = np.zeros_like(p)
+    on = np.zeros_like(n)
+    oi = np.zeros_like(i)
+    nv, ni = C.c_int64(), C.c_int64()
+    load().orc_remove_small_components(p.shape[0], i.size, p.ctypes.data, n.ctypes.data, i.ctypes.data,
+                                       float(fraction), int(min_faces), C.byref(nv), C.byref(ni),
+                                       op.ctypes.data, on.ctypes.data, oi.ctypes.data)
+    return op[:nv.value], on[:nv.value], oi[:ni.value]
+
+
+def brick_grid(origin, voxel, extent, points, radius):
+    """BrickGrid(origin, voxel, extent), mark(points, radius), build() -> (dims, coords, lookup)."""
+    lib = load()
+    o = np.ascontiguousarray(origin, np.float64)
+    e = np.ascontiguousarray(extent, np.float64)
+    dims = np.zeros(3, np.int32)
+    lib.orc_brick_grid_dims(float(voxel), e.ctypes.data, dims.ctypes.data)
+    marks = np.zeros(int(np.prod(dims.astype(np.int64))), np.uint8)
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    lib.orc_brick_grid_mark(o.ctypes.data, float(voxel), dims.ctypes.data, marks.ctypes.data,
+                            pts.ctypes.data, pts.shape[0], float(radius))
+    lookup = np.zeros(marks.size, np.int32)
+    count = lib.orc_brick_grid_build(dims.ctypes.data, marks.ctypes.data, None, lookup.ctypes.data)
+    coords = np.zeros((count, 4), np.int32)
+    lib.orc_brick_grid_build(dims.ctypes.data, marks.ctypes.data, coords.ctypes.data, lookup.ctypes.data)
+    return dims, coords, lookup
 
 
 class Cloud:

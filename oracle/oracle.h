@@ -140,6 +140,35 @@ double orc_cloud_cell(const orc_cloud* c);
 int32_t orc_cloud_read(const orc_cloud* c, int32_t min_support, float* pos, float* nrm,
                        uint8_t* col, uint16_t* support, int32_t* cells);
 
+/* ---- surface extraction (mesh.cpp) ---- */
+
+/* SdfBricks (surface-nets.ts:4-12): grid of dims bricks, lookup (dims product) -> pool brick or
+ * -1, tsdf and weight of `bricks` pool bricks (512 voxels each, b*512 + x + 8y + 64z). */
+typedef struct {
+    double origin[3];
+    double voxel;
+    int32_t dims[3];
+    const int32_t* lookup;
+    const float* tsdf;
+    const float* weight;
+    int64_t bricks;
+} orc_sdf_bricks;
+
+/* extractSurface + computeNormals; counts always, arrays when not NULL. */
+int orc_extract_surface(const orc_sdf_bricks* vol, double min_weight, int64_t* n_vertices,
+                        int64_t* n_indices, float* positions, float* normals, uint32_t* indices);
+/* removeSmallComponents (mesh.ts:37-87) */
+int orc_remove_small_components(int64_t nv, int64_t ni, const float* pos, const float* nrm,
+                                const uint32_t* idx, double fraction, int32_t min_faces,
+                                int64_t* out_nv, int64_t* out_ni, float* out_pos, float* out_nrm,
+                                uint32_t* out_idx);
+/* BrickGrid (tsdf-volume.ts:13-65) */
+void orc_brick_grid_dims(double voxel, const double* extent, int32_t* dims);
+void orc_brick_grid_mark(const double* origin, double voxel, const int32_t* dims, uint8_t* marks,
+                         const float* points, int64_t n, double radius);
+int32_t orc_brick_grid_build(const int32_t* dims, const uint8_t* marks, int32_t* coords,
+                             int32_t* lookup);
+
 /* Packing helpers (depth-packing.wgsl.ts:3-33) and primitives for unit tests. */
 uint32_t orc_pack_sample(float depth, float nx, float ny, float nz, float cost);
 float orc_unpack_depth(uint32_t packed);
