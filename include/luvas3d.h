@@ -365,6 +365,25 @@ int l3d_brick_grid_build(const double origin[3], double voxel, const double exte
                          const float* points, int64_t n, double radius, int32_t dims[3],
                          int32_t* count, int32_t* coords, int32_t* lookup);
 
+/* ---- Image preparation (device pointers; work on `stream`, a cudaStream_t, NULL = the
+ * default stream) ---- */
+
+/* rgbaToGray (image/gray-image.ts:12-46): luma (77 R + 150 G + 29 B) / 256 averaged over the
+ * source area of each target pixel (integer ratios: whole blocks, rounded half up; other
+ * ratios: exact box filter with partial weights). */
+int l3d_image_rgba_to_gray(const uint8_t* rgba, int32_t width, int32_t height, int32_t target_width,
+                           int32_t target_height, uint8_t* gray, void* stream);
+/* downsampleRgb (gray-image.ts:49-82): packed RGB thumbnail, block means truncated. */
+int l3d_image_downsample_rgb(const uint8_t* rgba, int32_t width, int32_t height, int32_t target_width,
+                             int32_t target_height, uint8_t* rgb, void* stream);
+/* downsampleGray (gray-image.ts:166-187): area average of a gray image. */
+int l3d_image_downsample_gray(const uint8_t* gray, int32_t width, int32_t height, int32_t target_width,
+                              int32_t target_height, uint8_t* out, void* stream);
+/* upsampleDepth (mvs/depth-maps.ts:9-42): bilinear upsampling of a phone depth grid (0 = no
+ * data) ignoring empty cells; 0 where less than half of the weight has data. */
+int l3d_depth_upsample(const float* grid, int32_t grid_width, int32_t grid_height, int32_t width,
+                       int32_t height, float* out, void* stream);
+
 /* ---- Differentiation (no reference counterpart) ----
  *
  * The reference has no gradients: its WGSL kernels only evaluate costs.  These entry points give

@@ -2384,3 +2384,145 @@ int l3d_brick_grid_build(const double origin[3], double voxel, const double exte
 }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------ image preparation ------ */
+
+namespace {
+
+/* coverage (gray-image.ts:226-239), flattened for the device */
+struct HostCover {
+    std::vector<int> first, count;
+    std::vector<double> weights;
+    int kmax = 1;
+};
+
+HostCover host_coverage(int source, int target) {
+    HostCover c;
+    const double scale = (double)source / target;
+    std::vector<std::vector<double>> w((size_t)target);
+    for (int t = 0; t < target; t++) {
+        const double start = t * scale;
+        const double end = std::min((double)source, (t + 1) * scale);
+        const int first = (int)std::floor(start);
+        c.first.push_back(first);
+        for (int i = first; i < end; i++)
+            w[t].push_back((std::min(end, (double)(i + 1)) - std::max(start, (double)i)) / scale);
+        c.count.push_back((int)w[t].size());
+        c.kmax = std::max(c.kmax, (int)w[t].size());
+    }
+    c.weights.assign((size_t)target * c.kmax, 0.0);
+    for (int t = 0; t < target; t++)
+        for (size_t k = 0; k < w[t].size(); k++) c.weights[(size_t)t * c.kmax + k] = w[t][k];
+    return c;
+}
+
+/* Stream-ordered device copy of a host cover table; freed with cudaFreeAsync on the stream. */
+int upload_cover(const HostCover& h, cudaStream_t s, L3dAreaCover* d, std::vector<void*>& owned) {
+    int *first, *count;
+    double* weights;
+    L3D_CUDA(cudaMallocAsync((void**)&first, h.first.size() * 4, s), "cover table");
+    owned.push_back(first);
+    L3D_CUDA(cudaMallocAsync((void**)&count, h.count.size() * 4, s), "cover table");
+    owned.push_back(count);
+    L3D_CUDA(cudaMallocAsync((void**)&weights, h.weights.size() * 8, s), "cover table");
+    owned.push_back(weights);
+    L3D_CUDA(cudaMemcpyAsync(first, h.first.data(), h.first.size() * 4, cudaMemcpyHostToDevice, s), "cover upload");
+    L3D_CUDA(cudaMemcpyAsync(count, h.count.data(), h.count.size() * 4, cudaMemcpyHostToDevice, s), "cover upload");
+    L3D_CUDA(cudaMemcpyAsync(weights, h.weights.data(), h.weights.size() * 8, cudaMemcpyHostToDevice, s),
+             "cover upload");
+    d->first = first;
+    d->count = count;
+    d->weights = weights;
+    d->kmax = h.kmax;
+    return L3D_OK;
+}
+
+int check_sizes(int w, int h, int tw, int th) {
+    if (w <= 0 || h <= 0 || tw <= 0 || th <= 0) return fail(L3D_EINVAL, "sizes must be positive");
+    if ((long long)w * h >= (1ll << 31) || (long long)tw * th >= (1ll << 31))
+        return fail(L3D_EINVAL, "image too large");
+    return L3D_OK;
+}
+
+/* resampleArea (gray-image.ts:193-221) of a device source (u8 or f32). */
+int area_resample(const void* src, int is_float, int w, int h, int tw, int th, uint8_t* out,
+                  cudaStream_t s) {
+    std::vector<void*> owned;
+    auto release = [&](int rc) {
+        for (void* p : owned) cudaFreeAsync(p, s);
+        return rc;
+    };
+    L3dAreaCover cols, rows;
+    int rc = upload_cover(host_coverage(w, tw), s, &cols, owned);
+    if (!rc) rc = upload_cover(host_coverage(h, th), s, &rows, owned);
+    if (rc) return release(rc);
+    float* temp;
+    cudaError_t e = cudaMallocAsync((void**)&temp, (size_t)tw * h * 4, s);
+    if (e != cudaSuccess) return release(cuda_fail(e, "area filter buffer"));
+    owned.push_back(temp);
+    e = l3d_launch_area(src, is_float, w, h, tw, th, cols, rows, temp, out, s);
+    if (e != cudaSuccess) return release(cuda_fail(e, "area filter launch"));
+    return release(L3D_OK);
+}
+
+}  // namespace
+
+extern "C" {
+
+int l3d_image_rgba_to_gray(const uint8_t* rgba, int32_t width, int32_t height, int32_t target_width,
+                           int32_t target_height, uint8_t* gray, void* stream) {
+    if (!rgba || !gray) return fail(L3D_EINVAL, "NULL image");
+    int rc = check_sizes(width, height, target_width, target_height);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (width % target_width == 0 && height % target_height == 0) {
+        L3D_CUDA(l3d_launch_gray_blocks(rgba, width, height, target_width, target_height, gray, s), "gray launch");
+        return L3D_OK;
+    }
+    float* luma;
+    L3D_CUDA(cudaMallocAsync((void**)&luma, (size_t)width * height * 4, s), "luma buffer");
+    cudaError_t e = l3d_launch_luma(rgba, (long long)width * height, luma, s);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(luma, s);
+        return cuda_fail(e, "luma launch");
+    }
+    rc = area_resample(luma, 1, width, height, target_width, target_height, gray, s);
+    cudaFreeAsync(luma, s);
+    return rc;
+}
+
+int l3d_image_downsample_rgb(const uint8_t* rgba, int32_t width, int32_t height, int32_t target_width,
+                             int32_t target_height, uint8_t* rgb, void* stream) {
+    if (!rgba || !rgb) return fail(L3D_EINVAL, "NULL image");
+    int rc = check_sizes(width, height, target_width, target_height);
+    if (rc) return rc;
+    L3D_CUDA(l3d_launch_rgb_blocks(rgba, width, height, target_width, target_height, rgb, (cudaStream_t)stream),
+             "rgb launch");
+    return L3D_OK;
+}
+
+int l3d_image_downsample_gray(const uint8_t* gray, int32_t width, int32_t height, int32_t target_width,
+                              int32_t target_height, uint8_t* out, void* stream) {
+    if (!gray || !out) return fail(L3D_EINVAL, "NULL image");
+    int rc = check_sizes(width, height, target_width, target_height);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (width % target_width == 0 && height % target_height == 0) {
+        L3D_CUDA(l3d_launch_gray_down_blocks(gray, width, height, target_width, target_height, out, s),
+                 "gray launch");
+        return L3D_OK;
+    }
+    return area_resample(gray, 0, width, height, target_width, target_height, out, s);
+}
+
+int l3d_depth_upsample(const float* grid, int32_t grid_width, int32_t grid_height, int32_t width,
+                       int32_t height, float* out, void* stream) {
+    if (!grid || !out) return fail(L3D_EINVAL, "NULL buffer");
+    int rc = check_sizes(grid_width, grid_height, width, height);
+    if (rc) return rc;
+    L3D_CUDA(l3d_launch_upsample_depth(grid, grid_width, grid_height, width, height, out,
+                                       (cudaStream_t)stream), "upsample launch");
+    return L3D_OK;
+}
+
+}  // extern "C"

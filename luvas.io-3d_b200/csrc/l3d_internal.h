@@ -330,6 +330,30 @@ cudaError_t l3d_launch_grid_widen(const uint8_t* marks, long long cells, uint32_
 cudaError_t l3d_launch_grid_build(const uint32_t* flags, const uint32_t* base, long long cells,
                                   const L3dBrickGrid& g, int32_t* lookup, int32_t* coords, cudaStream_t s);
 
+/* ---- image preparation (image.cu) ---- */
+
+/* coverage() of one axis of the area filter: per target pixel the first source pixel and
+ * `count` weights (stride kmax). */
+struct L3dAreaCover {
+    const int* first;
+    const int* count;
+    const double* weights;
+    int kmax;
+};
+
+cudaError_t l3d_launch_gray_blocks(const uint8_t* rgba, int W, int H, int tw, int th, uint8_t* out,
+                                   cudaStream_t s);
+cudaError_t l3d_launch_luma(const uint8_t* rgba, long long n, float* luma, cudaStream_t s);
+cudaError_t l3d_launch_area(const void* src, int src_is_float, int W, int H, int tw, int th,
+                            const L3dAreaCover& cols, const L3dAreaCover& rows, float* temp,
+                            uint8_t* out, cudaStream_t s);
+cudaError_t l3d_launch_rgb_blocks(const uint8_t* rgba, int W, int H, int tw, int th, uint8_t* out,
+                                  cudaStream_t s);
+cudaError_t l3d_launch_gray_down_blocks(const uint8_t* gray, int W, int H, int tw, int th, uint8_t* out,
+                                        cudaStream_t s);
+cudaError_t l3d_launch_upsample_depth(const float* grid, int gw, int gh, int W, int H, float* out,
+                                      cudaStream_t s);
+
 /* Sets the calling thread's l3d_last_error() message (capi.cu). */
 void l3d_set_error(const char* msg);
 

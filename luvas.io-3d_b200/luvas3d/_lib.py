@@ -184,6 +184,10 @@ SIGNATURES = [
     ("l3d_mesh_launches", C.c_int64, [_P]),
     ("l3d_mesh_destroy", None, [_P]),
     ("l3d_brick_grid_build", C.c_int, [_P, C.c_double, _P, _P, C.c_int64, C.c_double, _P, _P, _P, _P]),
+    ("l3d_image_rgba_to_gray", C.c_int, [_P, _I, _I, _I, _I, _P, _P]),
+    ("l3d_image_downsample_rgb", C.c_int, [_P, _I, _I, _I, _I, _P, _P]),
+    ("l3d_image_downsample_gray", C.c_int, [_P, _I, _I, _I, _I, _P, _P]),
+    ("l3d_depth_upsample", C.c_int, [_P, _I, _I, _I, _I, _P, _P]),
     ("l3d_ncc_forward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P]),
     ("l3d_ncc_backward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P, _P, _P, _P]),
     ("l3d_tsdf_forward_depth", C.c_int, [_P, C.POINTER(IntegrationView), _I, _I, _P, _P, _P, _P, _P,

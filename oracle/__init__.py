@@ -99,6 +99,9 @@ def load():
         lib.orc_brick_grid_mark.argtypes = [P, C.c_double, P, P, P, C.c_int64, C.c_double]
         lib.orc_brick_grid_build.restype = C.c_int32
         lib.orc_brick_grid_build.argtypes = [P, P, P, P]
+        for name in ("orc_rgba_to_gray", "orc_downsample_rgb", "orc_downsample_gray"):
+            getattr(lib, name).argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P]
+        lib.orc_upsample_depth.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P]
         lib.orc64_ncc_grad.argtypes = [C.POINTER(StereoArgs), P, P, P, P, P, P, P, P]
         lib.orc64_tsdf_depth.argtypes = [C.POINTER(TsdfDesc), C.POINTER(TsdfView)] + [P] * 11 + [C.c_int32]
         lib.orc_pack_sample.restype = C.c_uint32
@@ -355,6 +358,34 @@ def brick_grid(origin, voxel, extent, points, radius):
     coords = np.zeros((count, 4), np.int32)
     lib.orc_brick_grid_build(dims.ctypes.data, marks.ctypes.data, coords.ctypes.data, lookup.ctypes.data)
     return dims, coords, lookup
+
+
+def rgba_to_gray(rgba, tw, th):
+    a = np.ascontiguousarray(rgba, np.uint8)
+    out = np.zeros((th, tw), np.uint8)
+    load().orc_rgba_to_gray(a.ctypes.data, a.shape[1], a.shape[0], tw, th, out.ctypes.data)
+    return out
+
+
+def downsample_rgb(rgba, tw, th):
+    a = np.ascontiguousarray(rgba, np.uint8)
+    out = np.zeros((th, tw, 3), np.uint8)
+    load().orc_downsample_rgb(a.ctypes.data, a.shape[1], a.shape[0], tw, th, out.ctypes.data)
+    return out
+
+
+def downsample_gray(gray, tw, th):
+    a = np.ascontiguousarray(gray, np.uint8)
+    out = np.zeros((th, tw), np.uint8)
+    load().orc_downsample_gray(a.ctypes.data, a.shape[1], a.shape[0], tw, th, out.ctypes.data)
+    return out
+
+
+def upsample_depth(grid, width, height):
+    g = np.ascontiguousarray(grid, np.float32)
+    out = np.zeros((height, width), np.float32)
+    load().orc_upsample_depth(g.ctypes.data, g.shape[1], g.shape[0], width, height, out.ctypes.data)
+    return out
 
 
 class Cloud:

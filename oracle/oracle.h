@@ -169,6 +169,16 @@ void orc_brick_grid_mark(const double* origin, double voxel, const int32_t* dims
 int32_t orc_brick_grid_build(const int32_t* dims, const uint8_t* marks, int32_t* coords,
                              int32_t* lookup);
 
+/* ---- image preparation (image.cpp): gray-image.ts, depth-maps.ts upsampleDepth ---- */
+void orc_rgba_to_gray(const uint8_t* rgba, int32_t width, int32_t height, int32_t tw, int32_t th,
+                      uint8_t* out);
+void orc_downsample_rgb(const uint8_t* rgba, int32_t width, int32_t height, int32_t tw, int32_t th,
+                        uint8_t* out);
+void orc_downsample_gray(const uint8_t* gray, int32_t width, int32_t height, int32_t tw, int32_t th,
+                         uint8_t* out);
+void orc_upsample_depth(const float* grid, int32_t gw, int32_t gh, int32_t width, int32_t height,
+                        float* out);
+
 /* Packing helpers (depth-packing.wgsl.ts:3-33) and primitives for unit tests. */
 uint32_t orc_pack_sample(float depth, float nx, float ny, float nz, float cost);
 float orc_unpack_depth(uint32_t packed);
