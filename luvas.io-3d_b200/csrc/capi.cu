@@ -367,6 +367,21 @@ L3dFastView fast_view(const l3d_stereo* s, int ref, const l3d_solve_opts* o, lon
     v.has_prior = o->prior != nullptr && !o->geometric;
     v.pack = o->pack ? 1 : 0;
     const l3d_view& rv = s->views[ref];
+    if (o->from_coarse && s->opts.coarse) {
+        /* scaleIntrinsics (geometry/camera.ts:28-36) to the coarse level, in FP64 */
+        const l3d_stereo* c = s->opts.coarse;
+        const int cw = c->Wv[ref], ch = c->Hv[ref];
+        const double sx = (double)cw / v.W, sy = (double)ch / v.H;
+        v.ck[0] = (float)(rv.intrinsics.fx * sx);
+        v.ck[1] = (float)(rv.intrinsics.fy * sy);
+        v.ck[2] = (float)((rv.intrinsics.cx + 0.5) * sx - 0.5);
+        v.ck[3] = (float)((rv.intrinsics.cy + 0.5) * sy - 0.5);
+        v.cW = cw;
+        v.cH = ch;
+        v.has_coarse = 1;
+        v.has_prior = 0;
+        v.flags &= ~1u;
+    }
     const double kr[4] = {rv.intrinsics.fx, rv.intrinsics.fy, rv.intrinsics.cx, rv.intrinsics.cy};
     for (int k = 0; k < p.n; k++) {
         const L3dSrc& ps = p.src[k];
@@ -420,6 +435,8 @@ int fast_batch(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
     for (int i = 0; i < n; i++) {
         long long off = per_view_offsets ? s->offv[refs[i]] : 0;
         L3dFastView v = fast_view(s, refs[i], &opts[i], off);
+        /* batched coarse planes sit at the coarse level's per-view offsets */
+        if (v.has_coarse && per_view_offsets) v.coarse_off = s->opts.coarse->offv[refs[i]];
         v.tile_start = tiles;
         s->fviews_host[i] = v;
         s->tile_start_host[i] = tiles;
@@ -447,6 +464,7 @@ int fast_batch(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
     d.cost = cost;
     d.prior = prior;
     d.depths = s->depths;
+    d.coarse = nullptr;
     *out = d;
     return L3D_OK;
 }
@@ -569,7 +587,6 @@ int fast_solve(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
     bool any_pack = false;
     for (int i = 0; i < n; i++) {
         if (std::min(opts[i].n_sources, L3D_MAX_SOURCES) == 0) continue;  /* dense-stereo.ts:233 */
-        if (opts[i].from_coarse) return fail(L3D_EINVAL, "the fast form has no coarse-to-fine start");
         r.push_back(refs[i]);
         o.push_back(opts[i]);
         max_it = std::max(max_it, opts[i].iterations);
@@ -577,13 +594,32 @@ int fast_solve(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
         nn++;
     }
     if (nn == 0) return L3D_OK;
-    bool any_prior = false;
-    for (auto& q : o) any_prior |= q.prior != nullptr && !q.geometric;
-    if (all && s->graphs && !any_prior) return fast_solve_graph(s, r, o, max_it, any_pack);
+    bool any_prior = false, any_coarse = false;
+    for (auto& q : o) {
+        any_prior |= q.prior != nullptr && !q.geometric;
+        any_coarse |= q.from_coarse != 0;
+    }
+    /* coarse-to-fine: a single view starts from the coarse level's last solve of that view, a
+     * batch from the coarse level's batched planes of its views */
+    const float4* coarse = nullptr;
+    if (any_coarse) {
+        const l3d_stereo* c = s->opts.coarse;
+        if (all) {
+            if (!c->hyp_all) return fail(L3D_ESTATE, "the coarse level has no batched planes (solve_all it first)");
+            coarse = c->hyp_all;
+        } else {
+            if (c->hyp_ref != r[0]) return fail(L3D_ESTATE, "the coarse level's planes are of view %d, not %d", c->hyp_ref, r[0]);
+            coarse = c->hyp;
+        }
+        L3D_CUDA(cudaEventRecord(c->done, c->stream), "event record");
+        L3D_CUDA(cudaStreamWaitEvent(s->stream, c->done, 0), "stream wait");
+    }
+    if (all && s->graphs && !any_prior && !any_coarse) return fast_solve_graph(s, r, o, max_it, any_pack);
     L3dFastDev d;
     int rc = all ? fast_batch(s, nn, r.data(), o.data(), s->hyp_all, s->cost_all, s->prior_all, true, &d)
                  : fast_batch(s, nn, r.data(), o.data(), s->hyp, s->cost, s->prior, false, &d);
     if (rc) return rc;
+    d.coarse = coarse;
     return fast_schedule(s, d, max_it, any_pack);
 }
 

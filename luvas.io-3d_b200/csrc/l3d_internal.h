@@ -124,6 +124,12 @@ struct L3dFastView {
     unsigned long long ref_tex;
     int has_prior;
     int pack;                  /* store the packed depth map in the pack launch */
+    /* coarse-to-fine start (init_coarse, patchmatch.wgsl.ts:296-333) */
+    float ck[4];               /* coarse-level intrinsics */
+    int cW, cH;
+    long long coarse_off;      /* element offset of this view's planes in L3dFastDev.coarse */
+    int has_coarse;
+    int pad_;
     L3dFastSrc src[L3D_MAX_SOURCES];
 };
 
@@ -139,6 +145,7 @@ struct L3dFastDev {
     float* cost;               /* cost_all */
     const float* prior;        /* prior_all (rows of views with has_prior) */
     uint32_t* depths;
+    const float4* coarse;      /* coarse level's planes (views with has_coarse) or NULL */
 };
 
 /* kernel: L3D_K_INIT or L3D_K_PROPAGATE; iteration/phase select the RNG stream and the

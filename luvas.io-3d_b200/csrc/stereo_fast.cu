@@ -432,6 +432,35 @@ __global__ void __launch_bounds__(128) k_fast_init(const L3dFastDev d) {
         const long long index = (long long)y * sv.W + xx;
         float3 n = f.random_normal(s);
         float dd = f.random_depth(s);
+        if (sv.has_coarse && d.coarse) {
+            /* init_coarse (patchmatch.wgsl.ts:296-333): the random plane against the planes of
+             * the four nearest coarse pixels, re-intersected with this pixel's ray */
+            float c = f.hypothesis_cost(s, n, dd);
+            const float qx = ((s.px + 0.5f) * (float)sv.cW) / (float)sv.W - 0.5f;
+            const float qy = ((s.py + 0.5f) * (float)sv.cH) / (float)sv.H - 0.5f;
+            const int bx = (int)floorf(qx), by = (int)floorf(qy);
+            for (int corner = 0; corner < 4; corner++) {
+                const int cx = min(max(bx + (corner & 1), 0), sv.cW - 1);
+                const int cy = min(max(by + (corner >> 1), 0), sv.cH - 1);
+                const float4 h = d.coarse[sv.coarse_off + (long long)cy * sv.cW + cx];
+                if (!(h.w > 0.0f)) continue;
+                const float3 hn = make_float3(h.x, h.y, h.z);
+                const float3 point = make_float3(((float)cx - sv.ck[2]) / sv.ck[0] * h.w,
+                                                 ((float)cy - sv.ck[3]) / sv.ck[1] * h.w, h.w);
+                const float den = dot3f(hn, s.ray);
+                if (fabsf(den) < 1e-6f) continue;
+                const float hd = dot3f(hn, point) / den;
+                const float hc = f.hypothesis_cost(s, hn, hd);
+                if (hc < c) {
+                    c = hc;
+                    n = hn;
+                    dd = hd;
+                }
+            }
+            d.hyp[sv.pix_off + index] = make_float4(n.x, n.y, n.z, dd);
+            d.cost[sv.pix_off + index] = c;
+            continue;
+        }
         if (sv.flags & 1u) {
             uint32_t packed = d.depths[sv.ref_dep_off + index];
             if (unpack_depth(packed) > 0.0f) {
