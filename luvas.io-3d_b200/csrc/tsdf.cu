@@ -24,6 +24,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cuda_fp16.h>
+
 #include "l3d_fmath.h"
 #include "l3d_internal.h"
 
@@ -100,15 +102,15 @@ __device__ __forceinline__ bool observe(const L3dTsdfGrid& g, const L3dTsdfView&
 /* observe() with the same results, reordered for the many-view sweep: the depth and the
  * truncation test come first (most voxels of a view lie behind the surface or outside the
  * truncation band), and the decoded normal comes from `normals`, a table of unpack_normal over
- * all 4096 normal codes computed with the same arithmetic. */
+ * all 4096 normal codes computed with the same arithmetic.  The voxel's world position
+ * (fma(i + 0.5, voxel, origin), the same for every view) comes from the caller, and the f16
+ * depth is widened by the hardware conversion, which gives l3d_f16_to_f32's value for every
+ * non-NaN half (a NaN fails the d > 0 test either way). */
 __device__ __forceinline__ bool observe_lut(const L3dTsdfGrid& g, const L3dTsdfView& v,
                                             const uint32_t* __restrict__ depth,
                                             const float* __restrict__ prior,
-                                            const float4* __restrict__ normals, int gx, int gy,
-                                            int gz, float* obs, float* wout) {
-    float wx = fmaf((float)gx + 0.5f, g.voxel, g.origin[0]);
-    float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
-    float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
+                                            const float4* __restrict__ normals, float wx, float wy,
+                                            float wz, float* obs, float* wout) {
     const float* R = v.R;
     float3 cam = make_float3(fmaf(R[2], wz, fmaf(R[1], wy, fmaf(R[0], wx, v.t[0]))),
                              fmaf(R[5], wz, fmaf(R[4], wy, fmaf(R[3], wx, v.t[1]))),
@@ -120,7 +122,7 @@ __device__ __forceinline__ bool observe_lut(const L3dTsdfGrid& g, const L3dTsdfV
     if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)v.W && ry < (float)v.H)) return false;
     long long i = (long long)(int)ry * v.W + (int)rx;
     uint32_t packed = __ldg(depth + i);
-    float d = l3d_f16_to_f32(packed & 0xffffu);
+    float d = __half2float(__ushort_as_half((unsigned short)(packed & 0xffffu)));
     const bool stereo = d > 0.0f;
     if (!stereo) d = prior ? __ldg(prior + i) : 0.0f;
     if (!(d > 0.0f)) return false;
@@ -317,6 +319,11 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
     float t[VEC];
     float wf[VEC];
     uint32_t wq[VEC];
+    float wx[VEC];
+#pragma unroll
+    for (int j = 0; j < VEC; j++) wx[j] = fmaf((float)(gx + j) + 0.5f, g.voxel, g.origin[0]);
+    const float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
+    const float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
     bool loaded = false;
     for (int vi = 0; vi < n_views; vi++) {
         if (!mask[(long long)vi * g.bricks + brick]) continue;
@@ -326,7 +333,7 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
 #pragma unroll
         for (int j = 0; j < VEC; j++) {
             float obs, w;
-            if (!observe_lut(g, v, depth, prior, normals, gx + j, gy, gz, &obs, &w)) continue;
+            if (!observe_lut(g, v, depth, prior, normals, wx[j], wy, wz, &obs, &w)) continue;
             if (!loaded) {
                 loaded = true;
 #pragma unroll
