@@ -292,6 +292,8 @@ def main():
     ap.add_argument("--tsdf-dim", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--storage", default="f16", choices=["f16", "u8", "f32", "bf16"],
+                    help="fast-form image storage")
     ap.add_argument("--variant", type=int, default=-1,
                     help="fast-form kernel variant; default: the autotuner's choice")
     args = ap.parse_args()
@@ -315,8 +317,9 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
-    from luvas3d import (DTYPE_F16, DTYPE_F32, FORM_FAST, FORM_PLAIN, DenseStereo,
-                         IntegrationView, SolveOptions, StereoOptions, TsdfVolume)
+    from luvas3d import (DTYPE_BF16, DTYPE_F16, DTYPE_F32, DTYPE_U8, FORM_FAST, FORM_PLAIN,
+                         DenseStereo, IntegrationView, SolveOptions, StereoOptions, TsdfVolume)
+    from luvas3d.packing import unpack_depth
 
     w = build_workload(args)
     V = len(w.views)
@@ -342,7 +345,8 @@ def main():
     tuned = {}
 
     def make_stereo(form):
-        storage = DTYPE_F16 if form == FORM_FAST else DTYPE_F32
+        storage = {"f16": DTYPE_F16, "u8": DTYPE_U8, "f32": DTYPE_F32, "bf16": DTYPE_BF16}[args.storage] \
+            if form == FORM_FAST else DTYPE_F32
         st = DenseStereo(w.width, w.height, w.views,
                          StereoOptions(storage=storage, form=form, stream=sptr), sizes=sizes)
         for i, im in enumerate(w.images):
@@ -416,14 +420,35 @@ def main():
                     "launches": launches, "prop_ms": prop_ms,
                     "px_iters_per_s": px_iters_step * steps * world / pm_s}
 
+    def accuracy(st) -> dict:
+        """Packed depth maps of the last full solve against the rendered ground truth, scored
+        like the reference's stereo self-test (frontend/tools/verify/stereo-check.ts:55-77):
+        surface pixels (truth > 0) with a non-zero packed entry count as valid; relative error of
+        the packed half depth, median and p90, over all views of this rank."""
+        errs, surf, valid = [], 0, 0
+        for r in refs:
+            packed = st.depth_map(r)
+            t = w.truth[r]
+            m = t > 0
+            ok = m & (packed != 0)
+            surf += int(m.sum())
+            valid += int(ok.sum())
+            errs.append(np.abs(unpack_depth(packed[ok]) - t[ok]) / t[ok])
+        e = np.concatenate(errs)
+        return {"valid_fraction": round(valid / max(1, surf), 4),
+                "median_rel_err": float(np.percentile(e, 50)),
+                "p90_rel_err": float(np.percentile(e, 90))}
+
     plain_steps = max(1, min(args.steps, 2)) if args.form == "auto" else args.steps
     res = {}
+    acc = {}
     stereo = None
     forms = {"auto": [FORM_PLAIN, FORM_FAST], "plain": [FORM_PLAIN], "fast": [FORM_FAST]}[args.form]
     for form in forms:
         chosen = form == forms[-1]
         st, r = time_form(form, args.steps if chosen else plain_steps, args.warmup, chosen)
         res[form] = r
+        acc["fast" if form == FORM_FAST else "plain"] = accuracy(st)
         if chosen:
             stereo = st
         else:
@@ -443,6 +468,35 @@ def main():
     achieved = prop_flops / (R["prop_ms"] / 1e3) / 1e12
     sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    roof_fp32 = {"kernel": (f"k_fast_propagate (all {V} views, one colour)"
+                            if chosen_form == FORM_FAST else "k_propagate (one view, one colour)"),
+                 "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                 "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                 "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 flops) at "
+                                "the sampled median SM clock",
+                 "launch_ms": R["prop_ms"], "flop_per_launch": prop_flops,
+                 "flop_model": "14 candidates x sources x (18 + 36 x 37 + 15) + 936 per "
+                               "pixel of the colour"}
+    # the fast propagate kernel is bound by the texture data pipe: quote its bilinear samples
+    # against the rate a probe kernel with the same thread layout measures on this GPU
+    roof_tex = None
+    if chosen_form == FORM_FAST and args.storage != "bf16":
+        import ctypes as C
+        from luvas3d import _lib
+        rate = C.c_double()
+        dt = {"f16": DTYPE_F16, "u8": DTYPE_U8, "f32": DTYPE_F32}[args.storage]
+        _lib.check(_lib.load().l3d_measure_texture_rate(dt, 1, C.byref(rate)))
+        samples = 14 * S * 36 * (w.pixels / V / 2) * views_per_launch
+        got = samples / (R["prop_ms"] / 1e3) / 1e9
+        peak_tex = rate.value / 1e9
+        roof_tex = {"kernel": roof_fp32["kernel"], "bound": "texture", "achieved": got,
+                    "peak": peak_tex, "unit": "Gsample/s", "frac": got / peak_tex, "traffic": None,
+                    "peak_source": f"measured: l3d_measure_texture_rate({args.storage}, one "
+                                   "red/black colour), bilinear samples/s of a 2048x2048 texture",
+                    "launch_ms": R["prop_ms"], "samples_per_launch": samples,
+                    "sample_model": "14 candidates x sources x 36 bilinear samples per pixel of "
+                                    "the colour (the reference's count; sources the corner test "
+                                    "rejects are counted although not sampled)"}
     tsdf_ms = sum(R["ms"]["tsdf"]) / len(R["ms"]["tsdf"])
     tsdf_bytes = vox * 12
     tsdf_gbs = tsdf_bytes / (tsdf_ms / 1e3) / 1e9
@@ -502,7 +556,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "px-iters/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": R["st_s"] * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f16 images, f32 arithmetic" if chosen_form == FORM_FAST else "f32",
+        "dtype": f"{args.storage} images, f32 arithmetic" if chosen_form == FORM_FAST else "f32",
         "data": "synthetic (seeded sphere-on-plane scene, value-noise texture)",
         "config": {"workload": workload_name(w),
                    "form": "fast" if chosen_form == FORM_FAST else "plain",
@@ -512,21 +566,15 @@ def main():
                    "parallelism": f"replica x{world}"},
         "tsdf_voxel_updates_per_s": voxel_updates / R["ts_s"],
         "stage_ms": stage(R),
+        "depth_accuracy": acc,
         "plain": ({"px_iters_per_s": res[FORM_PLAIN]["px_iters_per_s"],
                    "stage_ms": stage(res[FORM_PLAIN]),
                    "propagate_launch_ms": res[FORM_PLAIN]["prop_ms"]}
                   if FORM_PLAIN in res else None),
         "speedup_vs_plain": (value / res[FORM_PLAIN]["px_iters_per_s"]
                              if FORM_PLAIN in res and chosen_form != FORM_PLAIN else None),
-        "roofline": {"kernel": (f"k_fast_propagate (all {V} views, one colour)"
-                                if chosen_form == FORM_FAST else "k_propagate (one view, one colour)"),
-                     "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                     "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
-                     "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 flops) at "
-                                    "the sampled median SM clock",
-                     "launch_ms": R["prop_ms"], "flop_per_launch": prop_flops,
-                     "flop_model": "14 candidates x sources x (18 + 36 x 37 + 15) + 936 per "
-                                   "pixel of the colour"},
+        "roofline": roof_tex or roof_fp32,
+        "roofline_fp32": roof_fp32,
         "roofline_tsdf": {"kernel": f"k_integrate_many ({V} views per sweep)", "bound": "hbm",
                           "achieved": tsdf_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                           "frac": tsdf_gbs / peaks.get("hbm_gbs", 6650.0),

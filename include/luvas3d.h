@@ -432,6 +432,14 @@ int l3d_tsdf_backward(l3d_tsdf* t, const l3d_integration_view* view, int32_t wid
                       const float* grad_weight_out, float* grad_depth, float* grad_tsdf_in,
                       float* grad_weight_in, void* stream);
 
+/* Measures the bilinear sample rate of this device's texture unit on a 2048 x 2048 texture of
+ * `dtype` (L3D_DTYPE_U8, _F16 or _F32) set up like the fast form's images, with a 6 x 6 window
+ * dilated by 2 per pixel and the propagate kernel's thread layout; `checker` != 0 samples the
+ * pixels of one red/black colour.  No counterpart in the reference: it is the measured peak
+ * that the fast propagate kernel, bound by the texture pipe, is quoted against.  Allocates and
+ * frees its own buffers and stream; blocks until the probe is done. */
+int l3d_measure_texture_rate(int32_t dtype, int32_t checker, double* samples_per_second);
+
 /* Largest volume, in 8^3 bricks, that l3d_tsdf_integrate_noalloc accepts (a dense grid has
  * ceil(X/8) * ceil(Y/8) * ceil(Z/8) bricks; 2^20 covers 768^3). */
 #define L3D_NOALLOC_MAX_BRICKS (1 << 20)

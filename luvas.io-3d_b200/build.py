@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "luvas3d", "lib")
 
-CUDA_SOURCES = ["capi.cu", "stereo.cu", "stereo_fast.cu", "tsdf.cu", "noalloc.cu", "grad.cu", "cloud.cu", "scan.cu", "mesh.cu", "image.cu"]
+CUDA_SOURCES = ["capi.cu", "stereo.cu", "stereo_fast.cu", "tsdf.cu", "noalloc.cu", "grad.cu", "cloud.cu", "scan.cu", "mesh.cu", "image.cu", "probe.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "--fmad=false", "-std=c++17",

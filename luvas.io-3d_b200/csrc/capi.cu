@@ -2561,4 +2561,77 @@ int l3d_depth_upsample(const float* grid, int32_t grid_width, int32_t grid_heigh
     return L3D_OK;
 }
 
+/* ------------------------------------------------------------------ texture-rate probe ----- */
+
+int l3d_measure_texture_rate(int32_t dtype, int32_t checker, double* samples_per_second) {
+    if (!samples_per_second) return fail(L3D_EINVAL, "NULL output");
+    if (dtype != L3D_DTYPE_U8 && dtype != L3D_DTYPE_F16 && dtype != L3D_DTYPE_F32)
+        return fail(L3D_EINVAL, "texture-rate probe: dtype must be u8, f16 or f32");
+    *samples_per_second = 0.0;
+    const int W = 2048, H = 2048, reps = 32, launches = 3;
+    const long long blocks = l3d_texture_rate_blocks(W, H, checker ? 1 : 0);
+    cudaChannelFormatDesc ch = dtype == L3D_DTYPE_F16  ? cudaCreateChannelDescHalf()
+                               : dtype == L3D_DTYPE_U8 ? cudaCreateChannelDesc<unsigned char>()
+                                                       : cudaCreateChannelDesc<float>();
+    const size_t es = dtype_size(dtype);
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    void* fill = nullptr;
+    float* out = nullptr;
+    cudaError_t e = cudaSuccess;
+    const char* what = "";
+    auto step = [&](cudaError_t r, const char* w) {
+        if (e == cudaSuccess && r != cudaSuccess) {
+            e = r;
+            what = w;
+        }
+        return e == cudaSuccess;
+    };
+    if (step(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream creation") &&
+        step(cudaEventCreate(&ev[0]), "event creation") && step(cudaEventCreate(&ev[1]), "event creation") &&
+        step(cudaMallocArray(&arr, &ch, W, H), "array allocation") &&
+        step(cudaMalloc(&fill, (size_t)W * H * es), "fill allocation") &&
+        step(cudaMalloc((void**)&out, (size_t)blocks * 128 * sizeof(float)), "output allocation") &&
+        step(cudaMemsetAsync(fill, 0x3c, (size_t)W * H * es, st), "fill") &&
+        step(cudaMemcpy2DToArrayAsync(arr, 0, 0, fill, (size_t)W * es, (size_t)W * es, H,
+                                      cudaMemcpyDeviceToDevice, st), "array fill")) {
+        cudaResourceDesc res;
+        std::memset(&res, 0, sizeof(res));
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = arr;
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof(td));
+        td.addressMode[0] = cudaAddressModeClamp;
+        td.addressMode[1] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = dtype == L3D_DTYPE_U8 ? cudaReadModeNormalizedFloat : cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        if (step(cudaCreateTextureObject(&tex, &res, &td, nullptr), "texture creation") &&
+            step(l3d_launch_texture_rate(tex, W, H, checker ? 1 : 0, reps, out, st), "probe launch") &&
+            step(cudaEventRecord(ev[0], st), "event record")) {
+            for (int i = 0; i < launches; i++)
+                if (!step(l3d_launch_texture_rate(tex, W, H, checker ? 1 : 0, reps, out, st), "probe launch"))
+                    break;
+            float ms = 0.0f;
+            if (step(cudaEventRecord(ev[1], st), "event record") &&
+                step(cudaEventSynchronize(ev[1]), "probe") &&
+                step(cudaEventElapsedTime(&ms, ev[0], ev[1]), "event timing") && ms > 0.0f)
+                *samples_per_second = (double)launches * blocks * 128 * reps * 36 / (ms * 1e-3);
+        }
+    }
+    if (st) cudaStreamSynchronize(st);
+    if (tex) cudaDestroyTextureObject(tex);
+    if (arr) cudaFreeArray(arr);
+    cudaFree(fill);
+    cudaFree(out);
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    if (st) cudaStreamDestroy(st);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    return L3D_OK;
+}
+
 }  // extern "C"
+

@@ -364,4 +364,9 @@ cudaError_t l3d_launch_upsample_depth(const float* grid, int gw, int gh, int W, 
 /* Sets the calling thread's l3d_last_error() message (capi.cu). */
 void l3d_set_error(const char* msg);
 
+/* texture-rate probe (probe.cu) */
+long long l3d_texture_rate_blocks(int width, int height, int checker);
+cudaError_t l3d_launch_texture_rate(cudaTextureObject_t tex, int width, int height, int checker,
+                                    int reps, float* out, cudaStream_t s);
+
 #endif

@@ -82,6 +82,10 @@ def test_bad_arguments_are_rejected_with_a_message():
     assert lib.l3d_tsdf_read(None, None, None) == _lib.L3D_EINVAL
     lib.l3d_stereo_destroy(None)
     lib.l3d_tsdf_destroy(None)
+    rate = C.c_double(-1.0)
+    assert lib.l3d_measure_texture_rate(_lib.DTYPE_BF16, 1, C.byref(rate)) == _lib.L3D_EINVAL
+    assert "dtype" in _lib.last_error()
+    assert lib.l3d_measure_texture_rate(_lib.DTYPE_F16, 1, None) == _lib.L3D_EINVAL
 
 
 def test_python_layer_raises_typed_errors():
