@@ -519,12 +519,11 @@ def main():
             stereo.solve_all(refs, opts)
             stereo.filter_all(refs, w.sources, w.needed)
             tsdf.reset()
-            tsdf.integrate_many(iviews, stereo=stereo, layers=refs)
             for r in refs:
                 _lib.check(lib.l3d_stereo_read_filtered_layer(
                     stereo._h(), r, C.c_void_p(out_f[int(f_off[r]):].data_ptr())))
-            _lib.check(lib.l3d_tsdf_read(tsdf._h(), C.c_void_p(out_t.data_ptr()),
-                                         C.c_void_p(out_w.data_ptr())))
+            # the sweep with the volume's read-back overlapped (l3d_tsdf_integrate_many_read)
+            tsdf.integrate_many_read(iviews, stereo=stereo, layers=refs, out=(out_t, out_w))
 
         e2e_step()
         torch.cuda.synchronize()
@@ -541,8 +540,9 @@ def main():
                "unit": "px-iters/s", "h2d_bytes_per_step": w.pixels * 4,
                "d2h_bytes_per_step": w.pixels * 4 + vox * 6,
                "ms_per_step": float(e2e_s.item()) * 1e3 / args.steps,
-               "includes": "image upload from pinned host memory, PatchMatch, filter, TSDF, "
-                           "read-back of the filtered maps and the TSDF volume"}
+               "includes": "image upload from pinned host memory, PatchMatch, filter, "
+                           "read-back of the filtered maps, TSDF sweep with the volume's "
+                           "read-back overlapped (l3d_tsdf_integrate_many_read)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

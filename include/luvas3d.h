@@ -271,6 +271,15 @@ int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packe
 int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
                             const uint32_t* packed, int32_t n, const l3d_integration_view* views);
 
+/* integrate_many followed by read(): the same volume, bit for bit, in the same host buffers
+ * (weight is float* or uint16_t* as for l3d_tsdf_read; either may be NULL, not both), with the
+ * read-back overlapped with the sweep: the sweep runs over consecutive voxel ranges and each
+ * range is copied out while the next is integrated.  Returns when the copies are done.  Host
+ * buffers from cudaHostAlloc / cudaHostRegister overlap fully; pageable ones still work. */
+int l3d_tsdf_integrate_many_read(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                                 const uint32_t* packed, int32_t n,
+                                 const l3d_integration_view* views, float* tsdf, void* weight);
+
 /* TsdfVolume.read() (tsdf-volume.ts:475-482).  weight is float* (F32) or uint16_t* (Q8).
  * Either pointer may be NULL. */
 int l3d_tsdf_read(l3d_tsdf* t, float* tsdf, void* weight);

@@ -26,6 +26,10 @@
  * bilinear on the pair image) + 8 for the 2x2 quad lane mapping. */
 #define L3D_FAST_DEFAULT_VARIANT 14
 
+/* Voxel ranges the sweep of l3d_tsdf_integrate_many_read is split into, each read back as soon
+ * as it is done. */
+#define L3D_TSDF_READ_SLABS 8
+
 namespace {
 
 thread_local std::string g_error;
@@ -1313,6 +1317,8 @@ struct l3d_tsdf {
     L3dTsdfView* views_host = nullptr;      /* pinned staging for views */
     const uint32_t** ptrs_host = nullptr;   /* pinned staging for depth pointers */
     long long launches = 0;
+    cudaStream_t copy = nullptr;      /* read-back stream of integrate_many_read */
+    cudaEvent_t slab_done[L3D_TSDF_READ_SLABS] = {};
 };
 
 namespace {
@@ -1547,8 +1553,12 @@ int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packe
     return L3D_OK;
 }
 
-int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
-                            const uint32_t* packed, int32_t n, const l3d_integration_view* views) {
+/* Body of l3d_tsdf_integrate_many and l3d_tsdf_integrate_many_read: with output buffers the
+ * sweep runs as L3D_TSDF_READ_SLABS launches over consecutive voxel ranges, and each range is
+ * copied out on the copy stream as soon as its launch is done. */
+static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                          const uint32_t* packed, int32_t n, const l3d_integration_view* views,
+                          float* tsdf_out, void* weight_out) {
     if (!t) return fail(L3D_EINVAL, "NULL handle");
     if (n < 0 || (n > 0 && !views)) return fail(L3D_EINVAL, "bad view list");
     if (n == 0) return L3D_OK;
@@ -1605,12 +1615,61 @@ int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* l
     cudaError_t e = l3d_launch_tsdf_visible(t->g, t->views, n, t->coords, t->mask, t->stream);
     t->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "visibility launch");
-    e = l3d_launch_tsdf_many(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
-                             t->normals, t->tsdf, t->weight, t->q8, t->stream);
-    t->launches++;
-    if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
+    if (!tsdf_out && !weight_out) {
+        e = l3d_launch_tsdf_many(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
+                                 t->normals, t->tsdf, t->weight, t->q8, t->stream);
+        t->launches++;
+        if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
+    } else {
+        if (!t->copy) {
+            L3D_CUDA(cudaStreamCreateWithFlags(&t->copy, cudaStreamNonBlocking), "stream creation");
+            for (cudaEvent_t& ev : t->slab_done)
+                L3D_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event creation");
+        }
+        int vpu = 1;
+        const long long units = l3d_tsdf_sweep_units(t->g, &vpu);
+        const long long per = (units + L3D_TSDF_READ_SLABS - 1) / L3D_TSDF_READ_SLABS;
+        /* every launch first, so that a copy into pageable memory (which blocks the host until
+         * it is done) does not hold back the next launch */
+        for (int i = 0; i < L3D_TSDF_READ_SLABS; i++) {
+            const long long q0 = std::min(units, i * per), q1 = std::min(units, q0 + per);
+            e = l3d_launch_tsdf_many_range(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs,
+                                           t->priors, t->normals, t->tsdf, t->weight, t->q8, q0, q1,
+                                           t->stream);
+            t->launches += q1 > q0 ? 1 : 0;
+            if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
+            L3D_CUDA(cudaEventRecord(t->slab_done[i], t->stream), "event record");
+        }
+        const size_t wsize = t->q8 ? 2 : 4;
+        for (int i = 0; i < L3D_TSDF_READ_SLABS; i++) {
+            const long long v0 = std::min(units, i * per) * vpu;
+            const long long v1 = std::min(units, i * per + per) * vpu;
+            if (v1 <= v0) continue;
+            L3D_CUDA(cudaStreamWaitEvent(t->copy, t->slab_done[i], 0), "stream wait");
+            if (tsdf_out)
+                L3D_CUDA(cudaMemcpyAsync(tsdf_out + v0, t->tsdf + v0, (size_t)(v1 - v0) * 4,
+                                         cudaMemcpyDeviceToHost, t->copy), "read tsdf");
+            if (weight_out)
+                L3D_CUDA(cudaMemcpyAsync((char*)weight_out + v0 * wsize, (char*)t->weight + v0 * wsize,
+                                         (size_t)(v1 - v0) * wsize, cudaMemcpyDeviceToHost, t->copy),
+                         "read weight");
+        }
+        L3D_CUDA(cudaStreamSynchronize(t->copy), "read");
+    }
     if (src && (rc = before_stereo(t, src))) return rc;
     return L3D_OK;
+}
+
+int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                            const uint32_t* packed, int32_t n, const l3d_integration_view* views) {
+    return integrate_many(t, src, layers, packed, n, views, nullptr, nullptr);
+}
+
+int l3d_tsdf_integrate_many_read(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                                 const uint32_t* packed, int32_t n,
+                                 const l3d_integration_view* views, float* tsdf, void* weight) {
+    if (!tsdf && !weight) return fail(L3D_EINVAL, "no output buffer");
+    return integrate_many(t, src, layers, packed, n, views, tsdf, weight);
 }
 
 /* Shared body of l3d_tsdf_forward_depth / l3d_tsdf_backward. */
@@ -1722,6 +1781,10 @@ void l3d_tsdf_destroy(l3d_tsdf* t) {
     cudaFreeHost(t->ptrs_host);
     if (t->done) cudaEventDestroy(t->done);
     if (t->staged) cudaEventDestroy(t->staged);
+    if (t->copy) cudaStreamSynchronize(t->copy);
+    for (cudaEvent_t ev : t->slab_done)
+        if (ev) cudaEventDestroy(ev);
+    if (t->copy) cudaStreamDestroy(t->copy);
     if (t->own_stream && t->stream) cudaStreamDestroy(t->stream);
     delete t;
 }

@@ -180,6 +180,14 @@ cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_
                                  const uint32_t* const* depth_ptrs_dev, const float* priors,
                                  const float4* normals, float* tsdf, void* weight, int q8,
                                  cudaStream_t stream);
+/* The sweep's work units (voxel runs of *voxels_per_unit along x, in voxel-index order) and a
+ * sweep over units [q_begin, q_end) only: voxels [q_begin, q_end) * voxels_per_unit. */
+long long l3d_tsdf_sweep_units(const L3dTsdfGrid& g, int* voxels_per_unit);
+cudaError_t l3d_launch_tsdf_many_range(const L3dTsdfGrid& g, const L3dTsdfView* views_dev,
+                                       int n_views, const int32_t* coords, const uint8_t* mask,
+                                       const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                       const float4* normals, float* tsdf, void* weight, int q8,
+                                       long long q_begin, long long q_end, cudaStream_t stream);
 cudaError_t l3d_launch_tsdf_fill(float* tsdf, void* weight, long long voxels, int q8,
                                  cudaStream_t stream);
 

@@ -310,9 +310,10 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
                                                         const float* __restrict__ priors,
                                                         const float4* __restrict__ normals,
                                                         float* __restrict__ tsdf,
-                                                        void* __restrict__ weight, long long quads) {
-    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= quads) return;
+                                                        void* __restrict__ weight,
+                                                        long long q_begin, long long q_end) {
+    long long q = q_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= q_end) return;
     int gx, gy, gz;
     long long idx, brick;
     if (!quad_coords<VEC>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
@@ -566,23 +567,39 @@ cudaError_t l3d_launch_normal_table(float4* normals, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+long long l3d_tsdf_sweep_units(const L3dTsdfGrid& g, int* voxels_per_unit) {
+    const int vec = vec4_ok(g) ? 4 : 1;
+    if (voxels_per_unit) *voxels_per_unit = vec;
+    return quad_count(g, vec);
+}
+
+cudaError_t l3d_launch_tsdf_many_range(const L3dTsdfGrid& g, const L3dTsdfView* views_dev,
+                                       int n_views, const int32_t* coords, const uint8_t* mask,
+                                       const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                       const float4* normals, float* tsdf, void* weight, int q8,
+                                       long long q_begin, long long q_end, cudaStream_t stream) {
+    const int vec = vec4_ok(g) ? 4 : 1;
+    q_end = q_end < quad_count(g, vec) ? q_end : quad_count(g, vec);
+    if (q_end <= q_begin || n_views == 0) return cudaSuccess;
+    unsigned blocks = (unsigned)((q_end - q_begin + 255) / 256);
+    if (vec == 4) {
+        if (q8) k_integrate_many<4, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, q_begin, q_end);
+        else k_integrate_many<4, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, q_begin, q_end);
+    } else {
+        if (q8) k_integrate_many<1, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, q_begin, q_end);
+        else k_integrate_many<1, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, q_begin, q_end);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
                                  const int32_t* coords, const uint8_t* mask,
                                  const uint32_t* const* depth_ptrs_dev, const float* priors,
                                  const float4* normals, float* tsdf, void* weight, int q8,
                                  cudaStream_t stream) {
-    const int vec = vec4_ok(g) ? 4 : 1;
-    long long quads = quad_count(g, vec);
-    if (quads == 0 || n_views == 0) return cudaSuccess;
-    unsigned blocks = (unsigned)((quads + 255) / 256);
-    if (vec == 4) {
-        if (q8) k_integrate_many<4, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
-        else k_integrate_many<4, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
-    } else {
-        if (q8) k_integrate_many<1, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
-        else k_integrate_many<1, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, quads);
-    }
-    return cudaGetLastError();
+    return l3d_launch_tsdf_many_range(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors,
+                                      normals, tsdf, weight, q8, 0, l3d_tsdf_sweep_units(g, nullptr),
+                                      stream);
 }
 
 cudaError_t l3d_launch_tsdf_depth(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,

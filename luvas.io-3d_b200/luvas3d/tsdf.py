@@ -76,6 +76,24 @@ class IntegrationView:
     confidence: float = 0.0
 
 
+def _host_ptr(a, count: int, itemsize: int):
+    """Address of a host buffer of at least `count` elements of `itemsize` bytes: a C-contiguous
+    numpy array or a contiguous CPU tensor.  None stays None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        ok = a.flags.c_contiguous and a.size >= count and a.itemsize == itemsize
+        addr = a.ctypes.data
+    else:
+        if getattr(a, "is_cuda", False):
+            raise ValueError("integrate_many_read writes host buffers, not device tensors")
+        ok = a.is_contiguous() and a.numel() >= count and a.element_size() == itemsize
+        addr = a.data_ptr()
+    if not ok:
+        raise ValueError(f"host buffer must be contiguous with >= {count} elements of {itemsize} bytes")
+    return C.c_void_p(addr)
+
+
 def _c_view(v: IntegrationView, keep: list):
     cv = _lib.IntegrationView()
     k = v.intrinsics
@@ -178,6 +196,39 @@ class TsdfVolume:
             keep.append(p)
         if keep:
             self.synchronize()
+
+    def integrate_many_read(self, views: Sequence[IntegrationView], depths=None, stereo=None,
+                            layers: Sequence[int] | None = None, out=None):
+        """integrate_many() then read(), with the read-back overlapped with the sweep.  `out`:
+        optional (tsdf, weight) host buffers of voxels elements each (pinned memory, e.g.
+        torch's pin_memory(), overlaps fully); returns them shaped like read()'s."""
+        keep: list = []
+        arr = (_lib.IntegrationView * len(views))(*[_c_view(v, keep) for v in views])
+        tsdf, weight = out if out is not None else self._host_volume()
+        tp = _host_ptr(tsdf, self.voxels, 4)
+        wp = _host_ptr(weight, self.voxels, 2 if self.weight_q8 else 4)
+        if stereo is not None:
+            lay = np.asarray(layers if layers is not None else range(len(views)), dtype=np.int32)
+            _lib.check(self._lib.l3d_tsdf_integrate_many_read(
+                self._h(), stereo._h(), lay.ctypes.data_as(C.POINTER(C.c_int32)), None,
+                len(views), arr, tp, wp))
+        else:
+            p = np.ascontiguousarray(depths, dtype=np.uint32)
+            _lib.check(self._lib.l3d_tsdf_integrate_many_read(self._h(), None, None, _lib.ptr(p),
+                                                              len(views), arr, tp, wp))
+            keep.append(p)
+        return self._shaped(tsdf, weight)
+
+    def _host_volume(self) -> tuple[np.ndarray, np.ndarray]:
+        n = self.voxels
+        return (np.empty(n, dtype=np.float32),
+                np.empty(n, dtype=np.uint16 if self.weight_q8 else np.float32))
+
+    def _shaped(self, tsdf, weight):
+        if self.dims is not None and isinstance(tsdf, np.ndarray):
+            X, Y, Z = self.dims
+            return tsdf.reshape(Z, Y, X), weight.reshape(Z, Y, X)
+        return tsdf, weight
 
     def read(self) -> tuple[np.ndarray, np.ndarray]:
         """read (tsdf-volume.ts:475-482): (tsdf f32, weight f32 or uint16 Q8.8)."""

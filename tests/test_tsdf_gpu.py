@@ -92,6 +92,54 @@ def test_integrate_many_equals_sequence(scene):
         assert_bit_equal(wb, wa, "weight")
 
 
+@pytest.mark.parametrize("layout", ["dense", "ragged", "pool"])
+@pytest.mark.parametrize("q8", [False, True])
+def test_integrate_many_read_equals_sweep_then_read(scene, layout, q8):
+    """The sweep split into voxel ranges with overlapped read-back gives the volume of
+    integrate_many + read, bit for bit, into pageable numpy and pinned torch buffers."""
+    import torch
+    views, maps = scene
+    W, H = 120, 90
+    iv = [gpu_view(v, confidence=1.5) for v in views]
+    if layout == "pool":
+        voxel = 0.03
+        grid = BrickGrid((-1.3, -1.2, -1.3), voxel, (2.6, 2.4, 2.6))
+        rng = np.random.default_rng(2)
+        pts = rng.normal(size=(2000, 3))
+        pts /= np.linalg.norm(pts, axis=1, keepdims=True)
+        for p in pts:
+            grid.mark(*p, voxel * 4)
+        coords, lookup, count = grid.build()
+
+        def make():
+            return TsdfVolume(W, H, voxel, grid.origin, grid=grid, layout=(coords, lookup, count),
+                              weight_q8=q8)
+    else:
+        dims = (64, 48, 56) if layout == "dense" else (37, 21, 29)
+
+        def make():
+            return TsdfVolume(W, H, 0.04, (-1.28, -1.1, -1.1), dense=dims, truncation=0.12,
+                              weight_q8=q8)
+    a, b, c = make(), make(), make()
+    a.integrate_many(iv, depths=np.stack(maps))
+    ta, wa = a.read()
+    tb, wb = b.integrate_many_read(iv, depths=np.stack(maps))
+    assert_bit_equal(tb, ta, "tsdf")
+    assert_bit_equal(wb, wa, "weight")
+    n = c.voxels
+    pt = torch.empty(n, dtype=torch.float32).pin_memory()
+    pw = torch.empty(n, dtype=torch.int16 if q8 else torch.float32).pin_memory()
+    c.integrate_many_read(iv, depths=np.stack(maps), out=(pt, pw))
+    assert_bit_equal(pt.numpy().reshape(ta.shape), ta, "tsdf (pinned)")
+    assert_bit_equal(pw.numpy().view(wa.dtype).reshape(wa.shape), wa, "weight (pinned)")
+    # weight only, then a second sweep on top (the read-back leaves the volume in place)
+    _, w2 = b.integrate_many_read(iv, depths=np.stack(maps), out=(None, np.empty_like(wb).reshape(-1)))
+    a.integrate_many(iv, depths=np.stack(maps))
+    assert_bit_equal(w2.reshape(-1), a.read()[1].reshape(-1), "weight after two sweeps")
+    with pytest.raises(ValueError):
+        b.integrate_many_read(iv, depths=np.stack(maps), out=(np.empty(3, np.float32), None))
+
+
 def test_brick_pool_and_prior_bit_exact(scene):
     views, maps = scene
     W, H = 120, 90
