@@ -1,7 +1,7 @@
 """TSDF parity: the CUDA integration kernels through the C ABI against the FP32 oracle.
 
 The per-voxel arithmetic is the oracle's, so tsdf values and weights (f32 or Q8.8 uint16) are
-compared bit for bit; the north-star tolerance (TSDF 1e-5 absolute, integer weights exact) is met
+compared bit for bit; the required tolerance (TSDF 1e-5 absolute, integer weights exact) is met
 with margin zero.  The many-view sweep must equal the per-view launches in order.
 """
 import numpy as np
