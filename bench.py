@@ -278,6 +278,225 @@ def run_polish(args) -> None:
     st.destroy()
 
 
+def run_fusion(args):
+    """The rows on either side of the stereo stage, on the scan workload (48 views 640x480):
+    image preparation from 1280x960 RGBA camera frames (rgbaToGray by block means and by the
+    area filter, RGB thumbnails), the coarse-to-fine schedule of the High profile (6 iterations
+    at 320x240, then 4 at 640x480 from the coarse planes, against 5 single-scale iterations),
+    the dense point cloud (consistency filter + addDepthMap of every view with the cell budget
+    of the High profile), the TSDF sweep and surface extraction (surface nets + normals, then
+    removeSmallComponents(0.01, 200)).  Every stage runs on one stream and is timed with CUDA
+    events there, after a warm-up run; a CPU-oracle sample of each stage runs on the host
+    cores.  `value` is camera pixels per second through the whole chain."""
+    import torch
+
+    import oracle
+    from luvas3d import (DTYPE_F16, FORM_FAST, DenseStereo, IntegrationView, SolveOptions,
+                         StereoOptions, TsdfVolume, scenes)
+    from luvas3d import image as I
+    from luvas3d import mesh as M
+    from luvas3d.camera import StereoView, scale_intrinsics
+    from luvas3d.cloud import FusionView, fuse_depth_maps
+    from luvas3d.packing import unpack_depth
+
+    w = scenes.scan(n_views=args.views or 48, tsdf_dim=args.tsdf_dim or 512)
+    V, W, H = len(w.views), w.width, w.height
+    refs = list(range(V))
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    peaks, peak_kind = _peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+
+    def timed(fn, reps: int = 1):
+        """Device ms of fn() on the bench stream (median of `reps` after one warm-up run)."""
+        with torch.cuda.stream(stream):
+            fn()
+            out = []
+            for _ in range(reps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                b.synchronize()
+                out.append(a.elapsed_time(b))
+        return statistics.median(out)
+
+    def host_s(fn):
+        t0 = time.perf_counter()
+        fn()
+        return time.perf_counter() - t0
+
+    # camera frames: the scan's gray images at 2x, as RGBA with a colour tint (synthetic)
+    with torch.cuda.stream(stream):
+        g = torch.stack([torch.from_numpy(np.ascontiguousarray(im)) for im in w.images]).cuda()
+        g = (g.clamp(0, 1) * 255).to(torch.uint8)
+        g2 = g.repeat_interleave(2, dim=1).repeat_interleave(2, dim=2)
+        rgba = torch.stack([g2, (g2.int() * 7 // 8).to(torch.uint8), (g2.int() * 3 // 4).to(torch.uint8),
+                            torch.full_like(g2, 255)], dim=-1).contiguous()
+    torch.cuda.synchronize()
+    FW, FH = rgba.shape[2], rgba.shape[1]
+    grays, thumbs = [None] * V, [None] * V
+
+    def prep_block():
+        for v in refs:
+            grays[v] = I.rgba_to_gray(rgba[v], W, H)
+
+    def prep_area():
+        for v in refs:
+            I.rgba_to_gray(rgba[v], 600, 450)
+
+    def prep_thumbs():
+        for v in refs:
+            thumbs[v] = I.downsample_rgb(rgba[v], 160, 120)
+
+    reps = max(1, args.steps)
+    ms_block, ms_area, ms_thumb = timed(prep_block, reps), timed(prep_area, reps), timed(prep_thumbs, reps)
+    frame_px = V * FW * FH
+    image = {
+        "rgba_to_gray_blocks": {"ms": ms_block, "frame_px_per_s": frame_px / (ms_block / 1e3),
+                                "hbm_frac": frame_px * 4 / (ms_block / 1e3) / 1e9 / hbm},
+        "rgba_to_gray_area_600x450": {"ms": ms_area, "frame_px_per_s": frame_px / (ms_area / 1e3)},
+        "thumbnails_160x120": {"ms": ms_thumb, "frame_px_per_s": frame_px / (ms_thumb / 1e3)},
+    }
+    fr0 = rgba[0].cpu().numpy()
+    cpu_img = host_s(lambda: oracle.rgba_to_gray(fr0, W, H))
+    image["cpu_oracle_frame_px_per_s"] = FW * FH / cpu_img
+    thumbs_host = [t.cpu().numpy() for t in thumbs]
+    grays_host = [t.cpu().numpy() for t in grays]
+
+    # stereo, single-scale (5 iterations) and the High profile's coarse-to-fine (6 + 4)
+    so = StereoOptions(storage=DTYPE_F16, form=FORM_FAST, stream=sptr)
+    single = DenseStereo(W, H, w.views, so)
+    for v in refs:
+        single.set_image(v, grays_host[v])
+    single.set_graphs(True)
+    o5 = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=5) for r in refs]
+    ms_single = timed(lambda: single.solve_all(refs, o5), reps)
+    cw, ch = W // 2, H // 2
+    cviews = [StereoView(scale_intrinsics(v.intrinsics, cw / W, ch / H), v.pose) for v in w.views]
+    coarse = DenseStereo(cw, ch, cviews, StereoOptions(depth_maps=False, storage=DTYPE_F16,
+                                                       form=FORM_FAST, stream=sptr))
+    fine = DenseStereo(W, H, w.views, StereoOptions(coarse=coarse, storage=DTYPE_F16, form=FORM_FAST,
+                                                    stream=sptr))
+    for v in refs:
+        coarse.set_image(v, I.downsample_gray(grays[v], cw, ch).cpu().numpy())
+        fine.set_image(v, grays_host[v])
+    oc = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=6, pack=False)
+          for r in refs]
+    of = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=4, from_coarse=True)
+          for r in refs]
+
+    def c2f():
+        coarse.solve_all(refs, oc)
+        fine.solve_all(refs, of)
+
+    ms_c2f = timed(c2f, reps)
+
+    def acc(st):
+        errs, surf, valid = [], 0, 0
+        for r in refs:
+            packed = st.depth_map(r)
+            t = w.truth[r]
+            m = t > 0
+            ok = m & (packed != 0)
+            surf += int(m.sum())
+            valid += int(ok.sum())
+            errs.append(np.abs(unpack_depth(packed[ok]) - t[ok]) / t[ok])
+        e = np.concatenate(errs)
+        return {"valid_fraction": round(valid / max(1, surf), 4),
+                "median_rel_err": float(np.percentile(e, 50)), "p90_rel_err": float(np.percentile(e, 90))}
+
+    px_c2f = V * (cw * ch * 6 + W * H * 4)
+    stereo = {
+        "single_scale_5": {"ms": ms_single, "px_iters_per_s": V * W * H * 5 / (ms_single / 1e3),
+                           "depth_accuracy": acc(single)},
+        "coarse_to_fine_6_4": {"ms": ms_c2f, "px_iters_per_s": px_c2f / (ms_c2f / 1e3),
+                               "depth_accuracy": acc(fine)},
+    }
+
+    # dense cloud: filter + addDepthMap per view (fuseDepthMaps), on the single-scale maps
+    fviews = [FusionView(w.views[r], w.sources[r], w.needed[r], thumbs_host[r]) for r in refs]
+    cell, budget = w.tsdf_voxel, 600_000
+    cloud_out = {}
+
+    def fuse():
+        pc, final_cell = fuse_depth_maps(single, fviews, cell, budget)
+        cloud_out["points"], cloud_out["cell"] = int(pc.positions.shape[0]), final_cell
+
+    ms_cloud = timed(fuse, reps)
+    f0 = single.filtered_map(0, w.sources[0], w.needed[0])
+    oc0 = oracle.Cloud(cell)
+    cpu_cloud = host_s(lambda: oc0.add_map(f0, w.views[0], thumbs_host[0]))
+    cloud = {"ms": ms_cloud, "px_per_s": V * W * H / (ms_cloud / 1e3), "points": cloud_out["points"],
+             "final_cell_m": cloud_out["cell"],
+             "cpu_oracle_px_per_s": W * H / cpu_cloud,
+             "note": "GPU: consistency filter + addDepthMap of every view, with the budget check "
+                     "(a host round trip) after each view; CPU oracle: addDepthMap of one "
+                     "already-filtered map"}
+
+    # TSDF sweep of the filtered maps and surface extraction
+    vox = int(np.prod(w.tsdf_dims))
+    tsdf = TsdfVolume(W, H, w.tsdf_voxel, w.tsdf_origin, dense=w.tsdf_dims,
+                      truncation=w.tsdf_truncation, weight_q8=True, stream=sptr)
+    iviews = [IntegrationView(v.intrinsics, v.pose, w.ranges[i][1]) for i, v in enumerate(w.views)]
+    single.filter_all(refs, w.sources, w.needed)
+
+    def sweep():
+        tsdf.reset()
+        tsdf.integrate_many(iviews, stereo=single, layers=refs)
+
+    ms_tsdf = timed(sweep, reps)
+    mesh_out = {}
+
+    def surface():
+        m = M.extract_surface_device(tsdf, 0.6)
+        r = m.remove_small_components(0.01, 200)
+        mesh_out["raw"], mesh_out["kept"] = m.counts, r.counts
+        r.destroy()
+        m.destroy()
+
+    ms_mesh = timed(surface, reps)
+    # CPU oracle sample: surface nets of a 128^3 crop at the volume's centre, brick-major
+    t_all, w_all = tsdf.read()
+    X0, Y0, Z0 = (np.array(w.tsdf_dims) // 2 - 64)
+    crop_t = t_all[Z0:Z0 + 128, Y0:Y0 + 128, X0:X0 + 128]
+    crop_w = w_all[Z0:Z0 + 128, Y0:Y0 + 128, X0:X0 + 128].astype(np.float32) / 256.0
+
+    def bricks(a):
+        b = a.reshape(16, 8, 16, 8, 16, 8).transpose(0, 2, 4, 1, 3, 5)  # bz by bx, z y x
+        return np.ascontiguousarray(b).reshape(-1)
+
+    origin = [w.tsdf_origin[0] + X0 * w.tsdf_voxel, w.tsdf_origin[1] + Y0 * w.tsdf_voxel,
+              w.tsdf_origin[2] + Z0 * w.tsdf_voxel]
+    lookup = np.arange(16 ** 3, dtype=np.int32)
+    bt, bw = bricks(crop_t), bricks(crop_w)
+    cpu_mesh = host_s(lambda: oracle.extract_surface(origin, w.tsdf_voxel, (16, 16, 16), lookup, bt, bw, 0.6))
+    surface_line = {"ms": ms_mesh, "voxels_per_s": vox / (ms_mesh / 1e3),
+                    "vertices_indices": [int(x) for x in mesh_out["raw"]],
+                    "after_remove_small_components": [int(x) for x in mesh_out["kept"]],
+                    "cpu_oracle_voxels_per_s": 128 ** 3 / cpu_mesh}
+
+    total_ms = ms_block + ms_thumb + ms_single + ms_cloud + ms_tsdf + ms_mesh
+    line = {
+        "metric": "camera px/s through image prep, PatchMatch, filter, dense cloud, TSDF and surface",
+        "value": V * FW * FH / (total_ms / 1e3), "unit": "frame-px/s", "n_gpus": 1,
+        "steps": reps, "warmup": 1, "ms_per_step": total_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8 frames, f16 images, f32/f64 arithmetic",
+        "data": "synthetic (seeded sphere-on-plane scene, value-noise texture)",
+        "config": {"workload": f"fusion: scan {V} views, frames {FW}x{FH} RGBA -> {W}x{H} gray, "
+                               f"TSDF {w.tsdf_dims[0]}^3, cloud cell {cell * 1e3:.0f} mm, budget {budget}",
+                   "timing": "CUDA events on the one stream every handle uses, median of the steps "
+                             "after a warm-up run (the calls that read counts back include those "
+                             "host round trips)"},
+        "image_prep": image, "stereo": stereo, "dense_cloud": cloud,
+        "tsdf_sweep": {"ms": ms_tsdf, "voxel_updates_per_s": vox * V / (ms_tsdf / 1e3)},
+        "surface": surface_line, "hbm_peak_source": peak_kind,
+    }
+    print(json.dumps(line), flush=True)
+    for h in (tsdf, fine, coarse, single):
+        h.destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -285,7 +504,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="auto", choices=["auto", "plain", "fast"])
-    ap.add_argument("--workload", default="scan", choices=["scan", "room", "polish"])
+    ap.add_argument("--workload", default="scan", choices=["scan", "room", "polish", "fusion"])
     ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--width", type=int, default=640)
     ap.add_argument("--height", type=int, default=480)
@@ -312,6 +531,10 @@ def main():
     if args.workload == "polish":
         if rank == 0:
             run_polish(args)
+        return
+    if args.workload == "fusion":
+        if rank == 0:
+            run_fusion(args)
         return
     if world > 1:
         from datetime import timedelta

@@ -1812,10 +1812,12 @@ struct l3d_cloud {
 
 namespace {
 
-void free_table(L3dCloudTable& t) {
-    cudaFree(t.keys);
-    cudaFree(t.sums);
-    cudaFree(t.counts);
+/* Tables are stream-ordered allocations: growing or coarsening the table does not wait for the
+ * whole device. */
+void free_table(L3dCloudTable& t, cudaStream_t s) {
+    if (t.keys) cudaFreeAsync(t.keys, s);
+    if (t.sums) cudaFreeAsync(t.sums, s);
+    if (t.counts) cudaFreeAsync(t.counts, s);
     t = L3dCloudTable{};
 }
 
@@ -1823,14 +1825,14 @@ int alloc_table(l3d_cloud* c, int capacity, L3dCloudTable* out) {
     L3dCloudTable t{};
     t.capacity = capacity;
     cudaError_t e;
-    if ((e = cudaMalloc(&t.keys, (size_t)capacity * 8)) != cudaSuccess ||
-        (e = cudaMalloc(&t.sums, (size_t)capacity * 9 * 8)) != cudaSuccess ||
-        (e = cudaMalloc(&t.counts, (size_t)capacity * 4)) != cudaSuccess) {
-        free_table(t);
+    if ((e = cudaMallocAsync((void**)&t.keys, (size_t)capacity * 8, c->stream)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&t.sums, (size_t)capacity * 9 * 8, c->stream)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&t.counts, (size_t)capacity * 4, c->stream)) != cudaSuccess) {
+        free_table(t, c->stream);
         return cuda_fail(e, "point table allocation");
     }
     if ((e = l3d_launch_cloud_clear(t, c->stream)) != cudaSuccess) {
-        free_table(t);
+        free_table(t, c->stream);
         return cuda_fail(e, "point table clear");
     }
     c->launches++;
@@ -1861,11 +1863,10 @@ int cloud_rebuild(l3d_cloud* c, int capacity, double cell) {
     cudaError_t e = l3d_launch_cloud_rebin(c->t, nt, cell, c->counters, c->err, c->stream);
     c->launches++;
     if (e != cudaSuccess) {
-        free_table(nt);
+        free_table(nt, c->stream);
         return cuda_fail(e, "rebin launch");
     }
-    L3D_CUDA(cudaStreamSynchronize(c->stream), "synchronize");
-    free_table(c->t);
+    free_table(c->t, c->stream);
     c->t = nt;
     c->cell = cell;
     return L3D_OK;
@@ -2105,8 +2106,8 @@ int64_t l3d_cloud_launches(const l3d_cloud* c) { return c ? c->launches : -1; }
 
 void l3d_cloud_destroy(l3d_cloud* c) {
     if (!c) return;
+    free_table(c->t, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    free_table(c->t);
     cudaFree(c->counters);
     cudaFree(c->err);
     cudaFree(c->thumb);
@@ -2131,16 +2132,19 @@ struct l3d_mesh {
 
 namespace {
 
-/* Device buffers freed when the holder goes out of scope. */
+/* Scratch buffers allocated and freed in the order of stream `s` (no device-wide wait), freed
+ * when the holder goes out of scope. */
 struct DevBufs {
+    cudaStream_t s;
     std::vector<void*> ptrs;
+    explicit DevBufs(cudaStream_t stream) : s(stream) {}
     ~DevBufs() {
-        for (void* p : ptrs) cudaFree(p);
+        for (void* p : ptrs) cudaFreeAsync(p, s);
     }
     template <typename T>
     cudaError_t get(T** p, size_t count) {
         *p = nullptr;
-        cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+        cudaError_t e = cudaMallocAsync((void**)p, std::max<size_t>(count, 1) * sizeof(T), s);
         if (e == cudaSuccess) ptrs.push_back(*p);
         return e;
     }
@@ -2165,7 +2169,7 @@ void mesh_free(l3d_mesh* m) {
 int extract_mesh(const L3dSdfView& v, long long bricks, cudaStream_t s, l3d_mesh** out) {
     const long long cells = bricks * 512;
     if (cells >= (1ll << 31)) return fail(L3D_EINVAL, "volume too large for surface extraction");
-    DevBufs tmp;
+    DevBufs tmp(s);
     uint32_t *flag, *base, *qcount, *qbase, *scratch, *total;
     int32_t* cell_vertex;
     L3D_CUDA(tmp.get(&flag, cells), "surface buffers");
@@ -2253,7 +2257,7 @@ int l3d_tsdf_extract_surface(l3d_tsdf* t, double min_weight, l3d_mesh** out) {
     for (int i = 0; i < 3; i++) v.origin[i] = t->g.origin_d[i];
     v.voxel = t->g.voxel_d;
     v.min_weight = min_weight;
-    DevBufs tmp;
+    DevBufs tmp(t->stream);
     long long bricks;
     if (t->g.dense) {
         v.dense = 1;
@@ -2307,7 +2311,7 @@ int l3d_extract_surface(const l3d_sdf_bricks* vol, double min_weight, l3d_mesh**
             cudaStreamDestroy(s);
         }
     } guard{s};
-    DevBufs tmp;
+    DevBufs tmp(s);
     int32_t *dl, *dc;
     float *dt, *dw;
     const size_t voxels = (size_t)vol->bricks * 512;
@@ -2364,7 +2368,7 @@ int l3d_mesh_remove_small_components(const l3d_mesh* m, double fraction, int32_t
             cudaStreamDestroy(s);
         }
     } guard{s};
-    DevBufs tmp;
+    DevBufs tmp(s);
     uint32_t *label, *comp, *kept, *first, *face_base, *marks, *rank, *scratch, *total;
     int* changed;
     L3D_CUDA(tmp.get(&label, nv), "component buffers");
@@ -2453,7 +2457,7 @@ int l3d_brick_grid_build(const double origin[3], double voxel, const double exte
             cudaStreamDestroy(s);
         }
     } guard{s};
-    DevBufs tmp;
+    DevBufs tmp(s);
     uint8_t* marks;
     float* pts;
     uint32_t *flags, *base, *scratch, *total;
