@@ -309,7 +309,10 @@ int l3d_cloud_create(double cell, void* stream, l3d_cloud** out);
  * point (FP64), a world normal and the colour of the nearest thumbnail pixel (thumb_rgb: host,
  * thumb_w * thumb_h * 3 bytes), added to its cell.  Give exactly one of `src` (its last
  * l3d_stereo_filter result stays on the device; width and height are ignored) or `packed`
- * (host, width * height).  `view` is the depth map's camera. */
+ * (host, width * height).  `view` is the depth map's camera.  The add is queued on the
+ * cloud's stream; an add that leaves the table room returns without waiting for the device, so
+ * a sample outside the table's range (more than 2^20 cells from the origin) is reported by the
+ * next call that reads the table back (size, coarsen, read, or an add that must grow it). */
 int l3d_cloud_add(l3d_cloud* c, const l3d_stereo* src, const uint32_t* packed, int32_t width,
                   int32_t height, const l3d_view* view, const uint8_t* thumb_rgb, int32_t thumb_w,
                   int32_t thumb_h);

@@ -1808,6 +1808,7 @@ struct l3d_cloud {
     double* pts = nullptr;            /* uploaded samples */
     size_t pts_cap = 0;
     long long launches = 0;
+    long long used_bound = 0;         /* host-side upper bound of the used slots */
 };
 
 namespace {
@@ -1851,6 +1852,7 @@ int cloud_state(l3d_cloud* c, unsigned* used) {
         return fail(L3D_EINVAL, "a point lies more than 2^20 cells from the origin (cell %g m)", c->cell);
     if (err & L3D_CLOUD_ERR_FULL) return fail(L3D_ECUDA, "point table overflow");
     if (used) *used = h[0];
+    c->used_bound = h[0];
     return L3D_OK;
 }
 
@@ -1872,17 +1874,46 @@ int cloud_rebuild(l3d_cloud* c, int capacity, double cell) {
     return L3D_OK;
 }
 
+/* Indices of `keys` in ascending key order: least-significant-digit radix sort, 8 bits a pass,
+ * passes whose digit is the same for every key skipped. */
+std::vector<uint32_t> radix_order(const std::vector<unsigned long long>& keys) {
+    const size_t n = keys.size();
+    std::vector<uint32_t> order(n), next(n);
+    for (size_t i = 0; i < n; i++) order[i] = (uint32_t)i;
+    for (int shift = 0; shift < 64; shift += 8) {
+        size_t count[257] = {0};
+        for (size_t i = 0; i < n; i++) count[((keys[i] >> shift) & 255u) + 1]++;
+        bool one_digit = false;
+        for (int d = 1; d <= 256; d++) one_digit |= count[d] == n;
+        if (one_digit) continue;
+        for (int d = 0; d < 256; d++) count[d + 1] += count[d];
+        for (size_t j = 0; j < n; j++) {
+            const uint32_t i = order[j];
+            next[count[(keys[i] >> shift) & 255u]++] = i;
+        }
+        order.swap(next);
+    }
+    return order;
+}
+
 /* Grows the table (grow(), point-accumulator.ts:77-79) until `extra` new cells keep the load
  * at or under 60 %. */
 int cloud_reserve(l3d_cloud* c, long long extra) {
+    /* every sample adds at most one cell: while the bound kept on the host leaves room, the
+     * table state need not be read back (no host round trip) */
+    if ((c->used_bound + extra) * 10 <= (long long)c->t.capacity * 6) {
+        c->used_bound += extra;
+        return L3D_OK;
+    }
     unsigned used = 0;
     int rc = cloud_state(c, &used);
     if (rc) return rc;
     long long cap = c->t.capacity;
     while (((long long)used + extra) * 10 > cap * 6) cap *= 2;
     if (cap > (1ll << 30)) return fail(L3D_ENOMEM, "point table would exceed 2^30 slots");
-    if (cap == c->t.capacity) return L3D_OK;
-    return cloud_rebuild(c, (int)cap, c->cell);
+    if (cap != c->t.capacity && (rc = cloud_rebuild(c, (int)cap, c->cell))) return rc;
+    c->used_bound = (long long)used + extra;
+    return L3D_OK;
 }
 
 template <typename T>
@@ -2038,15 +2069,14 @@ int l3d_cloud_read(l3d_cloud* c, int32_t min_support, int64_t capacity, int64_t*
     unsigned long long* dkey = nullptr;
     cudaError_t e;
     auto cleanup = [&]() {
-        cudaFree(dpos);
-        cudaFree(dnrm);
-        cudaFree(dcol);
-        cudaFree(dsup);
-        cudaFree(dkey);
+        for (void* q : {(void*)dpos, (void*)dnrm, (void*)dcol, (void*)dsup, (void*)dkey})
+            if (q) cudaFreeAsync(q, c->stream);
     };
-    if ((e = cudaMalloc(&dpos, n * 12)) != cudaSuccess || (e = cudaMalloc(&dnrm, n * 12)) != cudaSuccess ||
-        (e = cudaMalloc(&dcol, n * 3)) != cudaSuccess || (e = cudaMalloc(&dsup, n * 2)) != cudaSuccess ||
-        (e = cudaMalloc(&dkey, n * 8)) != cudaSuccess) {
+    if ((e = cudaMallocAsync((void**)&dpos, n * 12, c->stream)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&dnrm, n * 12, c->stream)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&dcol, n * 3, c->stream)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&dsup, n * 2, c->stream)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&dkey, n * 8, c->stream)) != cudaSuccess) {
         cleanup();
         return cuda_fail(e, "read buffers");
     }
@@ -2075,19 +2105,18 @@ int l3d_cloud_read(l3d_cloud* c, int32_t min_support, int64_t capacity, int64_t*
     std::vector<uint16_t> hs(total);
     std::vector<unsigned long long> hk(total);
     if (total &&
-        ((e = cudaMemcpy(hp.data(), dpos, total * 12, cudaMemcpyDeviceToHost)) != cudaSuccess ||
-         (e = cudaMemcpy(hn.data(), dnrm, total * 12, cudaMemcpyDeviceToHost)) != cudaSuccess ||
-         (e = cudaMemcpy(hc.data(), dcol, total * 3, cudaMemcpyDeviceToHost)) != cudaSuccess ||
-         (e = cudaMemcpy(hs.data(), dsup, total * 2, cudaMemcpyDeviceToHost)) != cudaSuccess ||
-         (e = cudaMemcpy(hk.data(), dkey, total * 8, cudaMemcpyDeviceToHost)) != cudaSuccess)) {
+        ((e = cudaMemcpyAsync(hp.data(), dpos, total * 12, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+         (e = cudaMemcpyAsync(hn.data(), dnrm, total * 12, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+         (e = cudaMemcpyAsync(hc.data(), dcol, total * 3, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+         (e = cudaMemcpyAsync(hs.data(), dsup, total * 2, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+         (e = cudaMemcpyAsync(hk.data(), dkey, total * 8, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)) {
         cleanup();
         return cuda_fail(e, "point download");
     }
     cleanup();
-    /* cells in ascending packed order: z, then y, then x */
-    std::vector<uint32_t> order(total);
-    for (uint32_t i = 0; i < total; i++) order[i] = i;
-    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return hk[a] < hk[b]; });
+    /* cells in ascending packed order: z, then y, then x (keys are distinct) */
+    const std::vector<uint32_t> order = radix_order(hk);
     const long long bias = 1 << 20;
     for (uint32_t j = 0; j < total; j++) {
         const uint32_t i = order[j];

@@ -80,17 +80,46 @@ __device__ __forceinline__ void accumulate(const L3dCloudTable& t, int slot, con
     atomicAdd(t.counts + slot, n);
 }
 
-/* addDepthMap (depth-fusion.ts:42-74) for one pixel; unpackDepthSample (depth-maps.ts:66-85). */
+__device__ void sample_of(const L3dCloudView& v, uint32_t value, double d, int x, int y, int W,
+                          int H, const uint8_t* __restrict__ rgb, double* p);
+
+/* addDepthMap (depth-fusion.ts:42-74) for one pixel; unpackDepthSample (depth-maps.ts:66-85).
+ * Neighbouring pixels mostly land in the same cell: the lanes of a warp that share a cell add
+ * their samples up first (in lane order), and one of them claims the cell and adds the sum, so
+ * the table sees one set of atomics per cell and warp instead of one per pixel. */
 __global__ void k_cloud_add_map(const L3dCloudTable t, double cell, const uint32_t* __restrict__ packed,
                                 int W, int H, const L3dCloudView v, const uint8_t* __restrict__ rgb,
                                 unsigned* used, int* err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= W * H) return;
-    const uint32_t value = __ldg(packed + i);
-    if (value == 0u) return;
-    const double d = (double)l3d_f16_to_f32(value & 0xffffu);
-    if (!(d > 0.0)) return;
-    const int x = i % W, y = i / W;
+    const uint32_t value = i < W * H ? __ldg(packed + i) : 0u;
+    const double d = value ? (double)l3d_f16_to_f32(value & 0xffffu) : 0.0;
+    double p[9];
+    unsigned long long key = 0;
+    bool valid = d > 0.0;
+    if (valid) {
+        sample_of(v, value, d, i % W, i / W, W, H, rgb, p);
+        int ix, iy, iz;
+        valid = pack_key(floor(p[0] / cell), floor(p[1] / cell), floor(p[2] / cell), &key, &ix, &iy, &iz);
+        if (!valid) atomicOr(err, L3D_CLOUD_ERR_RANGE);
+    }
+    const unsigned active = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    const unsigned group = __match_any_sync(active, key);
+    double s[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        double acc = 0.0;
+        for (unsigned m = group; m; m &= m - 1u) acc += __shfl_sync(group, p[k], __ffs(m) - 1);
+        s[k] = acc;
+    }
+    if ((int)(threadIdx.x & 31u) != __ffs(group) - 1) return;
+    const int slot = claim(t, p[0] / cell, p[1] / cell, p[2] / cell, used, err);
+    if (slot >= 0) accumulate(t, slot, s, (unsigned)__popc(group));
+}
+
+/* The world sample of one valid pixel (depth d > 0): position, normal, thumbnail colour. */
+__device__ void sample_of(const L3dCloudView& v, uint32_t value, double d, int x, int y, int W,
+                          int H, const uint8_t* __restrict__ rgb, double* p) {
     const double ex = ((double)((value >> 16) & 63u) / 63.0) * 2.0 - 1.0;
     const double ey = ((double)((value >> 22) & 63u) / 63.0) * 2.0 - 1.0;
     double nx = ex, ny = ey;
@@ -109,7 +138,6 @@ __global__ void k_cloud_add_map(const L3dCloudTable t, double cell, const uint32
     const double a0 = ((x - v.k[2]) / v.k[0]) * d - v.t[0];
     const double a1 = ((y - v.k[3]) / v.k[1]) * d - v.t[1];
     const double a2 = d - v.t[2];
-    double p[9];
     p[0] = R[0] * a0 + R[3] * a1 + R[6] * a2;
     p[1] = R[1] * a0 + R[4] * a1 + R[7] * a2;
     p[2] = R[2] * a0 + R[5] * a1 + R[8] * a2;
@@ -123,8 +151,6 @@ __global__ void k_cloud_add_map(const L3dCloudTable t, double cell, const uint32
     p[6] = c[0];
     p[7] = c[1];
     p[8] = c[2];
-    const int slot = claim(t, p[0] / cell, p[1] / cell, p[2] / cell, used, err);
-    if (slot >= 0) accumulate(t, slot, p, 1u);
 }
 
 /* PointAccumulator.add (point-accumulator.ts:29-56) of n samples of 9 doubles. */

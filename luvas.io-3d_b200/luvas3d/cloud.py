@@ -86,18 +86,20 @@ class PointAccumulator:
         _lib.check(self._lib.l3d_cloud_coarsen(self._h(), float(factor)))
 
     def cloud(self, min_support: int = 1) -> PointCloud:
-        n = C.c_int64()
-        _lib.check(self._lib.l3d_cloud_read(self._h(), int(min_support), 0, C.byref(n),
-                                            None, None, None, None, None))
-        k = int(n.value)
+        """cloud(minSupport) (point-accumulator.ts:114-143), ordered by cell.  One read into
+        buffers sized for every occupied cell, trimmed to the points returned."""
+        k = self.size
         out = PointCloud(np.zeros((k, 3), np.float32), np.zeros((k, 3), np.float32),
                          np.zeros((k, 3), np.uint8), np.zeros(k, np.uint16),
                          np.zeros((k, 3), np.int32))
+        n = C.c_int64()
         _lib.check(self._lib.l3d_cloud_read(self._h(), int(min_support), k, C.byref(n),
                                             _lib.ptr(out.positions), _lib.ptr(out.normals),
                                             _lib.ptr(out.colors), _lib.ptr(out.support),
                                             _lib.ptr(out.cells)))
-        return out
+        m = int(n.value)
+        return PointCloud(out.positions[:m], out.normals[:m], out.colors[:m], out.support[:m],
+                          out.cells[:m])
 
     @property
     def launches(self) -> int:

@@ -44,6 +44,20 @@ def test_grows_past_its_initial_capacity():
     np.testing.assert_array_equal(c.cells[:, 0], np.floor(s[:, 0] / 0.001).astype(np.int32))
 
 
+def test_many_small_adds_grow_the_table():
+    """Adds that fit the host-side bound skip the table read-back; the table still grows in
+    time when the bound runs out, and repeated cells are not counted twice."""
+    a = PointAccumulator(0.001)
+    for b in range(150):
+        s = np.zeros((2000, 9))
+        s[:, 0] = (np.arange(2000) + b * 1000) * 0.002   # half of each batch repeats the last
+        s[:, 4], s[:, 6], s[:, 7], s[:, 8] = 1, 1, 2, 3
+        a.add_points(s)
+    assert a.size == 151000
+    c = a.cloud()
+    assert c.support.max() == 2 and int(c.support.sum()) == 300000
+
+
 def test_rejects_cells_out_of_range():
     a = PointAccumulator(1e-6)
     a.add(2.0, 0, 0, 0, 0, 1, 0, 0, 0)          # 2e6 cells from the origin
