@@ -15,6 +15,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -63,6 +64,42 @@ size_t dtype_size(int dtype) {
         case L3D_DTYPE_BF16: return 2;
         default: return 0;
     }
+}
+
+/* Scratch buffers and tables that come and go with each call are stream-ordered allocations
+ * from a memory pool of the library's own on each device, which keeps up to
+ * L3D_POOL_KEEP_BYTES of freed memory mapped for the next call: handing memory back to the
+ * driver at every synchronisation and mapping it again costs milliseconds per GB. */
+#define L3D_POOL_KEEP_BYTES (16ull << 30)
+#define L3D_POOL_DEVICES 64
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[L3D_POOL_DEVICES] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= L3D_POOL_DEVICES) return cudaMallocAsync(p, bytes, s);
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!pools[dev]) {
+            cudaMemPoolProps props;
+            std::memset(&props, 0, sizeof(props));
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaMemPool_t created;
+            if ((e = cudaMemPoolCreate(&created, &props)) != cudaSuccess) return e;
+            uint64_t keep = L3D_POOL_KEEP_BYTES;
+            if ((e = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+                cudaMemPoolDestroy(created);
+                return e;
+            }
+            pools[dev] = created;
+        }
+        pool = pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, s);
 }
 
 template <typename T>
@@ -1826,9 +1863,9 @@ int alloc_table(l3d_cloud* c, int capacity, L3dCloudTable* out) {
     L3dCloudTable t{};
     t.capacity = capacity;
     cudaError_t e;
-    if ((e = cudaMallocAsync((void**)&t.keys, (size_t)capacity * 8, c->stream)) != cudaSuccess ||
-        (e = cudaMallocAsync((void**)&t.sums, (size_t)capacity * 9 * 8, c->stream)) != cudaSuccess ||
-        (e = cudaMallocAsync((void**)&t.counts, (size_t)capacity * 4, c->stream)) != cudaSuccess) {
+    if ((e = pool_alloc((void**)&t.keys, (size_t)capacity * 8, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&t.sums, (size_t)capacity * 9 * 8, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&t.counts, (size_t)capacity * 4, c->stream)) != cudaSuccess) {
         free_table(t, c->stream);
         return cuda_fail(e, "point table allocation");
     }
@@ -1919,11 +1956,10 @@ int cloud_reserve(l3d_cloud* c, long long extra) {
 template <typename T>
 int ensure_upload(T** p, size_t* cap, size_t n, cudaStream_t stream, const char* what) {
     if (*cap >= n) return L3D_OK;
-    cudaStreamSynchronize(stream);
-    cudaFree(*p);
+    if (*p) cudaFreeAsync(*p, stream);
     *p = nullptr;
     *cap = 0;
-    L3D_CUDA(cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)), what);
+    L3D_CUDA(pool_alloc((void**)p, std::max<size_t>(n, 1) * sizeof(T), stream), what);
     *cap = n;
     return L3D_OK;
 }
@@ -1953,8 +1989,8 @@ int l3d_cloud_create(double cell, void* stream, l3d_cloud** out) {
     }
     if ((e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming)) != cudaSuccess)
         return cleanup(cuda_fail(e, "event creation"));
-    if ((e = cudaMalloc(&c->counters, 2 * sizeof(unsigned))) != cudaSuccess ||
-        (e = cudaMalloc(&c->err, sizeof(int))) != cudaSuccess)
+    if ((e = pool_alloc((void**)&c->counters, 2 * sizeof(unsigned), c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&c->err, sizeof(int), c->stream)) != cudaSuccess)
         return cleanup(cuda_fail(e, "counter allocation"));
     if ((e = cudaMemsetAsync(c->counters, 0, 2 * sizeof(unsigned), c->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(c->err, 0, sizeof(int), c->stream)) != cudaSuccess)
@@ -2072,11 +2108,11 @@ int l3d_cloud_read(l3d_cloud* c, int32_t min_support, int64_t capacity, int64_t*
         for (void* q : {(void*)dpos, (void*)dnrm, (void*)dcol, (void*)dsup, (void*)dkey})
             if (q) cudaFreeAsync(q, c->stream);
     };
-    if ((e = cudaMallocAsync((void**)&dpos, n * 12, c->stream)) != cudaSuccess ||
-        (e = cudaMallocAsync((void**)&dnrm, n * 12, c->stream)) != cudaSuccess ||
-        (e = cudaMallocAsync((void**)&dcol, n * 3, c->stream)) != cudaSuccess ||
-        (e = cudaMallocAsync((void**)&dsup, n * 2, c->stream)) != cudaSuccess ||
-        (e = cudaMallocAsync((void**)&dkey, n * 8, c->stream)) != cudaSuccess) {
+    if ((e = pool_alloc((void**)&dpos, n * 12, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&dnrm, n * 12, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&dcol, n * 3, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&dsup, n * 2, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&dkey, n * 8, c->stream)) != cudaSuccess) {
         cleanup();
         return cuda_fail(e, "read buffers");
     }
@@ -2136,12 +2172,9 @@ int64_t l3d_cloud_launches(const l3d_cloud* c) { return c ? c->launches : -1; }
 void l3d_cloud_destroy(l3d_cloud* c) {
     if (!c) return;
     free_table(c->t, c->stream);
+    for (void* q : {(void*)c->counters, (void*)c->err, (void*)c->thumb, (void*)c->map, (void*)c->pts})
+        if (q) cudaFreeAsync(q, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    cudaFree(c->counters);
-    cudaFree(c->err);
-    cudaFree(c->thumb);
-    cudaFree(c->map);
-    cudaFree(c->pts);
     if (c->done) cudaEventDestroy(c->done);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -2173,7 +2206,7 @@ struct DevBufs {
     template <typename T>
     cudaError_t get(T** p, size_t count) {
         *p = nullptr;
-        cudaError_t e = cudaMallocAsync((void**)p, std::max<size_t>(count, 1) * sizeof(T), s);
+        cudaError_t e = pool_alloc((void**)p, std::max<size_t>(count, 1) * sizeof(T), s);
         if (e == cudaSuccess) ptrs.push_back(*p);
         return e;
     }
@@ -2185,11 +2218,13 @@ int read_u32(const uint32_t* dev, uint32_t* host, cudaStream_t s) {
     return L3D_OK;
 }
 
-void mesh_free(l3d_mesh* m) {
+/* Mesh buffers come from the library's pool.  Every mesh call waits for its own work before it
+ * returns, so a mesh handed back to the caller has nothing pending and is freed on the default
+ * stream; error paths free on the stream that may still hold work on the buffers. */
+void mesh_free(l3d_mesh* m, cudaStream_t s = 0) {
     if (!m) return;
-    cudaFree(m->pos);
-    cudaFree(m->nrm);
-    cudaFree(m->idx);
+    for (void* q : {(void*)m->pos, (void*)m->nrm, (void*)m->idx})
+        if (q) cudaFreeAsync(q, s);
     delete m;
 }
 
@@ -2211,7 +2246,7 @@ int extract_mesh(const L3dSdfView& v, long long bricks, cudaStream_t s, l3d_mesh
     l3d_mesh* m = new (std::nothrow) l3d_mesh();
     if (!m) return fail(L3D_ENOMEM, "host allocation failed");
     auto bail = [&](int rc) {
-        mesh_free(m);
+        mesh_free(m, s);
         return rc;
     };
     cudaError_t e;
@@ -2223,8 +2258,8 @@ int extract_mesh(const L3dSdfView& v, long long bricks, cudaStream_t s, l3d_mesh
     if (rc) return bail(rc);
     double* pos_d;
     if ((e = tmp.get(&pos_d, (size_t)nv * 3)) != cudaSuccess ||
-        (e = cudaMalloc(&m->pos, std::max<size_t>(nv, 1) * 12)) != cudaSuccess ||
-        (e = cudaMalloc(&m->nrm, std::max<size_t>(nv, 1) * 12)) != cudaSuccess)
+        (e = pool_alloc((void**)&m->pos, std::max<size_t>(nv, 1) * 12, s)) != cudaSuccess ||
+        (e = pool_alloc((void**)&m->nrm, std::max<size_t>(nv, 1) * 12, s)) != cudaSuccess)
         return bail(cuda_fail(e, "vertex buffers"));
     if ((e = l3d_launch_sn_vertex(v, cells, flag, base, cell_vertex, pos_d, m->pos, s)) != cudaSuccess ||
         (e = l3d_launch_sn_count(v, cells, cell_vertex, qcount, s)) != cudaSuccess ||
@@ -2232,7 +2267,7 @@ int extract_mesh(const L3dSdfView& v, long long bricks, cudaStream_t s, l3d_mesh
         return bail(cuda_fail(e, "surface quads"));
     if ((rc = read_u32(total, &nq, s))) return bail(rc);
     const long long faces = 2ll * nq;
-    if ((e = cudaMalloc(&m->idx, std::max<long long>(faces * 3, 1) * 4)) != cudaSuccess)
+    if ((e = pool_alloc((void**)&m->idx, std::max<long long>(faces * 3, 1) * 4, s)) != cudaSuccess)
         return bail(cuda_fail(e, "index buffer"));
     if ((e = l3d_launch_sn_emit(v, cells, cell_vertex, qcount, qbase, pos_d, m->idx, s)) != cudaSuccess)
         return bail(cuda_fail(e, "surface triangles"));
@@ -2411,12 +2446,15 @@ int l3d_mesh_remove_small_components(const l3d_mesh* m, double fraction, int32_t
     L3D_CUDA(tmp.get(&total, 2), "scan total");
     L3D_CUDA(tmp.get(&changed, 1), "flag");
     L3D_CUDA(l3d_launch_cc_init(nv, label, s), "component labels");
+    /* rounds in batches of 8 between host checks: once the labels have settled a round changes
+     * nothing, so the extra rounds of the last batch leave the result as it is */
     int rounds = 0;
-    for (;; rounds++) {
+    for (;;) {
         if (rounds >= 256) return fail(L3D_ECUDA, "connected components did not settle in 256 rounds");
         int h = 0;
         L3D_CUDA(cudaMemsetAsync(changed, 0, sizeof(int), s), "flag clear");
-        L3D_CUDA(l3d_launch_cc_round(m->idx, faces, nv, label, changed, s), "component round");
+        for (int k = 0; k < 8; k++, rounds++)
+            L3D_CUDA(l3d_launch_cc_round(m->idx, faces, nv, label, changed, s), "component round");
         L3D_CUDA(cudaMemcpyAsync(&h, changed, sizeof(int), cudaMemcpyDeviceToHost, s), "flag read");
         L3D_CUDA(cudaStreamSynchronize(s), "synchronize");
         if (!h) break;
@@ -2437,13 +2475,13 @@ int l3d_mesh_remove_small_components(const l3d_mesh* m, double fraction, int32_t
     l3d_mesh* r = new (std::nothrow) l3d_mesh();
     if (!r) return fail(L3D_ENOMEM, "host allocation failed");
     cudaError_t e;
-    if ((e = cudaMalloc(&r->pos, std::max<size_t>(kv, 1) * 12)) != cudaSuccess ||
-        (e = cudaMalloc(&r->nrm, std::max<size_t>(kv, 1) * 12)) != cudaSuccess ||
-        (e = cudaMalloc(&r->idx, std::max<size_t>(kf, 1) * 12)) != cudaSuccess ||
+    if ((e = pool_alloc((void**)&r->pos, std::max<size_t>(kv, 1) * 12, s)) != cudaSuccess ||
+        (e = pool_alloc((void**)&r->nrm, std::max<size_t>(kv, 1) * 12, s)) != cudaSuccess ||
+        (e = pool_alloc((void**)&r->idx, std::max<size_t>(kf, 1) * 12, s)) != cudaSuccess ||
         (e = l3d_launch_cc_emit(m->idx, faces, kept, face_base, first, rank, m->pos, m->nrm, r->idx,
                                 r->pos, r->nrm, s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess) {
-        mesh_free(r);
+        mesh_free(r, s);
         return cuda_fail(e, "component output");
     }
     r->nv = kv;
@@ -2552,11 +2590,11 @@ HostCover host_coverage(int source, int target) {
 int upload_cover(const HostCover& h, cudaStream_t s, L3dAreaCover* d, std::vector<void*>& owned) {
     int *first, *count;
     double* weights;
-    L3D_CUDA(cudaMallocAsync((void**)&first, h.first.size() * 4, s), "cover table");
+    L3D_CUDA(pool_alloc((void**)&first, h.first.size() * 4, s), "cover table");
     owned.push_back(first);
-    L3D_CUDA(cudaMallocAsync((void**)&count, h.count.size() * 4, s), "cover table");
+    L3D_CUDA(pool_alloc((void**)&count, h.count.size() * 4, s), "cover table");
     owned.push_back(count);
-    L3D_CUDA(cudaMallocAsync((void**)&weights, h.weights.size() * 8, s), "cover table");
+    L3D_CUDA(pool_alloc((void**)&weights, h.weights.size() * 8, s), "cover table");
     owned.push_back(weights);
     L3D_CUDA(cudaMemcpyAsync(first, h.first.data(), h.first.size() * 4, cudaMemcpyHostToDevice, s), "cover upload");
     L3D_CUDA(cudaMemcpyAsync(count, h.count.data(), h.count.size() * 4, cudaMemcpyHostToDevice, s), "cover upload");
@@ -2589,7 +2627,7 @@ int area_resample(const void* src, int is_float, int w, int h, int tw, int th, u
     if (!rc) rc = upload_cover(host_coverage(h, th), s, &rows, owned);
     if (rc) return release(rc);
     float* temp;
-    cudaError_t e = cudaMallocAsync((void**)&temp, (size_t)tw * h * 4, s);
+    cudaError_t e = pool_alloc((void**)&temp, (size_t)tw * h * 4, s);
     if (e != cudaSuccess) return release(cuda_fail(e, "area filter buffer"));
     owned.push_back(temp);
     e = l3d_launch_area(src, is_float, w, h, tw, th, cols, rows, temp, out, s);
@@ -2612,7 +2650,7 @@ int l3d_image_rgba_to_gray(const uint8_t* rgba, int32_t width, int32_t height, i
         return L3D_OK;
     }
     float* luma;
-    L3D_CUDA(cudaMallocAsync((void**)&luma, (size_t)width * height * 4, s), "luma buffer");
+    L3D_CUDA(pool_alloc((void**)&luma, (size_t)width * height * 4, s), "luma buffer");
     cudaError_t e = l3d_launch_luma(rgba, (long long)width * height, luma, s);
     if (e != cudaSuccess) {
         cudaFreeAsync(luma, s);

@@ -297,18 +297,23 @@ __global__ void k_cc_hook(const uint32_t* idx, long long faces, uint32_t* label,
     if (r2 != m && atomicMin(label + r2, m) > m) *changed = 1;
 }
 
+/* Points every vertex on the path from v to its root at the root.  Labels only ever point at
+ * smaller indices and roots do not move here, so concurrent compressions agree. */
 __global__ void k_cc_compress(long long vertices, uint32_t* label, int* changed) {
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= vertices) return;
-    uint32_t r = label[v];
+    uint32_t root = __ldcg(label + v);
     for (int guard = 0; guard < 1 << 20; guard++) {
-        const uint32_t p = __ldcg(label + r);
-        if (p == r) break;
-        r = p;
+        const uint32_t p = __ldcg(label + root);
+        if (p == root) break;
+        root = p;
     }
-    if (label[v] != r) {
-        label[v] = r;
-        *changed = 1;
+    uint32_t x = (uint32_t)v;
+    for (int guard = 0; guard < 1 << 20; guard++) {
+        const uint32_t p = __ldcg(label + x);
+        if (p == root || x == root) break;
+        if (atomicMin(label + x, root) > root) *changed = 1;
+        x = p;
     }
 }
 
