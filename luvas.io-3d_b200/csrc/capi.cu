@@ -1911,28 +1911,6 @@ int cloud_rebuild(l3d_cloud* c, int capacity, double cell) {
     return L3D_OK;
 }
 
-/* Indices of `keys` in ascending key order: least-significant-digit radix sort, 8 bits a pass,
- * passes whose digit is the same for every key skipped. */
-std::vector<uint32_t> radix_order(const std::vector<unsigned long long>& keys) {
-    const size_t n = keys.size();
-    std::vector<uint32_t> order(n), next(n);
-    for (size_t i = 0; i < n; i++) order[i] = (uint32_t)i;
-    for (int shift = 0; shift < 64; shift += 8) {
-        size_t count[257] = {0};
-        for (size_t i = 0; i < n; i++) count[((keys[i] >> shift) & 255u) + 1]++;
-        bool one_digit = false;
-        for (int d = 1; d <= 256; d++) one_digit |= count[d] == n;
-        if (one_digit) continue;
-        for (int d = 0; d < 256; d++) count[d + 1] += count[d];
-        for (size_t j = 0; j < n; j++) {
-            const uint32_t i = order[j];
-            next[count[(keys[i] >> shift) & 255u]++] = i;
-        }
-        order.swap(next);
-    }
-    return order;
-}
-
 /* Grows the table (grow(), point-accumulator.ts:77-79) until `extra` new cells keep the load
  * at or under 60 %. */
 int cloud_reserve(l3d_cloud* c, long long extra) {
@@ -2097,29 +2075,29 @@ int l3d_cloud_read(l3d_cloud* c, int32_t min_support, int64_t capacity, int64_t*
     unsigned used = 0;
     int rc = cloud_state(c, &used);
     if (rc) return rc;
-    const size_t n = std::max<unsigned>(used, 1u);
+    const unsigned sort_n = l3d_cloud_sort_length(std::max<unsigned>(used, 1u));
+    unsigned long long* dkey = nullptr;
+    uint32_t* dslot = nullptr;
     float* dpos = nullptr;
     float* dnrm = nullptr;
     uint8_t* dcol = nullptr;
     uint16_t* dsup = nullptr;
-    unsigned long long* dkey = nullptr;
+    int32_t* dcell = nullptr;
     cudaError_t e;
     auto cleanup = [&]() {
-        for (void* q : {(void*)dpos, (void*)dnrm, (void*)dcol, (void*)dsup, (void*)dkey})
+        for (void* q : {(void*)dkey, (void*)dslot, (void*)dpos, (void*)dnrm, (void*)dcol, (void*)dsup,
+                        (void*)dcell})
             if (q) cudaFreeAsync(q, c->stream);
     };
-    if ((e = pool_alloc((void**)&dpos, n * 12, c->stream)) != cudaSuccess ||
-        (e = pool_alloc((void**)&dnrm, n * 12, c->stream)) != cudaSuccess ||
-        (e = pool_alloc((void**)&dcol, n * 3, c->stream)) != cudaSuccess ||
-        (e = pool_alloc((void**)&dsup, n * 2, c->stream)) != cudaSuccess ||
-        (e = pool_alloc((void**)&dkey, n * 8, c->stream)) != cudaSuccess) {
+    if ((e = pool_alloc((void**)&dkey, (size_t)sort_n * 8, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&dslot, (size_t)sort_n * 4, c->stream)) != cudaSuccess) {
         cleanup();
         return cuda_fail(e, "read buffers");
     }
     unsigned total = 0;
     if ((e = cudaMemsetAsync(c->counters + 1, 0, sizeof(unsigned), c->stream)) != cudaSuccess ||
-        (e = l3d_launch_cloud_emit(c->t, (unsigned)std::max(min_support, 0), c->counters + 1, dpos,
-                                   dnrm, dcol, dsup, dkey, c->stream)) != cudaSuccess ||
+        (e = l3d_launch_cloud_emit_keys(c->t, (unsigned)std::max(min_support, 0), c->counters + 1, dkey,
+                                        dslot, c->stream)) != cudaSuccess ||
         (e = cudaMemcpyAsync(&total, c->counters + 1, sizeof(unsigned), cudaMemcpyDeviceToHost,
                              c->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
@@ -2136,34 +2114,36 @@ int l3d_cloud_read(l3d_cloud* c, int32_t min_support, int64_t capacity, int64_t*
         cleanup();
         return fail(L3D_EINVAL, "output holds %lld points, the cloud has %u", (long long)capacity, total);
     }
-    std::vector<float> hp(total * 3), hn(total * 3);
-    std::vector<uint8_t> hc(total * 3);
-    std::vector<uint16_t> hs(total);
-    std::vector<unsigned long long> hk(total);
-    if (total &&
-        ((e = cudaMemcpyAsync(hp.data(), dpos, total * 12, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
-         (e = cudaMemcpyAsync(hn.data(), dnrm, total * 12, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
-         (e = cudaMemcpyAsync(hc.data(), dcol, total * 3, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
-         (e = cudaMemcpyAsync(hs.data(), dsup, total * 2, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
-         (e = cudaMemcpyAsync(hk.data(), dkey, total * 8, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
-         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)) {
+    /* cells in ascending packed order (z, then y, then x; keys are distinct), sorted and
+     * gathered on the device, then copied straight into the caller's arrays */
+    const size_t m = std::max<unsigned>(total, 1u);
+    if ((e = pool_alloc((void**)&dpos, m * 12, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&dnrm, m * 12, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&dcol, m * 3, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&dsup, m * 2, c->stream)) != cudaSuccess ||
+        (e = pool_alloc((void**)&dcell, m * 12, c->stream)) != cudaSuccess ||
+        (e = l3d_launch_cloud_sort(dkey, dslot, total, sort_n, &c->launches, c->stream)) != cudaSuccess ||
+        (e = l3d_launch_cloud_emit_sorted(c->t, total, dkey, dslot, dpos, dnrm, dcol, dsup, dcell,
+                                          c->stream)) != cudaSuccess) {
         cleanup();
-        return cuda_fail(e, "point download");
+        return cuda_fail(e, "point ordering");
     }
-    cleanup();
-    /* cells in ascending packed order: z, then y, then x (keys are distinct) */
-    const std::vector<uint32_t> order = radix_order(hk);
-    const long long bias = 1 << 20;
-    for (uint32_t j = 0; j < total; j++) {
-        const uint32_t i = order[j];
-        for (int q = 0; q < 3; q++) {
-            if (positions) positions[j * 3 + q] = hp[i * 3 + q];
-            if (normals) normals[j * 3 + q] = hn[i * 3 + q];
-            if (colors) colors[j * 3 + q] = hc[i * 3 + q];
-            if (cells) cells[j * 3 + q] = (int32_t)((long long)((hk[i] >> (21 * q)) & 0x1FFFFFull) - bias);
+    c->launches += total ? 1 : 0;
+    struct Out {
+        void* host;
+        const void* dev;
+        size_t bytes;
+    } outs[] = {{positions, dpos, (size_t)total * 12}, {normals, dnrm, (size_t)total * 12},
+                {colors, dcol, (size_t)total * 3}, {support, dsup, (size_t)total * 2},
+                {cells, dcell, (size_t)total * 12}};
+    for (const Out& o : outs)
+        if (o.host && o.bytes &&
+            (e = cudaMemcpyAsync(o.host, o.dev, o.bytes, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess) {
+            cleanup();
+            return cuda_fail(e, "point download");
         }
-        if (support) support[j] = hs[i];
-    }
+    cleanup();
+    L3D_CUDA(cudaStreamSynchronize(c->stream), "point download");
     return L3D_OK;
 }
 

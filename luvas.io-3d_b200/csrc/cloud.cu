@@ -181,31 +181,100 @@ __global__ void k_cloud_rebin(const L3dCloudTable from, const L3dCloudTable to, 
     if (slot >= 0) accumulate(to, slot, p, n);
 }
 
-/* cloud(minSupport) (point-accumulator.ts:114-143): averaged points of the slots with enough
- * support, in arbitrary order, with their cell keys (the host orders them). */
-__global__ void k_cloud_emit(const L3dCloudTable t, unsigned min_support, unsigned* count,
-                             float* pos, float* nrm, uint8_t* col, uint16_t* support,
-                             unsigned long long* keys) {
+/* cloud(minSupport) (point-accumulator.ts:114-143), in three steps on the device: the cell keys
+ * and slots of the slots with enough support (arbitrary order), the pairs sorted by key, then
+ * the averaged points gathered in key order (cells ascending: z, then y, then x). */
+__global__ void k_cloud_emit_keys(const L3dCloudTable t, unsigned min_support, unsigned* count,
+                                  unsigned long long* keys, uint32_t* slots) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= t.capacity) return;
     const unsigned long long key = t.keys[s];
-    const unsigned n = t.counts[s];
-    if (key == kEmpty || n < min_support) return;
+    if (key == kEmpty || t.counts[s] < min_support) return;
     const unsigned o = atomicAdd(count, 1u);
+    keys[o] = key;
+    slots[o] = (uint32_t)s;
+}
+
+__global__ void k_cloud_emit_sorted(const L3dCloudTable t, unsigned total,
+                                    const unsigned long long* __restrict__ keys,
+                                    const uint32_t* __restrict__ slots, float* pos, float* nrm,
+                                    uint8_t* col, uint16_t* support, int32_t* cells) {
+    const unsigned o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= total) return;
+    const uint32_t s = slots[o];
+    const unsigned long long key = keys[o];
+    const unsigned n = t.counts[s];
     const double* sm = t.sums + (size_t)s * 9;
     const double dn = (double)n;
-    for (int j = 0; j < 3; j++) pos[o * 3 + j] = (float)(sm[j] / dn);
+    for (int j = 0; j < 3; j++) pos[(size_t)o * 3 + j] = (float)(sm[j] / dn);
     double len = sqrt(sm[3] * sm[3] + sm[4] * sm[4] + sm[5] * sm[5]);
     if (!(len != 0.0)) len = 1.0;
-    for (int j = 0; j < 3; j++) nrm[o * 3 + j] = (float)(sm[3 + j] / len);
+    for (int j = 0; j < 3; j++) nrm[(size_t)o * 3 + j] = (float)(sm[3 + j] / len);
     for (int j = 0; j < 3; j++) {
         /* Uint8Array store: truncation, then modulo 256 */
         double c = trunc(sm[6 + j] / dn);
         c = c - 256.0 * floor(c / 256.0);
-        col[o * 3 + j] = (uint8_t)c;
+        col[(size_t)o * 3 + j] = (uint8_t)c;
     }
     support[o] = (uint16_t)min(n, 65535u);
-    keys[o] = key;
+    for (int j = 0; j < 3; j++)
+        cells[(size_t)o * 3 + j] = (int32_t)((long long)((key >> (21 * j)) & 0x1FFFFFull) - kBias);
+}
+
+/* Bitonic sort of n = 2^m (key, value) pairs, m >= 11, ascending by key.  Stages with a
+ * partner distance under 2048 run in shared memory, 2048 pairs per block of 1024 threads. */
+constexpr int kSortTile = 2048;
+
+__global__ void k_pad_keys(unsigned long long* keys, unsigned from, unsigned n) {
+    const unsigned i = from + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) keys[i] = kEmpty;
+}
+
+__device__ __forceinline__ void order_pair(unsigned long long* k, uint32_t* v, unsigned i, unsigned l,
+                                           bool ascending) {
+    const unsigned long long a = k[i], b = k[l];
+    if ((a > b) == ascending) {
+        k[i] = b;
+        k[l] = a;
+        const uint32_t t = v[i];
+        v[i] = v[l];
+        v[l] = t;
+    }
+}
+
+/* stages (k, j) with j < kSortTile: every k from 2 up to kmax when kfrom == 2 (sorts each tile),
+ * or the single k = kfrom with j from kSortTile / 2 down to 1 */
+__global__ void __launch_bounds__(1024) k_bitonic_tile(unsigned long long* keys, uint32_t* vals,
+                                                       unsigned kfrom, unsigned kmax) {
+    __shared__ unsigned long long sk[kSortTile];
+    __shared__ uint32_t sv[kSortTile];
+    const unsigned base = blockIdx.x * kSortTile;
+    for (unsigned i = threadIdx.x; i < kSortTile; i += blockDim.x) {
+        sk[i] = keys[base + i];
+        sv[i] = vals[base + i];
+    }
+    __syncthreads();
+    for (unsigned k = kfrom; k <= kmax; k <<= 1) {
+        for (unsigned j = min(k >> 1, (unsigned)kSortTile >> 1); j > 0; j >>= 1) {
+            const unsigned t = threadIdx.x;
+            const unsigned i = 2 * j * (t / j) + (t % j);
+            order_pair(sk, sv, i, i + j, ((base + i) & k) == 0);
+            __syncthreads();
+        }
+    }
+    for (unsigned i = threadIdx.x; i < kSortTile; i += blockDim.x) {
+        keys[base + i] = sk[i];
+        vals[base + i] = sv[i];
+    }
+}
+
+/* one stage (k, j) with j >= kSortTile over all n / 2 pairs */
+__global__ void k_bitonic_global(unsigned long long* keys, uint32_t* vals, unsigned n, unsigned k,
+                                 unsigned j) {
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n / 2) return;
+    const unsigned i = 2 * j * (t / j) + (t % j);
+    order_pair(keys, vals, i, i + j, (i & k) == 0);
 }
 
 __global__ void k_cloud_clear(L3dCloudTable t) {
@@ -249,10 +318,46 @@ cudaError_t l3d_launch_cloud_rebin(const L3dCloudTable& from, const L3dCloudTabl
     return cudaGetLastError();
 }
 
-cudaError_t l3d_launch_cloud_emit(const L3dCloudTable& t, unsigned min_support, unsigned* count,
-                                  float* pos, float* nrm, uint8_t* col, uint16_t* support,
-                                  unsigned long long* keys, cudaStream_t stream) {
-    k_cloud_emit<<<blocks_for(t.capacity), 256, 0, stream>>>(t, min_support, count, pos, nrm, col,
-                                                             support, keys);
+cudaError_t l3d_launch_cloud_emit_keys(const L3dCloudTable& t, unsigned min_support,
+                                       unsigned* count, unsigned long long* keys, uint32_t* slots,
+                                       cudaStream_t stream) {
+    k_cloud_emit_keys<<<blocks_for(t.capacity), 256, 0, stream>>>(t, min_support, count, keys, slots);
+    return cudaGetLastError();
+}
+
+unsigned l3d_cloud_sort_length(unsigned total) {
+    unsigned n = kSortTile;
+    while (n < total) n <<= 1;
+    return n;
+}
+
+cudaError_t l3d_launch_cloud_sort(unsigned long long* keys, uint32_t* slots, unsigned total,
+                                  unsigned n, long long* launches, cudaStream_t stream) {
+    if (n < (unsigned)kSortTile || (n & (n - 1))) return cudaErrorInvalidValue;
+    long long count = 0;
+    if (n > total) {
+        k_pad_keys<<<blocks_for(n - total), 256, 0, stream>>>(keys, total, n);
+        count++;
+    }
+    const unsigned tiles = n / kSortTile;
+    k_bitonic_tile<<<tiles, 1024, 0, stream>>>(keys, slots, 2, kSortTile);
+    count++;
+    for (unsigned k = 2 * kSortTile; k <= n; k <<= 1) {
+        for (unsigned j = k >> 1; j >= (unsigned)kSortTile; j >>= 1, count++)
+            k_bitonic_global<<<blocks_for(n / 2), 256, 0, stream>>>(keys, slots, n, k, j);
+        k_bitonic_tile<<<tiles, 1024, 0, stream>>>(keys, slots, k, k);
+        count++;
+    }
+    if (launches) *launches += count;
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_cloud_emit_sorted(const L3dCloudTable& t, unsigned total,
+                                         const unsigned long long* keys, const uint32_t* slots,
+                                         float* pos, float* nrm, uint8_t* col, uint16_t* support,
+                                         int32_t* cells, cudaStream_t stream) {
+    if (total == 0) return cudaSuccess;
+    k_cloud_emit_sorted<<<blocks_for(total), 256, 0, stream>>>(t, total, keys, slots, pos, nrm, col,
+                                                              support, cells);
     return cudaGetLastError();
 }

@@ -274,9 +274,19 @@ cudaError_t l3d_launch_cloud_add_points(const L3dCloudTable& t, double cell, con
                                         long long n, unsigned* used, int* err, cudaStream_t stream);
 cudaError_t l3d_launch_cloud_rebin(const L3dCloudTable& from, const L3dCloudTable& to, double cell,
                                    unsigned* used, int* err, cudaStream_t stream);
-cudaError_t l3d_launch_cloud_emit(const L3dCloudTable& t, unsigned min_support, unsigned* count,
-                                  float* pos, float* nrm, uint8_t* col, uint16_t* support,
-                                  unsigned long long* keys, cudaStream_t stream);
+/* cloud read-back: (key, slot) of the slots with at least min_support samples, appended at
+ * *count; the pairs sorted by key on the device (n = l3d_cloud_sort_length(total) entries,
+ * padded); the points gathered in key order. */
+cudaError_t l3d_launch_cloud_emit_keys(const L3dCloudTable& t, unsigned min_support,
+                                       unsigned* count, unsigned long long* keys, uint32_t* slots,
+                                       cudaStream_t stream);
+unsigned l3d_cloud_sort_length(unsigned total);
+cudaError_t l3d_launch_cloud_sort(unsigned long long* keys, uint32_t* slots, unsigned total,
+                                  unsigned n, long long* launches, cudaStream_t stream);
+cudaError_t l3d_launch_cloud_emit_sorted(const L3dCloudTable& t, unsigned total,
+                                         const unsigned long long* keys, const uint32_t* slots,
+                                         float* pos, float* nrm, uint8_t* col, uint16_t* support,
+                                         int32_t* cells, cudaStream_t stream);
 
 /* ---- prefix sums (scan.cu) ---- */
 
