@@ -99,29 +99,35 @@ __device__ __forceinline__ bool observe(const L3dTsdfGrid& g, const L3dTsdfView&
     return true;
 }
 
-/* observe() with the same results, reordered for the many-view sweep: the depth and the
- * truncation test come first (most voxels of a view lie behind the surface or outside the
- * truncation band), and the decoded normal comes from `normals`, a table of unpack_normal over
- * all 4096 normal codes computed with the same arithmetic.  The voxel's world position
- * (fma(i + 0.5, voxel, origin), the same for every view) comes from the caller, and the f16
- * depth is widened by the hardware conversion, which gives l3d_f16_to_f32's value for every
+/* observe() with the same results, reordered for the many-view sweep and split in two.
+ * lut_pixel gives the camera point and the depth-map index of every voxel of a quad first, so
+ * that their depth loads are in flight together; lut_observe finishes from the loaded sample,
+ * with the depth and the truncation test before the weight (most voxels of a view lie behind
+ * the surface or outside the truncation band) and the decoded normal from `normals`, a table of
+ * unpack_normal over all 4096 normal codes computed with the same arithmetic.  The voxel's world
+ * position (fma(i + 0.5, voxel, origin), the same for every view) comes from the caller, and the
+ * f16 depth is widened by the hardware conversion, which gives l3d_f16_to_f32's value for every
  * non-NaN half (a NaN fails the d > 0 test either way). */
-__device__ __forceinline__ bool observe_lut(const L3dTsdfGrid& g, const L3dTsdfView& v,
-                                            const uint32_t* __restrict__ depth,
-                                            const float* __restrict__ prior,
-                                            const float4* __restrict__ normals, float wx, float wy,
-                                            float wz, float* obs, float* wout) {
+__device__ __forceinline__ bool lut_pixel(const L3dTsdfView& v, float wx, float wy, float wz,
+                                          float3* cam_out, int* pix) {
     const float* R = v.R;
     float3 cam = make_float3(fmaf(R[2], wz, fmaf(R[1], wy, fmaf(R[0], wx, v.t[0]))),
                              fmaf(R[5], wz, fmaf(R[4], wy, fmaf(R[3], wx, v.t[1]))),
                              fmaf(R[8], wz, fmaf(R[7], wy, fmaf(R[6], wx, v.t[2]))));
+    *cam_out = cam;
     if (!(cam.z > 0.01f)) return false;
     float iz = 1.0f / cam.z;
     float rx = rintf(fmaf(v.k[0] * cam.x, iz, v.k[2]));
     float ry = rintf(fmaf(v.k[1] * cam.y, iz, v.k[3]));
     if (!(rx >= 0.0f && ry >= 0.0f && rx < (float)v.W && ry < (float)v.H)) return false;
-    long long i = (long long)(int)ry * v.W + (int)rx;
-    uint32_t packed = __ldg(depth + i);
+    *pix = (int)ry * v.W + (int)rx;
+    return true;
+}
+
+__device__ __forceinline__ bool lut_observe(const L3dTsdfGrid& g, const L3dTsdfView& v,
+                                            const float* __restrict__ prior,
+                                            const float4* __restrict__ normals, float3 cam, int i,
+                                            uint32_t packed, float* obs, float* wout) {
     float d = __half2float(__ushort_as_half((unsigned short)(packed & 0xffffu)));
     const bool stereo = d > 0.0f;
     if (!stereo) d = prior ? __ldg(prior + i) : 0.0f;
@@ -331,10 +337,18 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
         const L3dTsdfView& v = views[vi];
         const uint32_t* depth = depths[vi];
         const float* prior = v.has_prior ? priors + v.prior_off : nullptr;
+        float3 cam[VEC];
+        int pix[VEC];
+        bool in[VEC];
+        uint32_t packed[VEC];
+#pragma unroll
+        for (int j = 0; j < VEC; j++) in[j] = lut_pixel(v, wx[j], wy, wz, &cam[j], &pix[j]);
+#pragma unroll
+        for (int j = 0; j < VEC; j++) packed[j] = in[j] ? __ldg(depth + pix[j]) : 0u;
 #pragma unroll
         for (int j = 0; j < VEC; j++) {
             float obs, w;
-            if (!observe_lut(g, v, depth, prior, normals, wx[j], wy, wz, &obs, &w)) continue;
+            if (!in[j] || !lut_observe(g, v, prior, normals, cam[j], pix[j], packed[j], &obs, &w)) continue;
             if (!loaded) {
                 loaded = true;
 #pragma unroll
