@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256) k_integrate(const L3dTsdfGrid g, const L3
 }
 
 template <int VEC, bool Q8>
-__global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
+__global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
                                                         const L3dTsdfView* __restrict__ views,
                                                         int n_views,
                                                         const int32_t* __restrict__ coords,
@@ -332,8 +332,16 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
     const float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
     const float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
     bool loaded = false;
-    for (int vi = 0; vi < n_views; vi++) {
-        if (!mask[(long long)vi * g.bricks + brick]) continue;
+    /* the brick's visibility in 32 views at a time: 32 independent mask loads, then only the
+     * views that see the brick, in view order */
+    for (int w0 = 0; w0 < n_views; w0 += 32) {
+      uint32_t seen = 0u;
+#pragma unroll
+      for (int k = 0; k < 32; k++)
+          if (w0 + k < n_views && mask[(long long)(w0 + k) * g.bricks + brick]) seen |= 1u << k;
+      while (seen) {
+        const int vi = w0 + __ffs(seen) - 1;
+        seen &= seen - 1u;
         const L3dTsdfView& v = views[vi];
         const uint32_t* depth = depths[vi];
         const float* prior = v.has_prior ? priors + v.prior_off : nullptr;
@@ -361,6 +369,7 @@ __global__ void __launch_bounds__(256) k_integrate_many(const L3dTsdfGrid g,
             if (Q8) apply_q8(t[j], wq[j], obs, w, g.max_q);
             else apply_f32(t[j], wf[j], obs, w, g.max_weight);
         }
+      }
     }
     if (!loaded) return;
     if (VEC == 4) {
