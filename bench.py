@@ -413,6 +413,21 @@ def run_fusion(args):
         "coarse_to_fine_6_4": {"ms": ms_c2f, "px_iters_per_s": px_c2f / (ms_c2f / 1e3),
                                "depth_accuracy": acc(fine)},
     }
+    # the geometric-consistency pass (1 iteration, as the Medium profile) on the coarse-to-fine
+    # maps: the photometric cost plus 0.2 x the forward-backward reprojection error per source
+    og = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=1, geometric=True)
+          for r in refs]
+    fine.solve_all(refs, og)  # warm-up: the maps it reads are the previous pass's
+    c2f()
+    with torch.cuda.stream(stream):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fine.solve_all(refs, og)
+        b.record(stream)
+        b.synchronize()
+    ms_geo = a.elapsed_time(b)
+    stereo["geometric_1_after_coarse_to_fine"] = {
+        "ms": ms_geo, "px_iters_per_s": V * W * H / (ms_geo / 1e3), "depth_accuracy": acc(fine)}
 
     # dense cloud: filter + addDepthMap per view (fuseDepthMaps), on the single-scale maps
     fviews = [FusionView(w.views[r], w.sources[r], w.needed[r], thumbs_host[r]) for r in refs]
