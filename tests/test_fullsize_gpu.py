@@ -1,0 +1,117 @@
+"""Properties at the benchmark's full size: the scan workload (48 views of 640x480, 8 sources,
+5 iterations, TSDF 512^3 at 4 mm).
+
+The oracle cannot solve this size in test time, so these check relations that hold at any size:
+the fast form's depth accuracy against the rendered ground truth equals the plain form's, a
+batched solve equals its views solved one by one, the batched consistency filter equals the
+per-view filter, and the many-view TSDF sweep (with and without the overlapped read-back)
+equals the per-view integrations bit for bit.
+"""
+import numpy as np
+import pytest
+
+from helpers import assert_bit_equal
+from luvas3d import (DTYPE_F16, DTYPE_F32, FORM_FAST, FORM_PLAIN, DenseStereo, IntegrationView,
+                     SolveOptions, StereoOptions, TsdfVolume, scenes)
+from luvas3d.packing import unpack_depth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def scan():
+    w = scenes.scan()
+    refs = list(range(len(w.views)))
+    opts = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=w.iterations)
+            for r in refs]
+    return w, refs, opts
+
+
+def solved(w, refs, opts, form, storage):
+    s = DenseStereo(w.width, w.height, w.views, StereoOptions(storage=storage, form=form))
+    for i, im in enumerate(w.images):
+        s.set_image(i, im)
+    s.solve_all(refs, opts)
+    return s
+
+
+def accuracy(s, w, refs):
+    errs, surf, valid = [], 0, 0
+    for r in refs:
+        packed = s.depth_map(r)
+        t = w.truth[r]
+        m = t > 0
+        ok = m & (packed != 0)
+        surf += int(m.sum())
+        valid += int(ok.sum())
+        errs.append(np.abs(unpack_depth(packed[ok]) - t[ok]) / t[ok])
+    e = np.concatenate(errs)
+    return valid / surf, float(np.median(e)), float(np.mean(e < 0.01))
+
+
+@pytest.fixture(scope="module")
+def fast(scan):
+    w, refs, opts = scan
+    s = solved(w, refs, opts, FORM_FAST, DTYPE_F16)
+    yield s
+    s.destroy()
+
+
+def test_fast_form_keeps_the_plain_forms_accuracy(scan, fast):
+    w, refs, opts = scan
+    plain = solved(w, refs, opts, FORM_PLAIN, DTYPE_F32)
+    vp, mp, fp = accuracy(plain, w, refs)
+    vf, mf, ff = accuracy(fast, w, refs)
+    plain.destroy()
+    print(f"plain: valid {vp:.4f} median {mp:.5f} within1% {fp:.4f}; "
+          f"fast: valid {vf:.4f} median {mf:.5f} within1% {ff:.4f}")
+    assert abs(vf - vp) < 0.005
+    assert mf < mp * 1.05 and ff > fp - 0.01
+    assert mp < 0.006          # the scene is solvable: median error under 0.6 %
+
+
+def test_batch_equals_views_one_by_one(scan, fast):
+    w, refs, opts = scan
+    one = DenseStereo(w.width, w.height, w.views, StereoOptions(storage=DTYPE_F16, form=FORM_FAST))
+    for i, im in enumerate(w.images):
+        one.set_image(i, im)
+    for r in (0, 17, 47):
+        one.solve_all([r], [opts[r]])
+        assert_bit_equal(one.read_hypotheses_layer(r)[0], fast.read_hypotheses_layer(r)[0],
+                         f"view {r} hypotheses")
+    one.destroy()
+
+
+def test_filter_all_equals_per_view_filter(scan, fast):
+    w, refs, opts = scan
+    fast.filter_all(refs, w.sources, w.needed)
+    for r in (0, 23, 47):
+        got = fast.read_filtered_layer(r)
+        fast.filter(r, w.sources[r], w.needed[r])
+        assert_bit_equal(got, fast.read_filtered(), f"view {r} filtered map")
+        assert (got != 0).mean() > 0.5
+
+
+def test_tsdf_sweep_equals_per_view_integration(scan, fast):
+    w, refs, opts = scan
+    fast.filter_all(refs, w.sources, w.needed)
+    views = [IntegrationView(v.intrinsics, v.pose, w.ranges[i][1]) for i, v in enumerate(w.views)]
+
+    def volume():
+        return TsdfVolume(w.width, w.height, w.tsdf_voxel, w.tsdf_origin, dense=w.tsdf_dims,
+                          truncation=w.tsdf_truncation, weight_q8=True)
+
+    a, b, c = volume(), volume(), volume()
+    for i, r in enumerate(refs):
+        a.integrate(views[i], depth=fast.read_filtered_layer(r))
+    b.integrate_many(views, stereo=fast, layers=refs)
+    ta, wa = a.read()
+    tb, wb = b.read()
+    assert_bit_equal(tb, ta, "tsdf")
+    assert_bit_equal(wb, wa, "weight")
+    tc, wc = c.integrate_many_read(views, stereo=fast, layers=refs)
+    assert_bit_equal(tc, ta, "tsdf (read-back overlapped)")
+    assert_bit_equal(wc, wa, "weight (read-back overlapped)")
+    assert (wa > 0).mean() > 0.05
+    for v in (a, b, c):
+        v.destroy()
