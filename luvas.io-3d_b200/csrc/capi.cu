@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -2566,27 +2567,6 @@ HostCover host_coverage(int source, int target) {
     return c;
 }
 
-/* Stream-ordered device copy of a host cover table; freed with cudaFreeAsync on the stream. */
-int upload_cover(const HostCover& h, cudaStream_t s, L3dAreaCover* d, std::vector<void*>& owned) {
-    int *first, *count;
-    double* weights;
-    L3D_CUDA(pool_alloc((void**)&first, h.first.size() * 4, s), "cover table");
-    owned.push_back(first);
-    L3D_CUDA(pool_alloc((void**)&count, h.count.size() * 4, s), "cover table");
-    owned.push_back(count);
-    L3D_CUDA(pool_alloc((void**)&weights, h.weights.size() * 8, s), "cover table");
-    owned.push_back(weights);
-    L3D_CUDA(cudaMemcpyAsync(first, h.first.data(), h.first.size() * 4, cudaMemcpyHostToDevice, s), "cover upload");
-    L3D_CUDA(cudaMemcpyAsync(count, h.count.data(), h.count.size() * 4, cudaMemcpyHostToDevice, s), "cover upload");
-    L3D_CUDA(cudaMemcpyAsync(weights, h.weights.data(), h.weights.size() * 8, cudaMemcpyHostToDevice, s),
-             "cover upload");
-    d->first = first;
-    d->count = count;
-    d->weights = weights;
-    d->kmax = h.kmax;
-    return L3D_OK;
-}
-
 int check_sizes(int w, int h, int tw, int th) {
     if (w <= 0 || h <= 0 || tw <= 0 || th <= 0) return fail(L3D_EINVAL, "sizes must be positive");
     if ((long long)w * h >= (1ll << 31) || (long long)tw * th >= (1ll << 31))
@@ -2594,25 +2574,97 @@ int check_sizes(int w, int h, int tw, int th) {
     return L3D_OK;
 }
 
-/* resampleArea (gray-image.ts:193-221) of a device source (u8 or f32). */
-int area_resample(const void* src, int is_float, int w, int h, int tw, int th, uint8_t* out,
+/* Coverage tables of both axes on the device, packed in one block: first/count ints of the
+ * columns then the rows, then the columns' and the rows' weights (8-byte aligned). */
+struct DeviceCover {
+    unsigned char* block = nullptr;
+    L3dAreaCover cols{}, rows{};
+};
+
+/* `s` != NULL: a stream-ordered block from the pool for one call (freed by the caller on `s`);
+ * else a plain allocation kept by the cache. */
+int make_device_cover(int w, int h, int tw, int th, cudaStream_t s, bool pooled, DeviceCover* out) {
+    const HostCover hc = host_coverage(w, tw), hr = host_coverage(h, th);
+    const size_t off_w = (((size_t)2 * tw + (size_t)2 * th) * 4 + 7) & ~(size_t)7;
+    std::vector<unsigned char> host(off_w + (hc.weights.size() + hr.weights.size()) * 8);
+    int* hi = (int*)host.data();
+    std::memcpy(hi, hc.first.data(), (size_t)tw * 4);
+    std::memcpy(hi + tw, hc.count.data(), (size_t)tw * 4);
+    std::memcpy(hi + 2 * tw, hr.first.data(), (size_t)th * 4);
+    std::memcpy(hi + 2 * tw + th, hr.count.data(), (size_t)th * 4);
+    double* hw = (double*)(host.data() + off_w);
+    std::memcpy(hw, hc.weights.data(), hc.weights.size() * 8);
+    std::memcpy(hw + hc.weights.size(), hr.weights.data(), hr.weights.size() * 8);
+    unsigned char* block;
+    cudaError_t e;
+    if (pooled) {
+        L3D_CUDA(pool_alloc((void**)&block, host.size(), s), "area filter tables");
+        if ((e = cudaMemcpyAsync(block, host.data(), host.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+            cudaFreeAsync(block, s);
+            return cuda_fail(e, "area filter tables");
+        }
+    } else {
+        L3D_CUDA(cudaMalloc((void**)&block, host.size()), "area filter tables");
+        if ((e = cudaMemcpy(block, host.data(), host.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
+            cudaFree(block);
+            return cuda_fail(e, "area filter tables");
+        }
+    }
+    const int* di = (const int*)block;
+    const double* dw = (const double*)(block + off_w);
+    out->block = block;
+    out->cols = L3dAreaCover{di, di + tw, dw, hc.kmax};
+    out->rows = L3dAreaCover{di + 2 * tw, di + 2 * tw + th, dw + hc.weights.size(), hr.kmax};
+    return L3D_OK;
+}
+
+/* The tables of the first few (device, source size, target size) combinations stay on their
+ * device for later calls (an app resamples every frame of a capture to the same size); other
+ * combinations get tables for one call (*temporary set: free the block on `s` after use). */
+constexpr size_t kCoverCacheEntries = 32;
+
+int device_cover(int w, int h, int tw, int th, cudaStream_t s, DeviceCover* out, bool* temporary) {
+    *temporary = false;
+    static std::mutex mu;
+    static std::vector<std::pair<std::array<int, 5>, DeviceCover>> cache;
+    int dev = 0;
+    L3D_CUDA(cudaGetDevice(&dev), "device query");
+    const std::array<int, 5> key{dev, w, h, tw, th};
+    std::lock_guard<std::mutex> lock(mu);
+    for (const auto& e : cache)
+        if (e.first == key) {
+            *out = e.second;
+            return L3D_OK;
+        }
+    if (cache.size() >= kCoverCacheEntries) {
+        *temporary = true;
+        return make_device_cover(w, h, tw, th, s, true, out);
+    }
+    DeviceCover c;
+    int rc = make_device_cover(w, h, tw, th, s, false, &c);
+    if (rc) return rc;
+    cache.emplace_back(key, c);
+    *out = c;
+    return L3D_OK;
+}
+
+/* resampleArea (gray-image.ts:193-221) of a device source (src_kind as l3d_launch_area), with
+ * the coverage tables from the cache and the row-pass buffer from the pool. */
+int area_resample(const void* src, int src_kind, int w, int h, int tw, int th, uint8_t* out,
                   cudaStream_t s) {
-    std::vector<void*> owned;
-    auto release = [&](int rc) {
-        for (void* p : owned) cudaFreeAsync(p, s);
-        return rc;
-    };
-    L3dAreaCover cols, rows;
-    int rc = upload_cover(host_coverage(w, tw), s, &cols, owned);
-    if (!rc) rc = upload_cover(host_coverage(h, th), s, &rows, owned);
-    if (rc) return release(rc);
+    DeviceCover c;
+    bool temporary = false;
+    int rc = device_cover(w, h, tw, th, s, &c, &temporary);
+    if (rc) return rc;
     float* temp;
     cudaError_t e = pool_alloc((void**)&temp, (size_t)tw * h * 4, s);
-    if (e != cudaSuccess) return release(cuda_fail(e, "area filter buffer"));
-    owned.push_back(temp);
-    e = l3d_launch_area(src, is_float, w, h, tw, th, cols, rows, temp, out, s);
-    if (e != cudaSuccess) return release(cuda_fail(e, "area filter launch"));
-    return release(L3D_OK);
+    if (e == cudaSuccess) {
+        e = l3d_launch_area(src, src_kind, w, h, tw, th, c.cols, c.rows, temp, out, s);
+        cudaFreeAsync(temp, s);
+    }
+    if (temporary) cudaFreeAsync(c.block, s);
+    if (e != cudaSuccess) return cuda_fail(e, "area filter launch");
+    return L3D_OK;
 }
 
 }  // namespace
@@ -2629,16 +2681,8 @@ int l3d_image_rgba_to_gray(const uint8_t* rgba, int32_t width, int32_t height, i
         L3D_CUDA(l3d_launch_gray_blocks(rgba, width, height, target_width, target_height, gray, s), "gray launch");
         return L3D_OK;
     }
-    float* luma;
-    L3D_CUDA(pool_alloc((void**)&luma, (size_t)width * height * 4, s), "luma buffer");
-    cudaError_t e = l3d_launch_luma(rgba, (long long)width * height, luma, s);
-    if (e != cudaSuccess) {
-        cudaFreeAsync(luma, s);
-        return cuda_fail(e, "luma launch");
-    }
-    rc = area_resample(luma, 1, width, height, target_width, target_height, gray, s);
-    cudaFreeAsync(luma, s);
-    return rc;
+    /* the area filter reads the RGBA pixels and forms their f32 luma itself */
+    return area_resample(rgba, 2, width, height, target_width, target_height, gray, s);
 }
 
 int l3d_image_downsample_rgb(const uint8_t* rgba, int32_t width, int32_t height, int32_t target_width,

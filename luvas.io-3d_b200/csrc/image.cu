@@ -54,28 +54,30 @@ __global__ void k_gray_blocks(const uint8_t* __restrict__ rgba, int W, int H, in
     out[i] = to_u8(js_round(sum / (256.0 * (y1 - y0) * (x1 - x0))));
 }
 
-/* rgbaToGray's f32 luma for the area filter (gray-image.ts:20-23) */
-__global__ void k_luma(const uint8_t* __restrict__ rgba, long long n, float* __restrict__ luma) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint8_t* p = rgba + i * 4;
-    luma[i] = (float)((double)(77 * p[0] + 150 * p[1] + 29 * p[2]) / 256.0);
+/* source pixel as the area filter reads it: u8 gray, f32, or the f32 luma of an RGBA pixel
+ * (rgbaToGray's Float32Array store, gray-image.ts:20-23) computed on the fly */
+template <int KIND>
+__device__ __forceinline__ double area_src(const void* __restrict__ src, long long i) {
+    if (KIND == 0) return (double)((const uint8_t*)src)[i];
+    if (KIND == 1) return (double)((const float*)src)[i];
+    const uint8_t* p = (const uint8_t*)src + i * 4;
+    return (double)(float)((double)(77 * p[0] + 150 * p[1] + 29 * p[2]) / 256.0);
 }
 
 /* resampleArea pass 1 (gray-image.ts:203-212): rows of the source -> f32 temp (tw per row).
  * cover: per target column, first source pixel and `k` weights (stride `kmax`). */
-template <typename T>
-__global__ void k_area_rows(const T* __restrict__ src, int W, int H, int tw,
+template <int KIND>
+__global__ void k_area_rows(const void* __restrict__ src, int W, int H, int tw,
                             const int* __restrict__ first, const int* __restrict__ count,
                             const double* __restrict__ weights, int kmax, float* __restrict__ temp) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long long)tw * H) return;
     const int x = (int)(i % tw);
     const long long y = i / tw;
-    const T* row = src + y * W + first[x];
+    const long long row = y * W + first[x];
     const double* w = weights + (size_t)x * kmax;
     double sum = 0.0;
-    for (int k = 0; k < count[x]; k++) sum += w[k] * (double)row[k];
+    for (int k = 0; k < count[x]; k++) sum += w[k] * area_src<KIND>(src, row + k);
     temp[i] = (float)sum;
 }
 
@@ -166,20 +168,19 @@ cudaError_t l3d_launch_gray_blocks(const uint8_t* rgba, int W, int H, int tw, in
     k_gray_blocks<<<blocks_for((long long)tw * th), 256, 0, s>>>(rgba, W, H, tw, th, out);
     return cudaGetLastError();
 }
-cudaError_t l3d_launch_luma(const uint8_t* rgba, long long n, float* luma, cudaStream_t s) {
-    k_luma<<<blocks_for(n), 256, 0, s>>>(rgba, n, luma);
-    return cudaGetLastError();
-}
-cudaError_t l3d_launch_area(const void* src, int src_is_float, int W, int H, int tw, int th,
+cudaError_t l3d_launch_area(const void* src, int src_kind, int W, int H, int tw, int th,
                             const L3dAreaCover& cols, const L3dAreaCover& rows, float* temp,
                             uint8_t* out, cudaStream_t s) {
     const long long n1 = (long long)tw * H;
-    if (src_is_float)
-        k_area_rows<float><<<blocks_for(n1), 256, 0, s>>>((const float*)src, W, H, tw, cols.first,
-                                                          cols.count, cols.weights, cols.kmax, temp);
+    if (src_kind == 2)
+        k_area_rows<2><<<blocks_for(n1), 256, 0, s>>>(src, W, H, tw, cols.first, cols.count,
+                                                      cols.weights, cols.kmax, temp);
+    else if (src_kind == 1)
+        k_area_rows<1><<<blocks_for(n1), 256, 0, s>>>(src, W, H, tw, cols.first, cols.count,
+                                                      cols.weights, cols.kmax, temp);
     else
-        k_area_rows<uint8_t><<<blocks_for(n1), 256, 0, s>>>((const uint8_t*)src, W, H, tw, cols.first,
-                                                            cols.count, cols.weights, cols.kmax, temp);
+        k_area_rows<0><<<blocks_for(n1), 256, 0, s>>>(src, W, H, tw, cols.first, cols.count,
+                                                      cols.weights, cols.kmax, temp);
     k_area_cols<<<blocks_for((long long)tw * th), 256, 0, s>>>(temp, tw, th, rows.first, rows.count,
                                                                rows.weights, rows.kmax, out);
     return cudaGetLastError();

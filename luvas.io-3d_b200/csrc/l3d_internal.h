@@ -368,8 +368,8 @@ struct L3dAreaCover {
 
 cudaError_t l3d_launch_gray_blocks(const uint8_t* rgba, int W, int H, int tw, int th, uint8_t* out,
                                    cudaStream_t s);
-cudaError_t l3d_launch_luma(const uint8_t* rgba, long long n, float* luma, cudaStream_t s);
-cudaError_t l3d_launch_area(const void* src, int src_is_float, int W, int H, int tw, int th,
+/* src_kind: 0 u8 gray, 1 f32, 2 RGBA (its f32 luma) */
+cudaError_t l3d_launch_area(const void* src, int src_kind, int W, int H, int tw, int th,
                             const L3dAreaCover& cols, const L3dAreaCover& rows, float* temp,
                             uint8_t* out, cudaStream_t s);
 cudaError_t l3d_launch_rgb_blocks(const uint8_t* rgba, int W, int H, int tw, int th, uint8_t* out,
