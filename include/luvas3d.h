@@ -240,8 +240,9 @@ int64_t l3d_stereo_launches(const l3d_stereo* s);
 int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant);
 int32_t l3d_stereo_variant(const l3d_stereo* s);
 
-/* Times every fast-form variant on one iteration of the given batch (it overwrites that batch's
- * hypotheses) and keeps the fastest; best_variant / best_ms (either may be NULL) report it.
+/* Times every fast-form variant on up to three iterations of the given batch (it overwrites
+ * that batch's hypotheses) and keeps the fastest; best_variant / best_ms (either may be NULL)
+ * report it.
  * No reference counterpart. */
 int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
                         const l3d_solve_opts* opts, int32_t* best_variant, float* best_ms);

@@ -1249,9 +1249,11 @@ int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
         return L3D_OK;  /* one sampler only */
     }
     const int candidates[] = {6, 14, 4, 12};
+    /* up to three iterations: the first propagates random planes, the later ones the converging
+     * planes whose neighbouring pixels agree, and the variants rank differently on the two */
     std::vector<l3d_solve_opts> one(opts, opts + n_refs);
     for (auto& q : one) {
-        q.iterations = 1;
+        q.iterations = std::max(1, std::min(q.iterations, 3));
         q.prior = nullptr;
         q.pack = 0;
     }
