@@ -312,6 +312,7 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_ncc_grad(
                     if (want_grad && raw > 0.0f && raw < 2.0f) {
                         const float inv_w = 1.0f / rsum, iden = 1.0f / den, ivs = 1.0f / vs;
                         const float ks0 = pr.ks[0], ks1 = pr.ks[1], ks2 = pr.ks[2], ks3 = pr.ks[3];
+                        const float iks0 = 1.0f / ks0, iks1 = 1.0f / ks1;
                         const float kt0 = pr.kt[0], kt1 = pr.kt[1], kt2 = pr.kt[2];
 #pragma unroll 4
                         for (int i = 0; i < S; i++) {
@@ -340,8 +341,8 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_ncc_grad(
                             const float e2 = lam * fmaf(ks2, g0, fmaf(ks3, g1, g2));
                             const float il = 1.0f / lam;
                             const float Y2 = qz * il;
-                            const float Y0 = (fmaf(-ks2, qz, qx) / ks0) * il;
-                            const float Y1 = (fmaf(-ks3, qz, qy) / ks1) * il;
+                            const float Y0 = (fmaf(-ks2, qz, qx) * iks0) * il;
+                            const float Y1 = (fmaf(-ks3, qz, qy) * iks1) * il;
                             S1x += e0;
                             S1y += e1;
                             S1z += e2;
