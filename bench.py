@@ -119,6 +119,29 @@ def workload_name(w) -> str:
             f"trunc {w.tsdf_truncation * 100:.0f} cm, Q8.8 weights")
 
 
+def scene_conventions(w) -> dict:
+    """Geometry, texture, camera and seed conventions of the synthetic scene (scene.cpp,
+    scenes.py), recorded with every bench line."""
+    if w.name == "room":
+        geometry = ("inside of the box x in [-2, 2], y in [-1.25, 1.25], z in [-1.5, 1.5] m with "
+                    "20 seeded axis-aligned cuboids")
+    else:
+        geometry = "unit sphere centred at the origin resting on the plane y = -1"
+    return {"geometry": geometry,
+            "texture": "3-octave value noise in [0, 1]: lattice frequencies 24, 57, 131 per m, "
+                       "amplitudes 0.5, 0.3, 0.2, smoothstep interpolation, PCG-hashed lattice",
+            "images": "2x2 supersampled, Gaussian pixel noise (sigma 0.01 on scan/room); "
+                      "depth = camera-z of the pixel-centre ray, 0 where the ray escapes",
+            "cameras": "x right, y down, z forward, x_cam = R X + t; look-at the origin with world "
+                       "up +y" + ("; one helix turn, radius 1.2 -> 2.0 m, elevation -10 -> 40 deg, "
+                                  "poses given to the solver perturbed by 2 mm / 0.1 deg"
+                                  if w.name == "scan" else ""),
+            "seeds": {"scene": {"scan": 2, "room": 4, "small": 1, "polish": 6}.get(w.name),
+                      "pose_noise": "scene seed + 1000" if w.name == "scan" else None,
+                      "patchmatch": "pcg(index ^ pcg(seed + 7919 iter + 104729 phase)), "
+                                    "seed = (ref + 1) 0x9e3779b1 + 97 iter + 13 phase + 7 flags"}}
+
+
 def cpu_baseline(w, threads: int, budget_s: float = 20.0) -> dict:
     """The FP32 oracle on the host cores: one reference view's init + 1 red/black iteration at
     full resolution with the workload's sources, and one TSDF view integration of the full
@@ -147,7 +170,15 @@ def cpu_baseline(w, threads: int, budget_s: float = 20.0) -> dict:
                       max_depth=w.ranges[0][1]), o.depths[0])
     t_tsdf = time.perf_counter() - t0
     vox = int(np.prod(w.tsdf_dims))
+    # one thread: one colour of the same iteration (half the pixels updated)
+    o1 = oracle.Stereo(w.width, w.height, w.views, w.images, 32, threads=1)
+    o1.kernel(oracle.INIT, 0, w.sources[0], min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
+    t0 = time.perf_counter()
+    o1.kernel(oracle.PROPAGATE, 0, w.sources[0], iteration=0, phase=0,
+              min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
+    t_one = time.perf_counter() - t0
     return {"value": pm, "unit": "px-iters/s", "cores": threads, "kind": "port",
+            "single_thread_px_iters_per_s": (w.images[0].size / 2) / t_one,
             "sample": (f"FP32 oracle: 1 reference view x 1 red/black iteration at "
                        f"{w0}x{h0}, {len(w.sources[0])} sources "
                        f"({t_prop:.2f} s); TSDF 1 view into {w.tsdf_dims[0]}^3 ({t_tsdf:.2f} s)"),
@@ -174,9 +205,11 @@ def run_reference(args, rank: int, world: int) -> None:
         "ms_per_step": 1e3 * w.pixels * w.iterations / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": workload_name(w), "sample": r["sample"]},
+        "scene": scene_conventions(w),
         "tsdf_voxel_updates_per_s": statistics.median(tv),
         "cpu_baseline": {"value": v, "unit": "px-iters/s", "cores": threads, "kind": "port",
-                         "sample": r["sample"]},
+                         "sample": r["sample"],
+                         "single_thread_px_iters_per_s": r["single_thread_px_iters_per_s"]},
         "e2e": {"value": v, "unit": "px-iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -795,7 +828,9 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": R["st_s"] * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": f"{args.storage} images, f32 arithmetic" if chosen_form == FORM_FAST else "f32",
-        "data": "synthetic (seeded sphere-on-plane scene, value-noise texture)",
+        "data": ("synthetic (seeded room scene with cuboids, value-noise texture)" if w.name == "room"
+                 else "synthetic (seeded sphere-on-plane scene, value-noise texture)"),
+        "scene": scene_conventions(w),
         "config": {"workload": workload_name(w),
                    "form": "fast" if chosen_form == FORM_FAST else "plain",
                    "variant": tuned.get("variant"),
@@ -816,7 +851,12 @@ def main():
         "roofline_tsdf": {"kernel": f"k_integrate_many ({V} views per sweep)", "bound": "hbm",
                           "achieved": tsdf_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                           "frac": tsdf_gbs / peaks.get("hbm_gbs", 6650.0),
-                          "peak_source": peak_kind, "bytes_per_launch": tsdf_bytes},
+                          "peak_source": peak_kind, "bytes_per_launch": tsdf_bytes,
+                          # the one-view-per-pass form streams 12 B per voxel-update; the sweep's
+                          # time against that form's bytes is its HBM-equivalent rate
+                          "per_view_form_bytes": vox * V * 12,
+                          "per_view_form_equivalent_frac":
+                              vox * V * 12 / (tsdf_ms / 1e3) / 1e9 / peaks.get("hbm_gbs", 6650.0)},
         "clocks": clk,
         "gpu_launches": R["launches"],
         "e2e": e2e,
