@@ -219,7 +219,15 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_ncc_grad(
     const float px = (float)x, py = (float)y;
 
     /* reference window: values and bilateral weights (prepare_window) */
-    float rv[S], rw[S];
+    /* the reference window in shared memory (lane-major) when it fits: the gradient pass
+     * indexes it in a loop that is not fully unrolled, which puts register arrays in local
+     * memory; the 11 x 11 window stays in (local) per-thread arrays */
+    constexpr bool kSharedWin = S <= 36;
+    constexpr int LS = kSharedWin ? kTileX * kTileY : 1;
+    __shared__ float rv_s[kSharedWin ? S : 1][kTileX * kTileY], rw_s[kSharedWin ? S : 1][kTileX * kTileY];
+    float rv_l[kSharedWin ? 1 : S], rw_l[kSharedWin ? 1 : S];
+    float* const rv = kSharedWin ? &rv_s[0][threadIdx.x] : rv_l;
+    float* const rw = kSharedWin ? &rw_s[0][threadIdx.x] : rw_l;
     float rsum = 1.0f, rmean = 0.0f, rvar = 0.0f;
     if (active) {
         const float center = texel<ST>(d.images, d.ref_img_off + idx);
@@ -232,8 +240,8 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_ncc_grad(
             const float dc = v - center;
             const float wgt = l3d_expf(-(dc * dc) / (2.0f * 0.06f * 0.06f) -
                                        (float)(ox * ox + oy * oy) / (2.0f * 5.0f * 5.0f));
-            rv[i] = v;
-            rw[i] = wgt;
+            rv[i * LS] = v;
+            rw[i * LS] = wgt;
             sw = sw + wgt;
             sr = fmaf(wgt, v, sr);
             srr = fmaf(wgt * v, v, srr);
@@ -293,10 +301,10 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_ncc_grad(
                 ok = ok && qz > 1e-6f && uu >= 0.0f && vv >= 0.0f && uu <= wmax && vv <= hmax;
                 float gx, gy;
                 const float val = ok ? bilinear_grad<ST>(img, pr.W, pr.H, uu, vv, &gx, &gy) : 0.0f;
-                ss = fmaf(rw[i], val, ss);
-                const float wv = rw[i] * val;
+                ss = fmaf(rw[i * LS], val, ss);
+                const float wv = rw[i * LS] * val;
                 sss = fmaf(wv, val, sss);
-                srs = fmaf(wv, rv[i], srs);
+                srs = fmaf(wv, rv[i * LS], srs);
             }
             if (ok) {
                 const float ms = ss / rsum;
@@ -325,8 +333,8 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_ncc_grad(
                             const float uu = qx * iz, vv = qy * iz;
                             float gx, gy;
                             const float val = bilinear_grad<ST>(img, pr.W, pr.H, uu, vv, &gx, &gy);
-                            const float dcs = -gout * (rw[i] * inv_w) *
-                                              ((rv[i] - rmean) * iden - ncc * (val - ms) * ivs);
+                            const float dcs = -gout * (rw[i * LS] * inv_w) *
+                                              ((rv[i * LS] - rmean) * iden - ncc * (val - ms) * ivs);
                             const float g0 = dcs * iz * gx, g1 = dcs * iz * gy;
                             const float g2 = -(g0 * uu + g1 * vv);
                             /* plane */
