@@ -86,3 +86,33 @@ def test_upsample_depth_ignores_empty_cells():
     # a constant grid stays constant; an empty grid stays empty
     np.testing.assert_array_equal(oracle.upsample_depth(np.full((3, 5), 2.5, np.float32), 17, 9), 2.5)
     np.testing.assert_array_equal(oracle.upsample_depth(np.zeros((3, 5), np.float32), 17, 9), 0.0)
+
+
+def _ramp_rgba(width=1280, height=8):
+    """The horizontal ramp of image.spec.ts:4-14: value round(20 + 0.15 x) in R, G and B."""
+    x = np.arange(width)
+    v = _js_round(20 + x * 0.15).astype(np.uint8)
+    rgba = np.zeros((height, width, 4), np.uint8)
+    rgba[..., :3] = v[None, :, None]
+    return rgba
+
+
+def ramp_worst_error(gray, width=1280, target=960):
+    """image.spec.ts:15-22: worst distance of row 2 from the ramp at the output pixel centres."""
+    scale = width / target
+    x = np.arange(2, target - 2)
+    expected = 20 + ((x + 0.5) * scale - 0.5) * 0.15
+    return float(np.abs(gray[2, x].astype(np.float64) - expected).max())
+
+
+def test_reference_ramp_keeps_pixel_centres_aligned():
+    """image.spec.ts:9-24: rgbaToGray 1280x8 -> 960x6 of a ramp is off by at most one level."""
+    gray = oracle.rgba_to_gray(_ramp_rgba(), 960, 6)
+    assert ramp_worst_error(gray) <= 1.0
+
+
+def test_reference_integer_ratio_blocks():
+    """image.spec.ts:26-30: downsampleGray of an 8x4 ramp to 4x2 averages exact blocks."""
+    data = ((np.arange(32) % 8) * 10).astype(np.uint8).reshape(4, 8)
+    half = oracle.downsample_gray(data, 4, 2)
+    assert half[0].tolist() == [5, 25, 45, 65]
