@@ -44,3 +44,13 @@ def test_upsample_depth():
     got = I.upsample_depth(torch.from_numpy(grid).cuda(), 640, 480).cpu().numpy()
     want = oracle.upsample_depth(grid, 640, 480)
     np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_reference_image_spec_cases():
+    """The two cases of image.spec.ts on the device: the 1280x8 ramp to 960x6 stays within one
+    level of the ramp at the pixel centres, and 2x2 blocks of an 8x4 ramp average exactly."""
+    from test_image_oracle import _ramp_rgba, ramp_worst_error
+    gray = I.rgba_to_gray(torch.from_numpy(_ramp_rgba()).cuda(), 960, 6).cpu().numpy()
+    assert ramp_worst_error(gray) <= 1.0
+    data = torch.from_numpy(((np.arange(32) % 8) * 10).astype(np.uint8).reshape(4, 8)).cuda()
+    assert I.downsample_gray(data, 4, 2).cpu().numpy()[0].tolist() == [5, 25, 45, 65]
