@@ -331,6 +331,14 @@ __global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
     for (int j = 0; j < VEC; j++) wx[j] = fmaf((float)(gx + j) + 0.5f, g.voxel, g.origin[0]);
     const float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
     const float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
+    /* the quad's volume values are loaded up front, so their latency overlaps the first view's
+     * projection; they are written back only when a view updated them */
+#pragma unroll
+    for (int k = 0; k < VEC; k++) {
+        t[k] = tsdf[idx + k];
+        if (Q8) wq[k] = ((const uint16_t*)weight)[idx + k];
+        else wf[k] = ((const float*)weight)[idx + k];
+    }
     bool loaded = false;
     /* the brick's visibility in 32 views at a time: 32 independent mask loads, then only the
      * views that see the brick, in view order */
@@ -357,15 +365,7 @@ __global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
         for (int j = 0; j < VEC; j++) {
             float obs, w;
             if (!in[j] || !lut_observe(g, v, prior, normals, cam[j], pix[j], packed[j], &obs, &w)) continue;
-            if (!loaded) {
-                loaded = true;
-#pragma unroll
-                for (int k = 0; k < VEC; k++) {
-                    t[k] = tsdf[idx + k];
-                    if (Q8) wq[k] = ((const uint16_t*)weight)[idx + k];
-                    else wf[k] = ((const float*)weight)[idx + k];
-                }
-            }
+            loaded = true;
             if (Q8) apply_q8(t[j], wq[j], obs, w, g.max_q);
             else apply_f32(t[j], wf[j], obs, w, g.max_weight);
         }
