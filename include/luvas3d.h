@@ -453,6 +453,22 @@ int l3d_tsdf_backward(l3d_tsdf* t, const l3d_integration_view* view, int32_t wid
  * frees its own buffers and stream; blocks until the probe is done. */
 int l3d_measure_texture_rate(int32_t dtype, int32_t checker, double* samples_per_second);
 
+/* ---- memory ---- */
+
+/* Scratch buffers, point tables and mesh outputs come from a stream-ordered memory pool of the
+ * library's own on each device, which keeps up to 16 GB of freed memory mapped for the next
+ * call.  l3d_memory_trim waits for the current device's queued work, then hands the pool's
+ * unused memory back to the driver until at most keep_bytes stay reserved (0 releases all of
+ * it); memory held by live handles stays.  It replaces what GPUBuffer.destroy() does for the
+ * reference at once (fusion/tsdf-volume.ts:279-290, mvs/dense-stereo.ts:357-369): a caller
+ * that shares the device with another allocator calls it after destroying handles. */
+int l3d_memory_trim(int64_t keep_bytes);
+
+/* The current device pool's reserved bytes (mapped: in use plus freed and kept) and the part
+ * in use by live allocations; both 0 before the pool's first allocation.  No counterpart in
+ * the reference. */
+int l3d_memory_reserved(int64_t* reserved, int64_t* used);
+
 /* Largest volume, in 8^3 bricks, that l3d_tsdf_integrate_noalloc accepts (a dense grid has
  * ceil(X/8) * ceil(Y/8) * ceil(Z/8) bricks; 2^20 covers 768^3). */
 #define L3D_NOALLOC_MAX_BRICKS (1 << 20)

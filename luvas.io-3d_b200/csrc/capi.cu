@@ -73,33 +73,41 @@ size_t dtype_size(int dtype) {
  * driver at every synchronisation and mapping it again costs milliseconds per GB. */
 #define L3D_POOL_KEEP_BYTES (16ull << 30)
 #define L3D_POOL_DEVICES 64
+std::mutex pool_mu;
+cudaMemPool_t pools[L3D_POOL_DEVICES] = {};
+
+/* The pool of device `dev`, created on first use when `create` is set (*out stays NULL
+ * otherwise). */
+cudaError_t device_pool(int dev, bool create, cudaMemPool_t* out) {
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(pool_mu);
+    if (!pools[dev] && create) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t created;
+        cudaError_t e = cudaMemPoolCreate(&created, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = L3D_POOL_KEEP_BYTES;
+        if ((e = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+            cudaMemPoolDestroy(created);
+            return e;
+        }
+        pools[dev] = created;
+    }
+    *out = pools[dev];
+    return cudaSuccess;
+}
+
 cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
-    static std::mutex mu;
-    static cudaMemPool_t pools[L3D_POOL_DEVICES] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= L3D_POOL_DEVICES) return cudaMallocAsync(p, bytes, s);
     cudaMemPool_t pool;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        if (!pools[dev]) {
-            cudaMemPoolProps props;
-            std::memset(&props, 0, sizeof(props));
-            props.allocType = cudaMemAllocationTypePinned;
-            props.location.type = cudaMemLocationTypeDevice;
-            props.location.id = dev;
-            cudaMemPool_t created;
-            if ((e = cudaMemPoolCreate(&created, &props)) != cudaSuccess) return e;
-            uint64_t keep = L3D_POOL_KEEP_BYTES;
-            if ((e = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
-                cudaMemPoolDestroy(created);
-                return e;
-            }
-            pools[dev] = created;
-        }
-        pool = pools[dev];
-    }
+    if ((e = device_pool(dev, true, &pool)) != cudaSuccess) return e;
     return cudaMallocFromPoolAsync(p, bytes, pool, s);
 }
 
@@ -2790,6 +2798,38 @@ int l3d_measure_texture_rate(int32_t dtype, int32_t checker, double* samples_per
         if (x) cudaEventDestroy(x);
     if (st) cudaStreamDestroy(st);
     if (e != cudaSuccess) return cuda_fail(e, what);
+    return L3D_OK;
+}
+
+int l3d_memory_trim(int64_t keep_bytes) {
+    if (keep_bytes < 0) return fail(L3D_EINVAL, "keep_bytes must not be negative");
+    int dev = 0;
+    L3D_CUDA(cudaGetDevice(&dev), "current device");
+    if (dev < 0 || dev >= L3D_POOL_DEVICES) return L3D_OK;
+    cudaMemPool_t pool;
+    L3D_CUDA(device_pool(dev, false, &pool), "memory pool");
+    if (!pool) return L3D_OK;
+    /* memory freed in stream order returns to the pool once its stream has passed the free */
+    L3D_CUDA(cudaDeviceSynchronize(), "synchronize");
+    L3D_CUDA(cudaMemPoolTrimTo(pool, (size_t)keep_bytes), "trim the memory pool");
+    return L3D_OK;
+}
+
+int l3d_memory_reserved(int64_t* reserved, int64_t* used) {
+    if (!reserved || !used) return fail(L3D_EINVAL, "reserved and used must not be NULL");
+    *reserved = 0;
+    *used = 0;
+    int dev = 0;
+    L3D_CUDA(cudaGetDevice(&dev), "current device");
+    if (dev < 0 || dev >= L3D_POOL_DEVICES) return L3D_OK;
+    cudaMemPool_t pool;
+    L3D_CUDA(device_pool(dev, false, &pool), "memory pool");
+    if (!pool) return L3D_OK;
+    uint64_t r = 0, u = 0;
+    L3D_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r), "pool reserved bytes");
+    L3D_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u), "pool used bytes");
+    *reserved = (int64_t)r;
+    *used = (int64_t)u;
     return L3D_OK;
 }
 

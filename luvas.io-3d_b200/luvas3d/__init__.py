@@ -7,6 +7,7 @@ kernels.
 from ._lib import (DTYPE_BF16, DTYPE_F16, DTYPE_F32, DTYPE_U8, FORM_FAST, FORM_PLAIN,
                    KERNEL_CONSISTENCY, KERNEL_INIT, KERNEL_INIT_COARSE, KERNEL_PACK,
                    KERNEL_PROPAGATE, L3dError, MAX_SOURCES, WEIGHT_F32, WEIGHT_Q8)
+from .memory import memory_reserved, trim_memory
 from .camera import Intrinsics, Pose, StereoView, look_at, relative_pose, scale_intrinsics
 from .stereo import (STEREO_METHODS, DenseStereo, SolveOptions, StereoInput, StereoOptions,
                      StereoRun, StereoSettings)
@@ -18,5 +19,5 @@ __all__ = [
     "StereoSettings", "StereoView", "TsdfVolume", "look_at", "relative_pose", "scale_intrinsics",
     "DTYPE_U8", "DTYPE_F32", "DTYPE_F16", "DTYPE_BF16", "FORM_PLAIN", "FORM_FAST", "WEIGHT_F32",
     "WEIGHT_Q8", "KERNEL_INIT", "KERNEL_INIT_COARSE", "KERNEL_PROPAGATE", "KERNEL_PACK",
-    "KERNEL_CONSISTENCY", "MAX_SOURCES",
+    "KERNEL_CONSISTENCY", "MAX_SOURCES", "memory_reserved", "trim_memory",
 ]

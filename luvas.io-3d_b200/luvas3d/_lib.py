@@ -190,6 +190,8 @@ SIGNATURES = [
     ("l3d_image_downsample_gray", C.c_int, [_P, _I, _I, _I, _I, _P, _P]),
     ("l3d_depth_upsample", C.c_int, [_P, _I, _I, _I, _I, _P, _P]),
     ("l3d_measure_texture_rate", C.c_int, [_I, _I, C.POINTER(C.c_double)]),
+    ("l3d_memory_trim", C.c_int, [C.c_int64]),
+    ("l3d_memory_reserved", C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("l3d_ncc_forward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P]),
     ("l3d_ncc_backward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P, _P, _P, _P]),
     ("l3d_tsdf_forward_depth", C.c_int, [_P, C.POINTER(IntegrationView), _I, _I, _P, _P, _P, _P, _P,

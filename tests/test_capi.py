@@ -91,6 +91,9 @@ def test_bad_arguments_are_rejected_with_a_message():
     assert lib.l3d_measure_texture_rate(_lib.DTYPE_BF16, 1, C.byref(rate)) == _lib.L3D_EINVAL
     assert "dtype" in _lib.last_error()
     assert lib.l3d_measure_texture_rate(_lib.DTYPE_F16, 1, None) == _lib.L3D_EINVAL
+    assert lib.l3d_memory_trim(-1) == _lib.L3D_EINVAL
+    assert "keep_bytes" in _lib.last_error()
+    assert lib.l3d_memory_reserved(None, None) == _lib.L3D_EINVAL
 
 
 def test_python_layer_raises_typed_errors():
