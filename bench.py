@@ -760,8 +760,18 @@ def main():
         samples = 14 * S * 36 * (w.pixels / V / 2) * views_per_launch
         got = samples / (R["prop_ms"] / 1e3) / 1e9
         peak_tex = rate.value / 1e9
+        # DRAM traffic of one launch: the ncu capture of the 8-view launch of this kernel (F16
+        # images, variant 14: 54.13 MB read + 1.90 MB written for 8 x 153 600 pixels of one
+        # colour) scaled by the pixels this launch processes; hyp, cost and images all grow
+        # with the views in the launch
+        traffic = None
+        if args.storage == "f16":
+            traffic = (54.13248e6 + 1.896704e6) / (8 * 153600) * (w.pixels / V / 2) * views_per_launch
         roof_tex = {"kernel": roof_fp32["kernel"], "bound": "texture", "achieved": got,
-                    "peak": peak_tex, "unit": "Gsample/s", "frac": got / peak_tex, "traffic": None,
+                    "peak": peak_tex, "unit": "Gsample/s", "frac": got / peak_tex, "traffic": traffic,
+                    "traffic_unit": "DRAM bytes per launch",
+                    "traffic_source": "profiles/k_fast_propagate_scan8.md (8-view capture, "
+                                      "scaled by the pixels per launch)" if traffic else None,
                     "peak_source": f"measured: l3d_measure_texture_rate({args.storage}, one "
                                    "red/black colour), bilinear samples/s of a 2048x2048 texture",
                     "launch_ms": R["prop_ms"], "samples_per_launch": samples,
