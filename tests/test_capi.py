@@ -100,3 +100,7 @@ def test_python_layer_raises_typed_errors():
     with pytest.raises(_lib.L3dError) as e:
         _lib.check(_lib.L3D_EINVAL)
     assert e.value.status == _lib.L3D_EINVAL
+    from luvas3d import trim_memory
+    with pytest.raises(_lib.L3dError, match="keep_bytes") as e:
+        trim_memory(-1)
+    assert e.value.status == _lib.L3D_EINVAL
