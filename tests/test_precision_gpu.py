@@ -1,5 +1,5 @@
 """Precision configuration: each form and storage type against the FP64 oracle on the small
-workload (tests/precision_report.py computes the report; BASELINE.md quotes it).
+workload (tests/precision_report.py prints the full table of these figures).
 
 Bounds: the plain FP32 form follows the FP64 oracle's search on >= 99 % of the kept pixels
 (depth within 1e-3 relative) and the costs of fixed planes to 5e-4 at p99; the fast form's
