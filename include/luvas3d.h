@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define L3D_ABI_VERSION 1
+#define L3D_ABI_VERSION 2
 
 /* Status codes. */
 #define L3D_OK 0
@@ -50,7 +50,13 @@ extern "C" {
 
 /* Kernel forms. */
 #define L3D_FORM_PLAIN 0 /* FP32, one reference view per launch, the oracle's operation order */
-#define L3D_FORM_FAST 1  /* FP16/BF16 image storage, batched views, compensated FP32 sums */
+#define L3D_FORM_FAST 1  /* mixed precision, batched views: FP16 (or U8, BF16, F32) image storage,
+                            hardware bilinear filtering, FP32 window sums of values shifted by the
+                            window centre (compensated when opts.compensated is set) */
+#define L3D_FORM_EXACT 2 /* batched views with the plain form's arithmetic: F32 storage, texture
+                            gathers with exact bilinear weights; equal to the plain form and the
+                            FP32 oracle bit for bit (to the oracle's compensated mode when
+                            opts.compensated is set) */
 
 /* TSDF weight storage. */
 #define L3D_WEIGHT_F32 0 /* f32 weights in [0, max_weight] (the reference's storage) */
@@ -93,6 +99,10 @@ typedef struct {
     int32_t window;           /* samples per window side: 6 (reference, offsets +-1,3,5) or 11 */
     int32_t dilation;         /* spacing of window samples: 2 (reference) or 1 */
     void* stream;             /* cudaStream_t to run on, or NULL to create one */
+    int32_t compensated;      /* fast and exact forms: 1 = compensated FP32 window sums for the
+                                 NCC means, variances and covariances (exact form: a Neumaier sum
+                                 of every term; fast form: FP32 sums of each 6-sample window row
+                                 added with Neumaier compensation); 0 = plain FP32 sums */
 } l3d_stereo_opts;
 
 /* SolveOptions (mvs/dense-stereo.ts:62-75). */
@@ -233,16 +243,19 @@ int l3d_stereo_synchronize(l3d_stereo* s);
 /* Device kernels launched by this handle since creation (for launch accounting). */
 int64_t l3d_stereo_launches(const l3d_stereo* s);
 
-/* Fast-form kernel variant (no reference counterpart; the reference has one WGSL kernel):
+/* Batched-form kernel variant (no reference counterpart; the reference has one WGSL kernel):
  * window rows sampled by the texture unit (6, 4, 3 or 2; the others use software bilinear
- * on the LSU path) + 8 for the 2x2 quad lane mapping.  All variants compute the same algorithm;
- * results differ only by the texture unit's 8-bit filter weights on the rows it samples. */
+ * on the LSU path) + 8 for the 2x2 quad lane mapping + 16 (fast form, 6 rows) for texture
+ * gathers weighted with exact FP32 bilinear weights instead of the hardware filter.  All
+ * variants compute the same algorithm; fast-form results differ only by the texture unit's 8-bit
+ * filter weights on the rows it filters.  The exact form and compensated sums take 6 or 14 (the
+ * exact form always gathers). */
 int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant);
 int32_t l3d_stereo_variant(const l3d_stereo* s);
 
-/* Times every fast-form variant on up to three iterations of the given batch (it overwrites
- * that batch's hypotheses) and keeps the fastest; best_variant / best_ms (either may be NULL)
- * report it.
+/* Times every variant of the handle's form on up to three iterations of the given batch (it
+ * overwrites that batch's hypotheses) and keeps the fastest; the gather bit (16) stays as set.
+ * best_variant / best_ms (either may be NULL) report it.
  * No reference counterpart. */
 int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
                         const l3d_solve_opts* opts, int32_t* best_variant, float* best_ms);
@@ -452,6 +465,19 @@ int l3d_tsdf_backward(l3d_tsdf* t, const l3d_integration_view* view, int32_t wid
  * that the fast propagate kernel, bound by the texture pipe, is quoted against.  Allocates and
  * frees its own buffers and stream; blocks until the probe is done. */
 int l3d_measure_texture_rate(int32_t dtype, int32_t checker, double* samples_per_second);
+
+/* Fetch modes of l3d_measure_fetch_rate. */
+#define L3D_FETCH_FILTERED 0 /* hardware bilinear filtering (the fast form) */
+#define L3D_FETCH_GATHER 1   /* one texture gather of the footprint + exact FP32 weights (the
+                                exact form) */
+#define L3D_FETCH_POINT 2    /* four point-sampled texture fetches + exact FP32 weights */
+#define L3D_FETCH_LOADS 3    /* four loads from linear F32 memory + exact FP32 weights (the plain
+                                form's path) */
+
+/* l3d_measure_texture_rate for one of the fetch modes above: bilinear samples per second
+ * (L3D_FETCH_LOADS needs dtype F32).  No reference counterpart: the measured rates the batched
+ * forms' propagate kernels are quoted against. */
+int l3d_measure_fetch_rate(int32_t dtype, int32_t checker, int32_t mode, double* samples_per_second);
 
 /* ---- memory ---- */
 

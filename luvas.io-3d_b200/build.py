@@ -9,6 +9,7 @@ the plain FP32 form reproducible bit for bit on the CPU.  The host compiler gets
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -53,9 +54,9 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
     sources = [os.path.join(CSRC, f) for f in CUDA_SOURCES if os.path.exists(os.path.join(CSRC, f))]
     target = os.path.join(LIB, "libluvas3d.so")
     if force or _stale(target, sources + headers):
-        objs = []
         build_dir = os.path.join(HERE, "_build")
         os.makedirs(build_dir, exist_ok=True)
+        cmds, objs = [], []
         for src in sources:
             obj = os.path.join(build_dir, os.path.basename(src) + ".o")
             cmd = [_nvcc(), *NVCC_FLAGS, "-c", src, "-o", obj]
@@ -63,8 +64,12 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
             objs.append(obj)
+        # one nvcc per translation unit, in parallel
+        with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+            for f in [ex.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+                f.result()
         cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", target, *objs,
                "-lcudart"]
         if verbose:

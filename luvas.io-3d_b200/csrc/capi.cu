@@ -344,6 +344,12 @@ int solve_one(l3d_stereo* s, int ref, const l3d_solve_opts* o, float4* hyp, floa
         ch = s->opts.coarse->H;
     }
     const bool coarse = o->from_coarse && s->opts.coarse;
+    if (coarse) {
+        /* the coarse level's planes are written on its own stream */
+        const l3d_stereo* c = s->opts.coarse;
+        L3D_CUDA(cudaEventRecord(c->done, c->stream), "event record");
+        L3D_CUDA(cudaStreamWaitEvent(s->stream, c->done, 0), "stream wait");
+    }
     L3dParams p = build_params(s, ref, o->sources, n, o->min_depth, o->max_depth, 0, 0, 1.0, flags,
                                0, cw, ch);
     int rc = launch(s, coarse ? L3D_K_INIT_COARSE : L3D_K_INIT, p, d);
@@ -369,6 +375,8 @@ int solve_one(l3d_stereo* s, int ref, const l3d_solve_opts* o, float4* hyp, floa
 /* ---- fast form ---- */
 
 bool fast_tex(const l3d_stereo* s) { return s->opts.storage != L3D_DTYPE_BF16; }
+/* fast or exact form: every reference view of a batch in one launch per kernel */
+bool batched(const l3d_stereo* s) { return s->opts.form != L3D_FORM_PLAIN; }
 
 int fast_capacity(l3d_stereo* s, int n) {
     if (s->fview_cap >= n) return L3D_OK;
@@ -454,14 +462,20 @@ L3dFastView fast_view(const l3d_stereo* s, int ref, const l3d_solve_opts* o, lon
         kt[0] = kv[0] * t[0] + kv[2] * t[2];
         kt[1] = kv[1] * t[1] + kv[3] * t[2];
         kt[2] = t[2];
-        for (int c = 0; c < 3; c++) {
-            f.Bt[0 * 3 + c] = (float)(B[0 * 3 + c] + 0.5 * B[2 * 3 + c]);
-            f.Bt[1 * 3 + c] = (float)(B[1 * 3 + c] + 0.5 * B[2 * 3 + c]);
-            f.Bt[2 * 3 + c] = (float)B[2 * 3 + c];
+        if (s->opts.form == L3D_FORM_EXACT) {
+            /* texel coordinates: the plain form's B and kt, rounded to f32 as it rounds them */
+            for (int i = 0; i < 9; i++) f.Bt[i] = ps.B[i];
+            for (int i = 0; i < 3; i++) f.ktt[i] = ps.kt[i];
+        } else {
+            for (int c = 0; c < 3; c++) {
+                f.Bt[0 * 3 + c] = (float)(B[0 * 3 + c] + 0.5 * B[2 * 3 + c]);
+                f.Bt[1 * 3 + c] = (float)(B[1 * 3 + c] + 0.5 * B[2 * 3 + c]);
+                f.Bt[2 * 3 + c] = (float)B[2 * 3 + c];
+            }
+            f.ktt[0] = (float)(kt[0] + 0.5 * kt[2]);
+            f.ktt[1] = (float)(kt[1] + 0.5 * kt[2]);
+            f.ktt[2] = (float)kt[2];
         }
-        f.ktt[0] = (float)(kt[0] + 0.5 * kt[2]);
-        f.ktt[1] = (float)(kt[1] + 0.5 * kt[2]);
-        f.ktt[2] = (float)kt[2];
         for (int i = 0; i < 4; i++) f.k[i] = ps.k[i];
         for (int i = 0; i < 9; i++) f.R[i] = ps.R[i];
         for (int i = 0; i < 3; i++) f.t[i] = ps.t[i];
@@ -515,6 +529,8 @@ int fast_batch(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
     d.prior = prior;
     d.depths = s->depths;
     d.coarse = nullptr;
+    d.exact = s->opts.form == L3D_FORM_EXACT ? 1 : 0;
+    d.comp = s->opts.compensated ? 1 : 0;
     *out = d;
     return L3D_OK;
 }
@@ -730,15 +746,22 @@ int l3d_stereo_create_sized(int32_t n_views, const l3d_view* views, const int32_
     else l3d_stereo_opts_default(&o);
     if (!((o.window == 6 && o.dilation == 2) || (o.window == 11 && o.dilation == 1)))
         return fail(L3D_EINVAL, "window %d / dilation %d not supported (6/2 or 11/1)", o.window, o.dilation);
-    if (o.form != L3D_FORM_PLAIN && o.form != L3D_FORM_FAST)
+    if (o.form != L3D_FORM_PLAIN && o.form != L3D_FORM_FAST && o.form != L3D_FORM_EXACT)
         return fail(L3D_EINVAL, "unknown form %d", o.form);
     if (o.form == L3D_FORM_PLAIN && o.storage != L3D_DTYPE_F32)
         return fail(L3D_EINVAL, "the plain form stores images as F32");
+    if (o.form == L3D_FORM_EXACT && o.storage != L3D_DTYPE_F32)
+        return fail(L3D_EINVAL, "the exact form stores images as F32");
+    if (o.compensated != 0 && o.compensated != 1)
+        return fail(L3D_EINVAL, "compensated must be 0 or 1");
+    if (o.compensated && o.form == L3D_FORM_PLAIN)
+        return fail(L3D_EINVAL, "compensated sums are a fast- and exact-form option (the plain form is "
+                                "the oracle's uncompensated order)");
     if (o.storage != L3D_DTYPE_F32 && o.storage != L3D_DTYPE_F16 && o.storage != L3D_DTYPE_BF16 &&
         o.storage != L3D_DTYPE_U8)
         return fail(L3D_EINVAL, "image storage must be U8, F32, F16 or BF16");
-    if (o.form == L3D_FORM_FAST && !(o.window == 6 && o.dilation == 2))
-        return fail(L3D_EINVAL, "the fast form uses the reference window (6 samples, dilation 2)");
+    if (o.form != L3D_FORM_PLAIN && !(o.window == 6 && o.dilation == 2))
+        return fail(L3D_EINVAL, "the fast and exact forms use the reference window (6 samples, dilation 2)");
     for (int i = 0; i < n_views; i++) {
         const l3d_intrinsics& k = views[i].intrinsics;
         if (!(k.fx != 0.0) || !(k.fy != 0.0) || !std::isfinite(k.fx) || !std::isfinite(k.fy))
@@ -788,16 +811,19 @@ int l3d_stereo_create_sized(int32_t n_views, const l3d_view* views, const int32_
     e = cudaEventCreateWithFlags(&s->staged, cudaEventDisableTiming);
     if (e != cudaSuccess) return cleanup(cuda_fail(e, "event creation"));
     size_t esize = dtype_size(o.storage);
-    if (o.form == L3D_FORM_FAST && o.storage != L3D_DTYPE_BF16) {
-        /* texture-sampled copies: block-linear CUDA arrays with hardware bilinear filtering,
-         * clamp-to-edge addressing and unnormalised coordinates (texel centres at +0.5) */
+    if (o.form != L3D_FORM_PLAIN && o.storage != L3D_DTYPE_BF16) {
+        /* texture-sampled copies: block-linear CUDA arrays with clamp-to-edge addressing and
+         * unnormalised coordinates (texel centres at +0.5); hardware bilinear filtering for
+         * the fast form, texture gathers (point filtering) for the exact form */
+        const bool gather = o.form == L3D_FORM_EXACT;
         cudaChannelFormatDesc ch = o.storage == L3D_DTYPE_F16  ? cudaCreateChannelDescHalf()
                                    : o.storage == L3D_DTYPE_U8 ? cudaCreateChannelDesc<unsigned char>()
                                                                : cudaCreateChannelDesc<float>();
         s->arrays.assign(n_views, nullptr);
         s->texs.assign(n_views, 0);
         for (int i = 0; i < n_views; i++) {
-            if ((e = cudaMallocArray(&s->arrays[i], &ch, s->Wv[i], s->Hv[i])) != cudaSuccess)
+            if ((e = cudaMallocArray(&s->arrays[i], &ch, s->Wv[i], s->Hv[i],
+                                     cudaArrayTextureGather)) != cudaSuccess)
                 return cleanup(cuda_fail(e, "image array allocation"));
             cudaResourceDesc res;
             std::memset(&res, 0, sizeof(res));
@@ -807,7 +833,7 @@ int l3d_stereo_create_sized(int32_t n_views, const l3d_view* views, const int32_
             std::memset(&td, 0, sizeof(td));
             td.addressMode[0] = cudaAddressModeClamp;
             td.addressMode[1] = cudaAddressModeClamp;
-            td.filterMode = cudaFilterModeLinear;
+            td.filterMode = gather ? cudaFilterModePoint : cudaFilterModeLinear;
             /* U8 texels read as value / 255 (the r8unorm format of the reference's textures) */
             td.readMode = o.storage == L3D_DTYPE_U8 ? cudaReadModeNormalizedFloat
                                                     : cudaReadModeElementType;
@@ -815,10 +841,12 @@ int l3d_stereo_create_sized(int32_t n_views, const l3d_view* views, const int32_
             if ((e = cudaCreateTextureObject(&s->texs[i], &res, &td, nullptr)) != cudaSuccess)
                 return cleanup(cuda_fail(e, "texture creation"));
         }
-        if ((e = dalloc(&s->pairs, (size_t)s->Ptot)) != cudaSuccess)
-            return cleanup(cuda_fail(e, "pair image allocation"));
-        if ((e = cudaMemsetAsync(s->pairs, 0, (size_t)s->Ptot * 4, s->stream)) != cudaSuccess)
-            return cleanup(cuda_fail(e, "device clear"));
+        if (!gather) {
+            if ((e = dalloc(&s->pairs, (size_t)s->Ptot)) != cudaSuccess)
+                return cleanup(cuda_fail(e, "pair image allocation"));
+            if ((e = cudaMemsetAsync(s->pairs, 0, (size_t)s->Ptot * 4, s->stream)) != cudaSuccess)
+                return cleanup(cuda_fail(e, "device clear"));
+        }
     }
     const size_t depth_len = s->n_maps > 1 ? (size_t)s->Ptot : (size_t)s->P;
     if ((e = cudaMalloc(&s->images, (size_t)s->Ptot * esize)) != cudaSuccess ||
@@ -888,7 +916,7 @@ int l3d_stereo_solve(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o) {
     int rc = check_solve(s, ref, o);
     if (rc) return rc;
     s->hyp_ref = ref;
-    if (s->opts.form == L3D_FORM_FAST) return fast_solve(s, 1, &ref, o, false);
+    if (batched(s)) return fast_solve(s, 1, &ref, o, false);
     return solve_one(s, ref, o, s->hyp, s->cost, s->prior);
 }
 
@@ -908,7 +936,7 @@ int l3d_stereo_solve_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
         L3D_CUDA(dalloc(&s->cost_all, (size_t)s->Ptot), "cost_all allocation");
         L3D_CUDA(dalloc(&s->prior_all, (size_t)s->Ptot), "prior_all allocation");
     }
-    if (s->opts.form == L3D_FORM_FAST) return fast_solve(s, n_refs, refs, opts, true);
+    if (batched(s)) return fast_solve(s, n_refs, refs, opts, true);
     for (int i = 0; i < n_refs; i++) {
         int r = refs[i];
         int rc = solve_one(s, r, &opts[i], s->hyp_all + s->offv[r], s->cost_all + s->offv[r],
@@ -930,8 +958,9 @@ int l3d_stereo_dispatch(l3d_stereo* s, int32_t kernel, int32_t ref, const l3d_so
     if (phase != 0 && phase != 1) return fail(L3D_EINVAL, "phase must be 0 or 1");
     s->hyp_ref = ref;
     int n = std::min(o->n_sources, L3D_MAX_SOURCES);
-    if (s->opts.form == L3D_FORM_FAST) {
-        if (kernel == L3D_KERNEL_INIT_COARSE) return fail(L3D_EINVAL, "the fast form has no init_coarse");
+    if (batched(s)) {
+        if (kernel == L3D_KERNEL_INIT_COARSE)
+            return fail(L3D_EINVAL, "the fast and exact forms start from the coarse level in init (from_coarse)");
         l3d_solve_opts one = *o;
         one.iterations = iteration + 1;
         one.pack = 1;
@@ -941,6 +970,11 @@ int l3d_stereo_dispatch(l3d_stereo* s, int32_t kernel, int32_t ref, const l3d_so
         return fast_launch(s, kernel == L3D_KERNEL_INIT ? L3D_K_INIT : L3D_K_PROPAGATE, fd, iteration, phase);
     }
     L3dStereoDev d = dev_of(s);
+    if (kernel == L3D_KERNEL_INIT_COARSE) {
+        const l3d_stereo* c = s->opts.coarse;
+        L3D_CUDA(cudaEventRecord(c->done, c->stream), "event record");
+        L3D_CUDA(cudaStreamWaitEvent(s->stream, c->done, 0), "stream wait");
+    }
     if (kernel == L3D_KERNEL_INIT && o->prior && !o->geometric) {
         rc = upload_prior(s, ref, o->prior, s->prior);
         if (rc) return rc;
@@ -1073,8 +1107,8 @@ int l3d_stereo_plane_cost(l3d_stereo* s, int32_t ref, const l3d_solve_opts* o, c
     }
     const size_t pn = (size_t)s->Wv[ref] * s->Hv[ref];
     L3D_CUDA(cudaMemcpyAsync(s->planes, planes, pn * 16, cudaMemcpyHostToDevice, s->stream), "planes upload");
-    if (s->opts.form == L3D_FORM_FAST) {
-        if (view_costs) return fail(L3D_EINVAL, "the fast form reports the combined cost only");
+    if (batched(s)) {
+        if (view_costs) return fail(L3D_EINVAL, "the fast and exact forms report the combined cost only");
         L3dFastDev fd;
         l3d_solve_opts one = *o;
         one.prior = nullptr;
@@ -1226,10 +1260,18 @@ int l3d_stereo_view_size(const l3d_stereo* s, int32_t layer, int32_t* width, int
 
 int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant) {
     if (!s) return fail(L3D_EINVAL, "NULL handle");
-    if (s->opts.form != L3D_FORM_FAST) return fail(L3D_ESTATE, "variants select fast-form kernels");
-    const int rows = variant & 7, rest = variant & ~15;
+    if (!batched(s)) return fail(L3D_ESTATE, "variants select fast- and exact-form kernels");
+    const int rows = variant & 7, rest = variant & ~31;
+    const bool gather = (variant & 16) != 0;
     if (rest || !(rows == 6 || rows == 4 || rows == 3 || rows == 2))
-        return fail(L3D_EINVAL, "variant %d: texture rows must be 6, 4, 3 or 2 (+8 for quads)", variant);
+        return fail(L3D_EINVAL, "variant %d: texture rows must be 6, 4, 3 or 2 (+8 for quads, +16 "
+                                "for gathers)", variant);
+    if (rows != 6 && (s->opts.form == L3D_FORM_EXACT || s->opts.compensated || gather))
+        return fail(L3D_EINVAL, "variant %d: the exact form, compensated sums and gathers sample all "
+                                "six rows through the texture unit", variant);
+    if (gather && (s->opts.form != L3D_FORM_FAST || s->opts.storage == L3D_DTYPE_BF16))
+        return fail(L3D_EINVAL, "variant %d: gathers with exact weights are a fast-form option for "
+                                "texture storage (U8, F16, F32); the exact form always gathers", variant);
     s->variant = variant;
     return L3D_OK;
 }
@@ -1238,7 +1280,7 @@ int32_t l3d_stereo_variant(const l3d_stereo* s) { return s ? s->variant : -1; }
 
 int l3d_stereo_set_graphs(l3d_stereo* s, int32_t enable) {
     if (!s) return fail(L3D_EINVAL, "NULL handle");
-    if (s->opts.form != L3D_FORM_FAST) return fail(L3D_ESTATE, "graph replay is a fast-form feature");
+    if (!batched(s)) return fail(L3D_ESTATE, "graph replay is a fast- and exact-form feature");
     s->graphs = enable != 0;
     if (!s->graphs) {
         cudaStreamSynchronize(s->stream);
@@ -1251,12 +1293,14 @@ int l3d_stereo_set_graphs(l3d_stereo* s, int32_t enable) {
 int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
                         const l3d_solve_opts* opts, int32_t* best_variant, float* best_ms) {
     if (!s) return fail(L3D_EINVAL, "NULL handle");
-    if (s->opts.form != L3D_FORM_FAST) return fail(L3D_ESTATE, "the autotuner picks fast-form variants");
+    if (!batched(s)) return fail(L3D_ESTATE, "the autotuner picks fast- and exact-form variants");
     if (s->opts.storage == L3D_DTYPE_BF16) {
         if (best_variant) *best_variant = s->variant;
         return L3D_OK;  /* one sampler only */
     }
-    const int candidates[] = {6, 14, 4, 12};
+    const bool six_only = s->opts.form == L3D_FORM_EXACT || s->opts.compensated || !s->pairs ||
+                          (s->variant & 16);
+    const std::vector<int> candidates = six_only ? std::vector<int>{6, 14} : std::vector<int>{6, 14, 4, 12};
     /* up to three iterations: the first propagates random planes, the later ones the converging
      * planes whose neighbouring pixels agree, and the variants rank differently on the two */
     std::vector<l3d_solve_opts> one(opts, opts + n_refs);
@@ -1270,10 +1314,13 @@ int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
     L3D_CUDA(cudaEventCreate(&b), "event");
     const bool graphs = s->graphs;
     s->graphs = false;
+    /* gathers change the weights, so they are the caller's accuracy choice, kept as set */
+    const int keep = s->variant & 16;
     int best = s->variant;
     float best_t = 3.0e38f;
     int rc = L3D_OK;
-    for (int v : candidates) {
+    for (int c : candidates) {
+        const int v = c | keep;
         s->variant = v;
         for (int rep = 0; rep < 2 && rc == L3D_OK; rep++) {  /* the first run warms the caches */
             cudaEventRecord(a, s->stream);
@@ -2732,9 +2779,17 @@ int l3d_depth_upsample(const float* grid, int32_t grid_width, int32_t grid_heigh
 /* ------------------------------------------------------------------ texture-rate probe ----- */
 
 int l3d_measure_texture_rate(int32_t dtype, int32_t checker, double* samples_per_second) {
+    return l3d_measure_fetch_rate(dtype, checker, L3D_FETCH_FILTERED, samples_per_second);
+}
+
+int l3d_measure_fetch_rate(int32_t dtype, int32_t checker, int32_t mode, double* samples_per_second) {
     if (!samples_per_second) return fail(L3D_EINVAL, "NULL output");
     if (dtype != L3D_DTYPE_U8 && dtype != L3D_DTYPE_F16 && dtype != L3D_DTYPE_F32)
         return fail(L3D_EINVAL, "texture-rate probe: dtype must be u8, f16 or f32");
+    if (mode < L3D_FETCH_FILTERED || mode > L3D_FETCH_LOADS)
+        return fail(L3D_EINVAL, "texture-rate probe: unknown fetch mode %d", mode);
+    if (mode == L3D_FETCH_LOADS && dtype != L3D_DTYPE_F32)
+        return fail(L3D_EINVAL, "texture-rate probe: loads from linear memory read F32 images");
     *samples_per_second = 0.0;
     const int W = 2048, H = 2048, reps = 32, launches = 3;
     const long long blocks = l3d_texture_rate_blocks(W, H, checker ? 1 : 0);
@@ -2759,7 +2814,8 @@ int l3d_measure_texture_rate(int32_t dtype, int32_t checker, double* samples_per
     };
     if (step(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream creation") &&
         step(cudaEventCreate(&ev[0]), "event creation") && step(cudaEventCreate(&ev[1]), "event creation") &&
-        step(cudaMallocArray(&arr, &ch, W, H), "array allocation") &&
+        step(cudaMallocArray(&arr, &ch, W, H, mode == L3D_FETCH_GATHER ? cudaArrayTextureGather : 0),
+             "array allocation") &&
         step(cudaMalloc(&fill, (size_t)W * H * es), "fill allocation") &&
         step(cudaMalloc((void**)&out, (size_t)blocks * 128 * sizeof(float)), "output allocation") &&
         step(cudaMemsetAsync(fill, 0x3c, (size_t)W * H * es, st), "fill") &&
@@ -2773,14 +2829,16 @@ int l3d_measure_texture_rate(int32_t dtype, int32_t checker, double* samples_per
         std::memset(&td, 0, sizeof(td));
         td.addressMode[0] = cudaAddressModeClamp;
         td.addressMode[1] = cudaAddressModeClamp;
-        td.filterMode = cudaFilterModeLinear;
+        td.filterMode = mode == L3D_FETCH_FILTERED ? cudaFilterModeLinear : cudaFilterModePoint;
         td.readMode = dtype == L3D_DTYPE_U8 ? cudaReadModeNormalizedFloat : cudaReadModeElementType;
         td.normalizedCoords = 0;
+        const float* img = (const float*)fill;
         if (step(cudaCreateTextureObject(&tex, &res, &td, nullptr), "texture creation") &&
-            step(l3d_launch_texture_rate(tex, W, H, checker ? 1 : 0, reps, out, st), "probe launch") &&
+            step(l3d_launch_texture_rate(tex, img, W, H, checker ? 1 : 0, mode, reps, out, st), "probe launch") &&
             step(cudaEventRecord(ev[0], st), "event record")) {
             for (int i = 0; i < launches; i++)
-                if (!step(l3d_launch_texture_rate(tex, W, H, checker ? 1 : 0, reps, out, st), "probe launch"))
+                if (!step(l3d_launch_texture_rate(tex, img, W, H, checker ? 1 : 0, mode, reps, out, st),
+                          "probe launch"))
                     break;
             float ms = 0.0f;
             if (step(cudaEventRecord(ev[1], st), "event record") &&

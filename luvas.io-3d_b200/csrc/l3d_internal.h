@@ -94,9 +94,10 @@ cudaError_t l3d_launch_plain(int kernel, const L3dParams& p, const L3dStereoDev&
 
 /* ---- fast form: every reference view of a batch in one launch per kernel ---- */
 
-/* One source of one reference view.  Bt/ktt are the homography base and K_s t with the
- * texture's half-texel offset folded in (rows 0 and 1 plus 0.5 x row 2), so q.xy / q.z is
- * directly the filtering coordinate. */
+/* One source of one reference view.  Fast evaluator: Bt/ktt are the homography base and K_s t
+ * with the texture's half-texel offset folded in (rows 0 and 1 plus 0.5 x row 2), so q.xy / q.z
+ * is directly the filtering coordinate.  Exact evaluator: Bt/ktt hold B and kt unshifted (the
+ * plain form's values), q.xy / q.z being texel coordinates. */
 struct L3dFastSrc {
     float Bt[9];
     float ktt[3];
@@ -146,6 +147,8 @@ struct L3dFastDev {
     const float* prior;        /* prior_all (rows of views with has_prior) */
     uint32_t* depths;
     const float4* coarse;      /* coarse level's planes (views with has_coarse) or NULL */
+    int exact;                 /* 1: exact evaluator (FP32 texture gathers, plain arithmetic) */
+    int comp;                  /* 1: Neumaier-compensated window sums */
 };
 
 /* kernel: L3D_K_INIT or L3D_K_PROPAGATE; iteration/phase select the RNG stream and the
@@ -384,7 +387,9 @@ void l3d_set_error(const char* msg);
 
 /* texture-rate probe (probe.cu) */
 long long l3d_texture_rate_blocks(int width, int height, int checker);
-cudaError_t l3d_launch_texture_rate(cudaTextureObject_t tex, int width, int height, int checker,
-                                    int reps, float* out, cudaStream_t s);
+/* probe launch; mode: 0 hardware bilinear, 1 gather + exact weights, 2 four point fetches,
+ * 3 four loads from img (linear F32, width * height) */
+cudaError_t l3d_launch_texture_rate(cudaTextureObject_t tex, const float* img, int width, int height,
+                                    int checker, int mode, int reps, float* out, cudaStream_t s);
 
 #endif

@@ -14,10 +14,11 @@ LIB_PATH = os.path.join(LIB_DIR, "libluvas3d.so")
 
 L3D_OK, L3D_EINVAL, L3D_ECUDA, L3D_ENOMEM, L3D_ESTATE, L3D_ETIMEOUT = range(6)
 DTYPE_U8, DTYPE_F32, DTYPE_F16, DTYPE_BF16 = range(4)
-FORM_PLAIN, FORM_FAST = 0, 1
+FORM_PLAIN, FORM_FAST, FORM_EXACT = 0, 1, 2
 WEIGHT_F32, WEIGHT_Q8 = 0, 1
 KERNEL_INIT, KERNEL_INIT_COARSE, KERNEL_PROPAGATE, KERNEL_PACK, KERNEL_CONSISTENCY = range(5)
 MAX_SOURCES = 8
+FETCH_FILTERED, FETCH_GATHER, FETCH_POINT, FETCH_LOADS = range(4)
 NOALLOC_MAX_BRICKS = 1 << 20
 
 
@@ -50,6 +51,7 @@ class StereoOpts(C.Structure):
         ("window", C.c_int32),
         ("dilation", C.c_int32),
         ("stream", C.c_void_p),
+        ("compensated", C.c_int32),
     ]
 
 
@@ -190,6 +192,7 @@ SIGNATURES = [
     ("l3d_image_downsample_gray", C.c_int, [_P, _I, _I, _I, _I, _P, _P]),
     ("l3d_depth_upsample", C.c_int, [_P, _I, _I, _I, _I, _P, _P]),
     ("l3d_measure_texture_rate", C.c_int, [_I, _I, C.POINTER(C.c_double)]),
+    ("l3d_measure_fetch_rate", C.c_int, [_I, _I, _I, C.POINTER(C.c_double)]),
     ("l3d_memory_trim", C.c_int, [C.c_int64]),
     ("l3d_memory_reserved", C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("l3d_ncc_forward", C.c_int, [_P, _I, C.POINTER(C.c_int32), _I, _P, _P, _P, _P]),

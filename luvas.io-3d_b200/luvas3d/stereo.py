@@ -44,6 +44,7 @@ class StereoOptions:
     window: int = 6
     dilation: int = 2
     stream: int | None = None              # cudaStream_t as an integer, or None
+    compensated: bool = False              # fast/exact forms: Neumaier-compensated window sums
 
 
 def _c_views(views: Sequence[StereoView]):
@@ -106,6 +107,7 @@ class DenseStereo:
         copts.window = int(o.window)
         copts.dilation = int(o.dilation)
         copts.stream = o.stream
+        copts.compensated = int(bool(o.compensated))
         self._coarse = o.coarse  # the coarse level must outlive this one
         h = C.c_void_p()
         cviews = _c_views(self.views)
@@ -387,10 +389,12 @@ def _coarse_to_fine(inp: StereoInput, settings: StereoSettings) -> StereoRun:
                     for v in inp.views]
     copts = StereoOptions(depth_maps=False, storage=settings.options.storage,
                           form=settings.options.form, window=settings.options.window,
-                          dilation=settings.options.dilation)
+                          dilation=settings.options.dilation,
+                          compensated=settings.options.compensated)
     coarse = DenseStereo(cw, ch, coarse_views, copts)
     fopts = StereoOptions(coarse=coarse, storage=settings.options.storage, form=settings.options.form,
-                          window=settings.options.window, dilation=settings.options.dilation)
+                          window=settings.options.window, dilation=settings.options.dilation,
+                          compensated=settings.options.compensated)
     stereo = DenseStereo(inp.width, inp.height, inp.views, fopts)
     try:
         upload_images(coarse, inp)

@@ -32,6 +32,7 @@ class StereoArgs(C.Structure):
         ("coarse_w", C.c_int32), ("coarse_h", C.c_int32),
         ("needed", C.c_int32), ("threads", C.c_int32),
         ("sizes", C.c_void_p),
+        ("compensated", C.c_int32),
     ]
 
 
@@ -143,7 +144,7 @@ class Stereo:
     reference view of the last call."""
 
     def __init__(self, width, height, views, images, precision: int = 32, window: int = 6,
-                 dilation: int = 2, threads: int = 0):
+                 dilation: int = 2, threads: int = 0, compensated: bool = False):
         self.V = len(views)
         self.views = _views_array(views)
         imgs = [np.ascontiguousarray(i, dtype=np.float32) for i in images]
@@ -162,6 +163,7 @@ class Stereo:
         self._depths = np.zeros(int(self.offsets[-1]), dtype=np.uint32)
         self._ref_shape = self.shapes[0]
         self.window, self.dilation, self.threads = window, dilation, threads
+        self.compensated = bool(compensated)
         self.coarse = None  # (hyp (h, w, 4) in this precision)
 
     @property
@@ -227,6 +229,7 @@ class Stereo:
         a.from_coarse = int(bool(from_coarse))
         a.needed = int(needed)
         a.threads = int(self.threads)
+        a.compensated = int(self.compensated)
         return a, keep
 
     def solve(self, ref, sources, **kw) -> None:

@@ -32,7 +32,8 @@
  *   bilinear sample    = at texel coordinates (u, v) = q.xy / q.z (the centre-aligned texture
  *                        coordinate of textureSampleLevel), exact weights, clamp-to-edge:
  *                        top = fma(fx, b - a, a), bot = fma(fx, d - c, c), fma(fy, bot-top, top)
- *   window sums        = sequential in sample order, sr = fma(w, v, sr), srr = fma(w v, v, srr)
+ *   window sums        = sequential in sample order, sr = fma(w, v, sr), srr = fma(w v, v, srr);
+ *                        with args.compensated, Neumaier sums of the rounded products instead
  *   range checks       = written NaN-safe (a NaN coordinate is out of range)
  */
 #include "oracle.h"
@@ -76,6 +77,31 @@ template <> struct Mth<double> {
 
 template <typename T> struct V3 { T x, y, z; };
 
+/* A window sum: plain (s = s + x, s = fma(a, b, s): the reference's running sums) or, with
+ * comp, Neumaier's compensated summation (Neumaier 1974) of the addends, products rounded first:
+ *   t = s + x;  c = c + (|s| >= |x| ? (s - t) + x : (x - t) + s);  s = t;  sum = s + c. */
+template <typename T> struct Sum {
+    bool comp;
+    T s = 0, c = 0;
+    explicit Sum(bool compensated) : comp(compensated) {}
+    void add(T x) {
+        if (comp) {
+            T t = s + x;
+            bool big = Mth<T>::abs(s) >= Mth<T>::abs(x);
+            T hi = big ? s : x, lo = big ? x : s;
+            c = c + ((hi - t) + lo);
+            s = t;
+        } else {
+            s = s + x;
+        }
+    }
+    void fma_add(T a, T b) {
+        if (comp) add(a * b);
+        else s = Mth<T>::fma(a, b, s);
+    }
+    T value() const { return comp ? s + c : s; }
+};
+
 template <typename T> inline T dot3(V3<T> a, V3<T> b) {
     return Mth<T>::fma(a.z, b.z, Mth<T>::fma(a.y, b.y, a.x * b.x));
 }
@@ -110,6 +136,7 @@ template <typename T> struct Params {
     T ck[4];
     int cW, cH;
     int win_n, win_dil;
+    int comp;                   /* compensated window sums */
     size_t ref_off;             /* offset of the reference image and depth map */
     Src<T> src[MAX_SOURCES];
 };
@@ -181,6 +208,7 @@ Params<T> build_params(const orc_stereo_args* a, int iteration, int phase, doubl
     }
     p.win_n = a->win_n > 0 ? a->win_n : 6;
     p.win_dil = a->win_dil > 0 ? a->win_dil : 2;
+    p.comp = a->compensated ? 1 : 0;
     const double kr[4] = {ref[0], ref[1], ref[2], ref[3]};
     for (int s = 0; s < p.n; s++) {
         const double* v = a->views + (size_t)a->sources[s] * ORC_VIEW_DOUBLES;
@@ -312,20 +340,20 @@ template <typename T> struct Kernel {
         const T c1 = T(2.0f) * T(0.06f) * T(0.06f);
         const T c2 = T(2.0f) * T(5.0f) * T(5.0f);
         T center = ref_pixel(x, y);
-        T sw = 0, sr = 0, srr = 0;
+        Sum<T> sw(p.comp), sr(p.comp), srr(p.comp);
         for (int i = 0; i < S; i++) {
             T v = ref_pixel(x + off[i][0], y + off[i][1]);
             T dc = v - center;
             T w = Mth<T>::exp(-(dc * dc) / c1 - ds[i] / c2);
             s.rv[i] = v;
             s.rw[i] = w;
-            sw = sw + w;
-            sr = Mth<T>::fma(w, v, sr);
-            srr = Mth<T>::fma(w * v, v, srr);
+            sw.add(w);
+            sr.fma_add(w, v);
+            srr.fma_add(w * v, v);
         }
-        s.rsum = sw;
-        s.rmean = sr / sw;
-        s.rvar = maxT(Mth<T>::fma(-s.rmean, s.rmean, srr / sw), T(0));
+        s.rsum = sw.value();
+        s.rmean = sr.value() / s.rsum;
+        s.rvar = maxT(Mth<T>::fma(-s.rmean, s.rmean, srr.value() / s.rsum), T(0));
     }
 
     T bilinear(const Src<T>& src, T u, T v) const {
@@ -346,7 +374,7 @@ template <typename T> struct Kernel {
         for (int r = 0; r < 3; r++)
             for (int c = 0; c < 3; c++) h[r * 3 + c] = Mth<T>::fma(src.kt[r], u[c], src.B[r * 3 + c]);
         const T wmax = (T)(src.W - 1), hmax = (T)(src.H - 1);
-        T ss = 0, sss = 0, srs = 0;
+        Sum<T> ss(p.comp), sss(p.comp), srs(p.comp);
         for (int i = 0; i < S; i++) {
             T x = s.px + (T)off[i][0];
             T y = s.py + (T)off[i][1];
@@ -359,16 +387,16 @@ template <typename T> struct Kernel {
             if (!(uu >= T(0) && vv >= T(0) && uu <= wmax && vv <= hmax)) return T(2);
             T val = bilinear(src, uu, vv);
             T w = s.rw[i];
-            ss = Mth<T>::fma(w, val, ss);
+            ss.fma_add(w, val);
             T wv = w * val;
-            sss = Mth<T>::fma(wv, val, sss);
-            srs = Mth<T>::fma(wv, s.rv[i], srs);
+            sss.fma_add(wv, val);
+            srs.fma_add(wv, s.rv[i]);
         }
-        T mean = ss / s.rsum;
-        T var_s = maxT(Mth<T>::fma(-mean, mean, sss / s.rsum), T(0));
+        T mean = ss.value() / s.rsum;
+        T var_s = maxT(Mth<T>::fma(-mean, mean, sss.value() / s.rsum), T(0));
         T den = Mth<T>::sqrt(s.rvar * var_s);
         if (den < T(1e-5f)) return T(1);
-        T cov = Mth<T>::fma(-s.rmean, mean, srs / s.rsum);
+        T cov = Mth<T>::fma(-s.rmean, mean, srs.value() / s.rsum);
         return clampT(T(1) - cov / den, T(0), T(2));
     }
 

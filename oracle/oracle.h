@@ -45,6 +45,8 @@ typedef struct {
     int32_t threads;           /* OpenMP threads, <= 0 for the default */
     const int32_t* sizes;      /* n_views (width, height) pairs, or NULL: every view is
                                   width x height.  Images and depth maps are concatenated per view */
+    int32_t compensated;       /* 1: window sums as Neumaier-compensated sums (the arithmetic of
+                                  the product's compensated mode); 0: the reference's plain sums */
 } orc_stereo_args;
 
 /* Full schedule of DenseStereo.solve (dense-stereo.ts:231-285) for one reference view. */

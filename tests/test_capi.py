@@ -42,7 +42,7 @@ def test_python_binding_covers_the_header():
 def test_struct_layouts_match_the_c_abi():
     # sizes under the x86-64 System V ABI
     assert C.sizeof(_lib.View) == 16 * 8
-    assert C.sizeof(_lib.StereoOpts) == 8 + 5 * 4 + 4 + 8
+    assert C.sizeof(_lib.StereoOpts) == 8 + 5 * 4 + 4 + 8 + 4 + 4
     assert C.sizeof(_lib.SolveOpts) == 8 + 8 + 16 + 8 + 16
     assert C.sizeof(_lib.IntegrationView) == 16 * 8 + 8 + 8 + 8
     assert C.sizeof(_lib.TsdfDesc) == 7 * 8 + 4 * 4 + 8 + 4 * 4 + 8
@@ -70,6 +70,20 @@ def test_bad_arguments_are_rejected_with_a_message():
     assert "window" in _lib.last_error()
     lib.l3d_stereo_opts_default(C.byref(opts))
     opts.storage = _lib.DTYPE_F16
+    assert lib.l3d_stereo_create(10, 10, 2, _views(), C.byref(opts), C.byref(h)) == _lib.L3D_EINVAL
+    opts.form = _lib.FORM_EXACT  # the exact form keeps FP32 texels
+    assert lib.l3d_stereo_create(10, 10, 2, _views(), C.byref(opts), C.byref(h)) == _lib.L3D_EINVAL
+    assert "exact form" in _lib.last_error()
+    lib.l3d_stereo_opts_default(C.byref(opts))
+    opts.compensated = 1  # the plain form is the oracle's uncompensated order
+    assert lib.l3d_stereo_create(10, 10, 2, _views(), C.byref(opts), C.byref(h)) == _lib.L3D_EINVAL
+    assert "compensated" in _lib.last_error()
+    lib.l3d_stereo_opts_default(C.byref(opts))
+    opts.form = _lib.FORM_EXACT
+    opts.window, opts.dilation = 11, 1
+    assert lib.l3d_stereo_create(10, 10, 2, _views(), C.byref(opts), C.byref(h)) == _lib.L3D_EINVAL
+    lib.l3d_stereo_opts_default(C.byref(opts))
+    opts.form = 3
     assert lib.l3d_stereo_create(10, 10, 2, _views(), C.byref(opts), C.byref(h)) == _lib.L3D_EINVAL
     bad = _views()
     bad[1].intrinsics.fx = 0

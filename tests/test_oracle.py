@@ -237,6 +237,31 @@ def test_fp32_and_fp64_oracles_agree_on_fixed_planes():
     assert err.max() < 1e-3
 
 
+def test_compensated_sums_are_a_distinct_arithmetic_closer_to_fp64():
+    """The compensated mode (Neumaier sums of the window terms) changes some FP32 costs in their
+    last bits, agrees with the plain sums to the NCC tolerance, and is at least as close to the
+    FP64 oracle."""
+    views, imgs, truth = wall_scene()
+    W, H = 160, 120
+    rng = np.random.default_rng(8)
+    planes = np.zeros((H, W, 4))
+    n = rng.normal(size=(H, W, 3)) * 0.2 + np.array([0, 0, -1.0])
+    planes[..., :3] = n / np.linalg.norm(n, axis=-1, keepdims=True)
+    planes[..., 3] = rng.uniform(1.3, 1.7, size=(H, W))
+    p32 = planes.astype(np.float32)
+    kw = dict(min_depth=0.5, max_depth=5.0)
+    plain, _ = oracle.Stereo(W, H, views, imgs, 32).plane_cost(2, [0, 1, 3, 4], p32, **kw)
+    comp, _ = oracle.Stereo(W, H, views, imgs, 32, compensated=True).plane_cost(2, [0, 1, 3, 4], p32, **kw)
+    c64, _ = oracle.Stereo(W, H, views, imgs, 64).plane_cost(2, [0, 1, 3, 4], p32.astype(np.float64), **kw)
+    valid = (c64 < 1.5) & (plain < 1.5) & (comp < 1.5)
+    assert valid.mean() > 0.8
+    assert np.any(plain != comp)
+    assert np.percentile(np.abs(plain - comp)[valid], 99.9) < 1e-4
+    e_plain = np.abs(plain[valid] - c64[valid])
+    e_comp = np.abs(comp[valid] - c64[valid])
+    assert e_comp.mean() <= e_plain.mean()
+
+
 def test_threads_do_not_change_results():
     """Red/black phases read only the other colour, so the parallel oracle is deterministic."""
     views, imgs, truth = wall_scene()
