@@ -698,7 +698,7 @@ def main():
 
     def accuracy(st) -> dict:
         """Packed depth maps of the last full solve against the rendered ground truth, scored
-        like the reference's stereo self-test (frontend/tools/verify/stereo-check.ts:55-77):
+        like the reference's stereo self-test (frontend/tools/verify/stereo-check.ts:56-73):
         surface pixels (truth > 0) with a non-zero packed entry count as valid; relative error of
         the packed half depth, median and p90, over all views of this rank."""
         errs, surf, valid = [], 0, 0

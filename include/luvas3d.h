@@ -83,15 +83,15 @@ typedef struct {
     double t[3];
 } l3d_pose;
 
-/* StereoView (mvs/dense-stereo.ts:57-60). */
+/* StereoView (mvs/dense-stereo.ts:11-14). */
 typedef struct {
     l3d_intrinsics intrinsics;
     l3d_pose pose;
 } l3d_view;
 
-/* StereoOptions (mvs/dense-stereo.ts:84-88) plus the device layout choices. */
+/* StereoOptions (mvs/dense-stereo.ts:38-42) plus the device layout choices. */
 typedef struct {
-    const l3d_stereo* coarse; /* CoarseLevel (dense-stereo.ts:78-82): its planes seed from_coarse
+    const l3d_stereo* coarse; /* CoarseLevel (dense-stereo.ts:32-36): its planes seed from_coarse
                                  solves; it must outlive this handle.  NULL = none */
     int32_t depth_maps;       /* 1: a packed depth map per view (default); 0: one map */
     int32_t storage;          /* device image storage: F32 (plain form); U8, F16, BF16 or F32 (fast) */
@@ -105,7 +105,7 @@ typedef struct {
                                  added with Neumaier compensation); 0 = plain FP32 sums */
 } l3d_stereo_opts;
 
-/* SolveOptions (mvs/dense-stereo.ts:62-75). */
+/* SolveOptions (mvs/dense-stereo.ts:16-29). */
 typedef struct {
     const int32_t* sources;   /* source layers; the first 8 are used (MAX_SOURCES) */
     int32_t n_sources;
@@ -163,12 +163,12 @@ typedef struct {
  * (pipeline/stages/stage-runner.ts:40-49, gpu/gpu-device.ts:92-100). */
 size_t l3d_last_error(char* buf, size_t size);
 
-/* ---- stereo: DenseStereo (mvs/dense-stereo.ts:107-416) ---- */
+/* ---- stereo: DenseStereo (mvs/dense-stereo.ts:61-370) ---- */
 
 /* Fills the reference defaults: depth_maps 1, storage F32, form PLAIN, window 6, dilation 2. */
 void l3d_stereo_opts_default(l3d_stereo_opts* opts);
 
-/* new DenseStereo(device, width, height, views, options) (dense-stereo.ts:126-218). */
+/* new DenseStereo(device, width, height, views, options) (dense-stereo.ts:80-172). */
 int l3d_stereo_create(int32_t width, int32_t height, int32_t n_views, const l3d_view* views,
                       const l3d_stereo_opts* opts, l3d_stereo** out);
 
@@ -180,12 +180,12 @@ int l3d_stereo_create_sized(int32_t n_views, const l3d_view* views, const int32_
 /* Image size of one view. */
 int l3d_stereo_view_size(const l3d_stereo* s, int32_t layer, int32_t* width, int32_t* height);
 
-/* DenseStereo.setImage(layer, gray) (dense-stereo.ts:221-228).  dtype is the host element type;
+/* DenseStereo.setImage(layer, gray) (dense-stereo.ts:175-182).  dtype is the host element type;
  * row_stride_bytes = 0 means tightly packed rows. */
 int l3d_stereo_set_image(l3d_stereo* s, int32_t layer, int32_t dtype, const void* pixels,
                          int64_t row_stride_bytes);
 
-/* DenseStereo.solve(ref, options) (dense-stereo.ts:231-285): init (or init_coarse), iterations
+/* DenseStereo.solve(ref, options) (dense-stereo.ts:185-239): init (or init_coarse), iterations
  * x red/black propagate, pack. */
 int l3d_stereo_solve(l3d_stereo* s, int32_t ref, const l3d_solve_opts* opts);
 
@@ -198,11 +198,11 @@ int l3d_stereo_solve_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
                          const l3d_solve_opts* opts);
 
 /* One kernel of the schedule over the whole image of view ref, with the dispatch state of
- * (iteration, phase): the unit DenseStereo.sliced submits (dense-stereo.ts:315-335). */
+ * (iteration, phase): the unit DenseStereo.sliced submits (dense-stereo.ts:269-289). */
 int l3d_stereo_dispatch(l3d_stereo* s, int32_t kernel, int32_t ref, const l3d_solve_opts* opts,
                         int32_t iteration, int32_t phase);
 
-/* DenseStereo.filter(ref, sources, needed) (dense-stereo.ts:296-309): consistency filter of
+/* DenseStereo.filter(ref, sources, needed) (dense-stereo.ts:250-263): consistency filter of
  * depths[ref] into the filtered map. */
 int l3d_stereo_filter(l3d_stereo* s, int32_t ref, const int32_t* checks, int32_t n_checks,
                       int32_t needed);
@@ -213,13 +213,13 @@ int l3d_stereo_filter_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
                           const int32_t* checks, const int32_t* needed);
 
 /* Reads (block until the handle's queued work is done). */
-/* DenseStereo.filteredMap readback (dense-stereo.ts:347-352) of the filtered map. */
+/* DenseStereo.filteredMap readback (dense-stereo.ts:301-306) of the filtered map. */
 int l3d_stereo_read_filtered(l3d_stereo* s, uint32_t* out);
 /* filtered_all[layer]. */
 int l3d_stereo_read_filtered_layer(l3d_stereo* s, int32_t layer, uint32_t* out);
-/* DenseStereo.depthMap(ref) (dense-stereo.ts:355-358). */
+/* DenseStereo.depthMap(ref) (dense-stereo.ts:309-312). */
 int l3d_stereo_read_depth(l3d_stereo* s, int32_t ref, uint32_t* out);
-/* DenseStereo.hypotheses (dense-stereo.ts:288-290) and the cost buffer; hyp4 is
+/* DenseStereo.hypotheses (dense-stereo.ts:242-244) and the cost buffer; hyp4 is
  * width * height * 4 floats (normal xyz, depth).  Either pointer may be NULL. */
 int l3d_stereo_read_hyp(l3d_stereo* s, float* hyp4, float* cost);
 /* hyp_all/cost_all of one layer after solve_all. */
@@ -264,20 +264,34 @@ int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
  * first use and replays the graph for identical requests (batches with priors are launched
  * directly).  No reference counterpart. */
 int l3d_stereo_set_graphs(l3d_stereo* s, int32_t enable);
-/* DenseStereo.destroy() (dense-stereo.ts:403-416). */
+/* DenseStereo.destroy() (dense-stereo.ts:357-370). */
 void l3d_stereo_destroy(l3d_stereo* s);
 
 /* ---- TSDF: TsdfVolume (fusion/tsdf-volume.ts:158-291) ---- */
 
-/* new TsdfVolume(device, grid, layout, depthBuffer, width, height) (tsdf-volume.ts:171-222). */
+/* new TsdfVolume(device, grid, layout, depthBuffer, width, height) (tsdf-volume.ts:171-217). */
 int l3d_tsdf_create(const l3d_tsdf_desc* desc, l3d_tsdf** out);
 
-/* TsdfVolume.integrate(view) (tsdf-volume.ts:445-473): integrates one packed depth map, either
+/* TsdfVolume.integrate(view) (tsdf-volume.ts:240-268): integrates one packed depth map, either
  * the filtered map of stereo (src != NULL, the buffer shared at tsdf-meshing.ts:71) or a host
- * map (packed, width * height u32).  Brick culling (visibleBricks, tsdf-volume.ts:425-439) runs
+ * map (packed, width * height u32).  Brick culling (visibleBricks, tsdf-volume.ts:220-234) runs
  * on the device. */
 int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packed,
                        const l3d_integration_view* view);
+
+/* TsdfVolume.integrate(view) (tsdf-volume.ts:240-268) of the filter_all map of one layer of
+ * src: the reference's one-view-per-pass form on the batched filtered maps. */
+int l3d_tsdf_integrate_layer(l3d_tsdf* t, const l3d_stereo* src, int32_t layer,
+                             const l3d_integration_view* view);
+
+/* The work of integrating n depth maps (arguments as for l3d_tsdf_integrate_many) without doing
+ * it: *visible receives the voxel-views that visibleBricks keeps, *updates the voxel-updates the
+ * integration applies (the voxels a view's depth sample updates).  12 bytes per update (f32 tsdf
+ * and Q8.8 weight read and written) are the algorithmic bytes of the one-view-per-pass form.
+ * Synchronises.  No reference counterpart. */
+int l3d_tsdf_count_updates(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                           const uint32_t* packed, int32_t n, const l3d_integration_view* views,
+                           int64_t* visible, int64_t* updates);
 
 /* Integrates n depth maps in one sweep over the volume (each voxel read and written once);
  * equal, bit for bit, to n integrate() calls in order.  Maps come from src's filtered_all
@@ -294,7 +308,7 @@ int l3d_tsdf_integrate_many_read(l3d_tsdf* t, const l3d_stereo* src, const int32
                                  const uint32_t* packed, int32_t n,
                                  const l3d_integration_view* views, float* tsdf, void* weight);
 
-/* TsdfVolume.read() (tsdf-volume.ts:475-482).  weight is float* (F32) or uint16_t* (Q8).
+/* TsdfVolume.read() (tsdf-volume.ts:270-277).  weight is float* (F32) or uint16_t* (Q8).
  * Either pointer may be NULL. */
 int l3d_tsdf_read(l3d_tsdf* t, float* tsdf, void* weight);
 /* Back to the initial state (tsdf 1, weight 0). */
@@ -305,7 +319,7 @@ int l3d_tsdf_device_buffers(const l3d_tsdf* t, float** tsdf, void** weight);
 int l3d_tsdf_stream(const l3d_tsdf* t, void** stream);
 int l3d_tsdf_synchronize(l3d_tsdf* t);
 int64_t l3d_tsdf_launches(const l3d_tsdf* t);
-/* TsdfVolume.destroy() (tsdf-volume.ts:484-495). */
+/* TsdfVolume.destroy() (tsdf-volume.ts:279-290). */
 void l3d_tsdf_destroy(l3d_tsdf* t);
 
 /* ---- Dense point cloud: PointAccumulator (fusion/point-accumulator.ts:16-147) fed by
@@ -486,7 +500,7 @@ int l3d_measure_fetch_rate(int32_t dtype, int32_t checker, int32_t mode, double*
  * call.  l3d_memory_trim waits for the current device's queued work, then hands the pool's
  * unused memory back to the driver until at most keep_bytes stay reserved (0 releases all of
  * it); memory held by live handles stays.  It replaces what GPUBuffer.destroy() does for the
- * reference at once (fusion/tsdf-volume.ts:279-290, mvs/dense-stereo.ts:357-369): a caller
+ * reference at once (fusion/tsdf-volume.ts:279-290, mvs/dense-stereo.ts:357-370): a caller
  * that shares the device with another allocator calls it after destroying handles. */
 int l3d_memory_trim(int64_t keep_bytes);
 

@@ -5,8 +5,8 @@
  * The host side replaces DenseStereo and TsdfVolume (frontend/src/app/vision/mvs/dense-stereo.ts,
  * frontend/src/app/vision/fusion/tsdf-volume.ts).  Differences from the WebGPU host, by design:
  * whole-image launches instead of 20 ms row bands with a host wait per band
- * (dense-stereo.ts:315-344), brick culling on the device instead of a CPU loop
- * (tsdf-volume.ts:425-439), and stream-ordered asynchronous calls instead of awaits.
+ * (dense-stereo.ts:269-298), brick culling on the device instead of a CPU loop
+ * (tsdf-volume.ts:220-234), and stream-ordered asynchronous calls instead of awaits.
  */
 #include <cuda_runtime.h>
 
@@ -180,7 +180,7 @@ struct l3d_stereo {
 
 namespace {
 
-/* DenseStereo.params (dense-stereo.ts:360-401) for one dispatch, FP64 -> f32.  The homography
+/* DenseStereo.params (dense-stereo.ts:314-355) for one dispatch, FP64 -> f32.  The homography
  * base B = K_s R K_r^-1 and kt = K_s t are composed in FP64 here. */
 void relative_pose(const l3d_pose& a, const l3d_pose& b, double* R, double* t) {
     /* relativePose (geometry/camera.ts:73-77), reference summation order */
@@ -220,7 +220,7 @@ L3dParams build_params(const l3d_stereo* s, int ref, const int32_t* sources, int
     p.range[0] = (float)(1.0 / min_depth);
     p.range[1] = (float)(1.0 / max_depth);
     p.range[2] = (float)step;
-    p.range[3] = (float)0.2;                 /* GEOMETRIC_WEIGHT, dense-stereo.ts:92 */
+    p.range[3] = (float)0.2;                 /* GEOMETRIC_WEIGHT, dense-stereo.ts:46 */
     p.iter = (unsigned)iteration;
     p.phase = (unsigned)phase;
     p.seed = seed_of(ref, iteration, phase, flags);
@@ -323,12 +323,12 @@ int launch(l3d_stereo* s, int kernel, const L3dParams& p, const L3dStereoDev& d)
     return L3D_OK;
 }
 
-/* One reference view through the schedule of DenseStereo.solve (dense-stereo.ts:231-285),
+/* One reference view through the schedule of DenseStereo.solve (dense-stereo.ts:185-239),
  * on hypothesis buffers hyp/cost. */
 int solve_one(l3d_stereo* s, int ref, const l3d_solve_opts* o, float4* hyp, float* cost,
               float* prior_dev) {
     int n = std::min(o->n_sources, L3D_MAX_SOURCES);
-    if (n == 0) return L3D_OK;                            /* dense-stereo.ts:233 */
+    if (n == 0) return L3D_OK;                            /* dense-stereo.ts:187 */
     const int flags = o->geometric ? 1 : 0;
     L3dStereoDev d = dev_of(s);
     d.hyp = hyp;
@@ -399,7 +399,7 @@ int fast_capacity(l3d_stereo* s, int n) {
 }
 
 /* The parameters of one reference view for the fast kernels: DenseStereo.params
- * (dense-stereo.ts:360-401) with the homography base shifted by half a texel for the texture
+ * (dense-stereo.ts:314-355) with the homography base shifted by half a texel for the texture
  * unit (Bt = S B, ktt = S kt, S = [[1, 0, .5], [0, 1, .5], [0, 0, 1]]), composed in FP64. */
 L3dFastView fast_view(const l3d_stereo* s, int ref, const l3d_solve_opts* o, long long pix_off) {
     L3dParams p = build_params(s, ref, o->sources, std::min(o->n_sources, L3D_MAX_SOURCES),
@@ -652,7 +652,7 @@ int fast_solve(l3d_stereo* s, int n, const int32_t* refs, const l3d_solve_opts* 
     int max_it = 0;
     bool any_pack = false;
     for (int i = 0; i < n; i++) {
-        if (std::min(opts[i].n_sources, L3D_MAX_SOURCES) == 0) continue;  /* dense-stereo.ts:233 */
+        if (std::min(opts[i].n_sources, L3D_MAX_SOURCES) == 0) continue;  /* dense-stereo.ts:187 */
         r.push_back(refs[i]);
         o.push_back(opts[i]);
         max_it = std::max(max_it, opts[i].iterations);
@@ -993,7 +993,7 @@ int l3d_stereo_filter(l3d_stereo* s, int32_t ref, const int32_t* checks, int32_t
     int rc = check_sources(s, checks, n);
     if (rc) return rc;
     if (s->n_maps == 1 && s->V > 1) return fail(L3D_ESTATE, "handle was created without per-view depth maps");
-    /* DenseStereo.filter (dense-stereo.ts:296-309): range 0.01 - 100 m, no flags */
+    /* DenseStereo.filter (dense-stereo.ts:250-263): range 0.01 - 100 m, no flags */
     L3dParams p = build_params(s, ref, checks, std::min(n, L3D_MAX_SOURCES), 0.01, 100.0, 0, 0, 0.0,
                                0, needed, 0, 0);
     s->filtered_ref = ref;
@@ -1409,6 +1409,8 @@ struct l3d_tsdf {
     float* priors = nullptr;          /* uploaded priors, prior_cap * P */
     long long prior_cap = 0;
     float4* normals = nullptr;        /* decoded normal per 12-bit normal code */
+    float* tiles = nullptr;           /* depth tiles of the depth-aware brick cull, tile_cap */
+    long long tile_cap = 0;
     L3dTsdfView* views_host = nullptr;      /* pinned staging for views */
     const uint32_t** ptrs_host = nullptr;   /* pinned staging for depth pointers */
     long long launches = 0;
@@ -1468,6 +1470,18 @@ int ensure_mask(l3d_tsdf* t, int n) {
     t->mask_views = 0;
     L3D_CUDA(cudaMalloc(&t->mask, (size_t)t->g.bricks * n), "brick mask");
     t->mask_views = n;
+    return L3D_OK;
+}
+
+/* Depth tiles of the depth-aware brick cull, sized in tiles. */
+int ensure_tiles(l3d_tsdf* t, long long n) {
+    if (t->tile_cap >= n) return L3D_OK;
+    cudaStreamSynchronize(t->stream);
+    cudaFree(t->tiles);
+    t->tiles = nullptr;
+    t->tile_cap = 0;
+    L3D_CUDA(cudaMalloc(&t->tiles, (size_t)n * sizeof(float)), "depth tiles");
+    t->tile_cap = n;
     return L3D_OK;
 }
 
@@ -1609,16 +1623,23 @@ int l3d_tsdf_reset(l3d_tsdf* t) {
     return L3D_OK;
 }
 
-int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packed,
-                       const l3d_integration_view* view) {
+/* Body of l3d_tsdf_integrate and l3d_tsdf_integrate_layer: layer < 0 takes the stereo handle's
+ * last filter() map, layer >= 0 its filter_all map of that layer. */
+static int integrate_one(l3d_tsdf* t, const l3d_stereo* src, int layer, const uint32_t* packed,
+                         const l3d_integration_view* view) {
     if (!t) return fail(L3D_EINVAL, "NULL handle");
     int rc = check_view(view);
     if (rc) return rc;
     if ((src == nullptr) == (packed == nullptr))
         return fail(L3D_EINVAL, "give exactly one of a stereo handle or a packed map");
+    if (src && layer >= 0) {
+        if (layer >= src->V) return fail(L3D_EINVAL, "layer %d out of range [0, %d)", layer, src->V);
+        if (!src->filtered_all) return fail(L3D_ESTATE, "stereo handle has no filter_all output");
+    }
     /* a stereo handle's filtered map has the size of the view it was filtered for */
-    const int mw = src ? src->Wv[src->filtered_ref] : t->g.W;
-    const int mh = src ? src->Hv[src->filtered_ref] : t->g.H;
+    const int ml = src ? (layer >= 0 ? layer : src->filtered_ref) : 0;
+    const int mw = src ? src->Wv[ml] : t->g.W;
+    const int mh = src ? src->Hv[ml] : t->g.H;
     const long long P = (long long)mw * mh;
     if ((rc = ensure_mask(t, 1))) return rc;
     L3dTsdfView v = make_view(*view);
@@ -1627,7 +1648,7 @@ int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packe
     const uint32_t* depth;
     if (src) {
         if ((rc = after_stereo(t, src))) return rc;
-        depth = src->filtered;
+        depth = layer >= 0 ? src->filtered_all + src->offv[layer] : src->filtered;
     } else {
         if ((rc = ensure_maps(t, P))) return rc;
         L3D_CUDA(cudaMemcpyAsync(t->maps, packed, P * 4, cudaMemcpyHostToDevice, t->stream), "map upload");
@@ -1640,12 +1661,25 @@ int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packe
         prior = t->priors;
     }
     /* visibility of this view's bricks, then the integration: two launches */
-    cudaError_t e = l3d_launch_tsdf_view(t->g, v, t->coords, t->mask, depth, prior, t->tsdf, t->weight,
-                                         t->q8, t->stream);
-    t->launches += 2;
+    if ((rc = ensure_tiles(t, l3d_depth_tile_count(mw, mh)))) return rc;
+    cudaError_t e = l3d_launch_tsdf_view(t->g, v, t->coords, t->mask, depth, prior, t->normals, t->tiles,
+                                         t->tsdf, t->weight, t->q8, t->stream);
+    t->launches += 3;
     if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
     if (src && (rc = before_stereo(t, src))) return rc;
     return L3D_OK;
+}
+
+int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packed,
+                       const l3d_integration_view* view) {
+    return integrate_one(t, src, -1, packed, view);
+}
+
+int l3d_tsdf_integrate_layer(l3d_tsdf* t, const l3d_stereo* src, int32_t layer,
+                             const l3d_integration_view* view) {
+    if (!src) return fail(L3D_EINVAL, "stereo handle is NULL");
+    if (layer < 0) return fail(L3D_EINVAL, "layer %d out of range", layer);
+    return integrate_one(t, src, layer, nullptr, view);
 }
 
 /* Body of l3d_tsdf_integrate_many and l3d_tsdf_integrate_many_read: with output buffers the
@@ -1653,7 +1687,7 @@ int l3d_tsdf_integrate(l3d_tsdf* t, const l3d_stereo* src, const uint32_t* packe
  * copied out on the copy stream as soon as its launch is done. */
 static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
                           const uint32_t* packed, int32_t n, const l3d_integration_view* views,
-                          float* tsdf_out, void* weight_out) {
+                          float* tsdf_out, void* weight_out, int64_t* counts_out = nullptr) {
     if (!t) return fail(L3D_EINVAL, "NULL handle");
     if (n < 0 || (n > 0 && !views)) return fail(L3D_EINVAL, "bad view list");
     if (n == 0) return L3D_OK;
@@ -1695,6 +1729,17 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
                 L3D_CUDA(cudaMemcpyAsync(t->priors + poff[i], views[i].prior, (size_t)mw[i] * mh[i] * 4,
                                          cudaMemcpyHostToDevice, t->stream), "prior upload");
     }
+    /* depth tiles per view for the depth-aware brick cull (integration only: the update count
+     * reports what visibleBricks alone keeps) */
+    std::vector<long long> toff(n);
+    long long ttotal = 0, tmax = 0;
+    for (int i = 0; i < n; i++) {
+        toff[i] = ttotal;
+        const long long nt = l3d_depth_tile_count(mw[i], mh[i]);
+        ttotal += nt;
+        tmax = std::max(tmax, nt);
+    }
+    if (!counts_out && (rc = ensure_tiles(t, ttotal))) return rc;
     /* the pinned staging tables are reused: wait until the previous call's copies have run */
     L3D_CUDA(cudaEventSynchronize(t->staged), "staging wait");
     for (int i = 0; i < n; i++) {
@@ -1702,15 +1747,38 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
         t->views_host[i].W = mw[i];
         t->views_host[i].H = mh[i];
         t->views_host[i].prior_off = poff[i];
+        t->views_host[i].tile_off = toff[i];
         t->ptrs_host[i] = src ? src->filtered_all + src->offv[layers[i]] : t->maps + (size_t)i * P;
     }
     L3D_CUDA(cudaMemcpyAsync(t->views, t->views_host, (size_t)n * sizeof(L3dTsdfView), cudaMemcpyHostToDevice, t->stream), "view upload");
     L3D_CUDA(cudaMemcpyAsync(t->depth_ptrs, t->ptrs_host, (size_t)n * sizeof(void*), cudaMemcpyHostToDevice, t->stream), "view upload");
     L3D_CUDA(cudaEventRecord(t->staged, t->stream), "event record");
-    cudaError_t e = l3d_launch_tsdf_visible(t->g, t->views, n, t->coords, t->mask, t->stream);
-    t->launches++;
+    cudaError_t e;
+    if (counts_out) {
+        e = l3d_launch_tsdf_visible(t->g, t->views, n, t->coords, t->mask, t->stream);
+        t->launches++;
+    } else {
+        e = l3d_launch_depth_tiles(t->views, n, t->depth_ptrs, t->priors, t->tiles, tmax, t->stream);
+        if (e == cudaSuccess)
+            e = l3d_launch_tsdf_visible_depth(t->g, t->views, n, t->coords, t->tiles, t->mask, t->stream);
+        t->launches += 2;
+    }
     if (e != cudaSuccess) return cuda_fail(e, "visibility launch");
-    if (!tsdf_out && !weight_out) {
+    if (counts_out) {
+        unsigned long long* counts = nullptr;
+        unsigned long long host[2] = {0, 0};
+        L3D_CUDA(pool_alloc((void**)&counts, 2 * sizeof(unsigned long long), t->stream), "count buffer");
+        if ((e = cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), t->stream)) == cudaSuccess &&
+            (e = l3d_launch_tsdf_count(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
+                                       t->normals, counts, t->stream)) == cudaSuccess &&
+            (e = cudaMemcpyAsync(host, counts, sizeof(host), cudaMemcpyDeviceToHost, t->stream)) == cudaSuccess)
+            e = cudaStreamSynchronize(t->stream);
+        t->launches++;
+        cudaFreeAsync(counts, t->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "update count");
+        counts_out[0] = (int64_t)host[0];
+        counts_out[1] = (int64_t)host[1];
+    } else if (!tsdf_out && !weight_out) {
         e = l3d_launch_tsdf_many(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
                                  t->normals, t->tsdf, t->weight, t->q8, t->stream);
         t->launches++;
@@ -1753,6 +1821,17 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
     }
     if (src && (rc = before_stereo(t, src))) return rc;
     return L3D_OK;
+}
+
+int l3d_tsdf_count_updates(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                           const uint32_t* packed, int32_t n, const l3d_integration_view* views,
+                           int64_t* visible, int64_t* updates) {
+    if (!visible || !updates) return fail(L3D_EINVAL, "visible and updates must not be NULL");
+    int64_t c[2] = {0, 0};
+    int rc = integrate_many(t, src, layers, packed, n, views, nullptr, nullptr, c);
+    *visible = c[0];
+    *updates = c[1];
+    return rc;
 }
 
 int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
@@ -1872,6 +1951,7 @@ void l3d_tsdf_destroy(l3d_tsdf* t) {
     cudaFree(t->maps);
     cudaFree(t->priors);
     cudaFree(t->normals);
+    cudaFree(t->tiles);
     cudaFreeHost(t->views_host);
     cudaFreeHost(t->ptrs_host);
     if (t->done) cudaEventDestroy(t->done);

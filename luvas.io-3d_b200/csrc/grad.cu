@@ -127,7 +127,7 @@ __device__ void current_pose(const L3dGradView& b, const float* deltas, int view
 }
 
 /* One thread per (reference, source) pair: relative pose (relativePose, geometry/camera.ts:73-77)
- * and homography base B = K_s R K_r^-1, kt = K_s t (DenseStereo.params, dense-stereo.ts:360-401)
+ * and homography base B = K_s R K_r^-1, kt = K_s t (DenseStereo.params, dense-stereo.ts:314-355)
  * in FP64, rounded to f32. */
 __global__ void k_compose(const L3dGradView* __restrict__ views, const float* __restrict__ deltas,
                           const L3dGradJob job, L3dGradPair* __restrict__ pairs) {

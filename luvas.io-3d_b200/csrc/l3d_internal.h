@@ -7,7 +7,7 @@
 #include <stdint.h>
 #include <cuda_runtime.h>
 
-#define L3D_MAX_SOURCES 8      /* MAX_SOURCES, mvs/dense-stereo.ts:90 */
+#define L3D_MAX_SOURCES 8      /* MAX_SOURCES, mvs/dense-stereo.ts:44 */
 #define L3D_FILTER_COST 7u     /* FILTER_COST, mvs/patchmatch.wgsl.ts:43 */
 
 /* One source view of a dispatch: the View block of patchmatch.wgsl.ts:4-10 (k, R rows, t,
@@ -26,7 +26,7 @@ struct L3dSrc {
 };
 
 /* The Params block of patchmatch.wgsl.ts:12-26 as DenseStereo.params fills it
- * (dense-stereo.ts:360-401); the band rows are gone (whole-image launches). */
+ * (dense-stereo.ts:314-355); the band rows are gone (whole-image launches). */
 struct L3dParams {
     float k[4];
     float kinv[4];             /* 1/fx, 1/fy, -cx/fx, -cy/fy in f32 */
@@ -40,7 +40,7 @@ struct L3dParams {
     L3dSrc src[L3D_MAX_SOURCES];
 };
 
-/* Per-view constants of the TSDF integrate uniform (tsdf-volume.ts:286-296), in f32, plus the
+/* Per-view constants of the TSDF integrate uniform (tsdf-volume.ts:81-91), in f32, plus the
  * FP64 pose for brick culling. */
 struct L3dTsdfView {
     float k[4];
@@ -50,6 +50,7 @@ struct L3dTsdfView {
     int has_prior;
     int W, H;                  /* this view's depth-map size */
     long long prior_off;       /* element offset of this view's prior in the prior buffer */
+    long long tile_off;        /* element offset of this view's depth tiles (depth-aware culling) */
     double kd[4];
     double Rd[9];
     double td[3];
@@ -172,10 +173,34 @@ cudaError_t l3d_launch_convert(const void* src, int dtype, int64_t row_stride, i
 
 cudaError_t l3d_launch_tsdf_visible(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
                                     const int32_t* coords, uint8_t* mask, cudaStream_t stream);
-/* visibility of one view (into mask) followed by its integration: two launches */
+/* visibility of one view (into mask) followed by its integration: two launches (three with
+ * tiles).  normals: the decoded-normal table (l3d_launch_normal_table), or NULL to decode each
+ * normal in place; tiles: scratch of l3d_depth_tile_count(v.W, v.H) floats for the depth-aware
+ * cull, or NULL for visibleBricks alone (same results either way) */
 cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,
                                  uint8_t* mask, const uint32_t* depth, const float* prior,
-                                 float* tsdf, void* weight, int q8, cudaStream_t stream);
+                                 const float4* normals, float* tiles, float* tsdf, void* weight, int q8,
+                                 cudaStream_t stream);
+/* Depth tiles for the depth-aware brick cull: per view, the largest depth a voxel of that view
+ * can be updated from over every L3D_DEPTH_TILE x L3D_DEPTH_TILE pixel tile (decoded f16 depth,
+ * or the prior where the map has none), views[i].tile_off elements into `tiles`. */
+#define L3D_DEPTH_TILE 8
+long long l3d_depth_tile_count(int W, int H);
+cudaError_t l3d_launch_depth_tiles(const L3dTsdfView* views_dev, int n_views,
+                                   const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                   float* tiles, long long max_tiles, cudaStream_t stream);
+/* brick mask of n views with the depth-aware cull: visibleBricks and, where `tiles` is given
+ * (l3d_launch_depth_tiles first), not provably behind every depth of its footprint by more than
+ * the truncation band (such a brick has no voxel that updates) */
+cudaError_t l3d_launch_tsdf_visible_depth(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
+                                          const int32_t* coords, const float* tiles, uint8_t* mask,
+                                          cudaStream_t stream);
+/* counts[0] += visible voxel-views, counts[1] += voxel-updates of a many-view integration */
+cudaError_t l3d_launch_tsdf_count(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
+                                  const int32_t* coords, const uint8_t* mask,
+                                  const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                  const float4* normals, unsigned long long* counts,
+                                  cudaStream_t stream);
 /* normals[code] = unpack_normal(code << 16) for the 4096 normal codes */
 cudaError_t l3d_launch_normal_table(float4* normals, cudaStream_t stream);
 cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,

@@ -1,20 +1,27 @@
 /*
  * TSDF integration of packed depth maps (frontend/src/app/vision/fusion/tsdf-volume.ts).
  *
- *   k_visible      visibleBricks (tsdf-volume.ts:425-439) on the device: one thread per
+ *   k_visible      visibleBricks (tsdf-volume.ts:220-234) on the device: one thread per
  *                  (brick, view) evaluates the reference's FP64 frustum test, in the reference's
  *                  operation order (built with --fmad=false, so no FP64 contraction).
- *   k_integrate    one view per launch (TsdfVolume.integrate, tsdf-volume.ts:445-473).  A thread
+ *   k_integrate    one view per launch (TsdfVolume.integrate, tsdf-volume.ts:240-268).  A thread
  *                  owns four consecutive voxels along x (inside one 8^3 brick): it computes the
- *                  four observations from the L2-resident depth map first and touches the volume
- *                  only when one of them updates, with one 128-bit tsdf access and one 64-bit
- *                  (Q8.8) or 128-bit (f32) weight access.  HBM-bound.
+ *                  four observations from the L2-resident depth map first (the four depth loads
+ *                  in flight together, normals from the decoded-normal table) and touches the
+ *                  volume only when one of them updates, with one 128-bit tsdf access and one
+ *                  64-bit (Q8.8) or 128-bit (f32) weight access; culled bricks read nothing but
+ *                  their mask byte.
+ *   k_count_updates
+ *                  the visible voxel-views and voxel-updates of a many-view integration, without
+ *                  its writes (the algorithmic bytes of the one-view-per-launch form).
+ *   k_depth_tiles, k_visible_depth
+ *                  the depth-aware half of the brick cull (see brick_behind_depths).
  *   k_integrate_many
  *                  many views per sweep: the same thread keeps its four voxels in registers,
  *                  applies every view in order and writes back once; per-voxel results equal the
  *                  per-view launches bit for bit (the per-voxel update order is unchanged).
  *
- * Per-voxel arithmetic (tsdf-volume.ts:316-358), fixed order shared with the FP32 restatement:
+ * Per-voxel arithmetic (tsdf-volume.ts:111-153), fixed order shared with the FP32 restatement:
  *   world = fma(i + 0.5, voxel, origin); cam = R world + t (fma chain); pixel =
  *   rint(fma(f * cam, 1 / cam.z, c)); weight w = max(0.2, |n . normalize(cam)|) x confidence
  *   factor, or the prior weight; tsdf <- fma(tsdf, w0, obs * w) / (w0 + w);
@@ -201,7 +208,7 @@ __device__ __forceinline__ bool quad_coords(const L3dTsdfGrid& g, const int32_t*
     return true;
 }
 
-/* visibleBricks (tsdf-volume.ts:425-439) for brick b of view v, FP64, reference order. */
+/* visibleBricks (tsdf-volume.ts:220-234) for brick b of view v, FP64, reference order. */
 __device__ __forceinline__ uint8_t brick_visible(const L3dTsdfGrid& g, const L3dTsdfView& v,
                                                  const int32_t* __restrict__ coords, long long b) {
     int bx, by, bz;
@@ -241,6 +248,119 @@ __global__ void k_visible(const L3dTsdfGrid g, const L3dTsdfView* __restrict__ v
     mask[t] = brick_visible(g, views[vi], coords, b);
 }
 
+/* The depth-aware half of the brick cull.  A voxel of view v is updated only from the depth d
+ * of the pixel it rounds to (the packed map's, or the prior where the map has none), and only
+ * if d - z >= -mu for its camera depth z.  The voxel centres of brick b span a box; its eight
+ * corners, projected in FP64, bound every centre's camera depth from below (z is affine) and its
+ * pixel to the corners' bounding rectangle widened by a pixel (the FP32 projection is rounded
+ * to the nearest pixel and differs from FP64 by far less than that).  If the smallest corner
+ * depth exceeds the largest depth over the depth tiles covering that rectangle by more than mu
+ * plus a margin far above the FP32 rounding of the voxel's camera depth, no voxel of the brick
+ * updates: the cull changes which voxels are visited, never a result.  Bricks with a corner at
+ * z <= 0.02 or a footprint wider than 32 x 32 tiles are kept. */
+__device__ __forceinline__ bool brick_behind_depths(const L3dTsdfGrid& g, const L3dTsdfView& v,
+                                                    const int32_t* __restrict__ coords,
+                                                    const float* __restrict__ tiles, long long b) {
+    int bx, by, bz;
+    if (g.dense) {
+        bx = (int)(b % g.nb[0]);
+        by = (int)((b / g.nb[0]) % g.nb[1]);
+        bz = (int)(b / ((long long)g.nb[0] * g.nb[1]));
+    } else {
+        bx = coords[b * 4];
+        by = coords[b * 4 + 1];
+        bz = coords[b * 4 + 2];
+    }
+    const double lo[3] = {g.origin_d[0] + (bx * 8 + 0.5) * g.voxel_d, g.origin_d[1] + (by * 8 + 0.5) * g.voxel_d,
+                          g.origin_d[2] + (bz * 8 + 0.5) * g.voxel_d};
+    const double span = 7.0 * g.voxel_d;
+    double zmin = 1e300, umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+    for (int c = 0; c < 8; c++) {
+        const double x = lo[0] + ((c & 1) ? span : 0.0);
+        const double y = lo[1] + ((c & 2) ? span : 0.0);
+        const double z = lo[2] + ((c & 4) ? span : 0.0);
+        const double* R = v.Rd;
+        const double p0 = R[0] * x + R[1] * y + R[2] * z + v.td[0];
+        const double p1 = R[3] * x + R[4] * y + R[5] * z + v.td[1];
+        const double p2 = R[6] * x + R[7] * y + R[8] * z + v.td[2];
+        if (!(p2 > 0.02)) return false;
+        const double u = v.kd[0] * p0 / p2 + v.kd[2], w = v.kd[1] * p1 / p2 + v.kd[3];
+        zmin = fmin(zmin, p2);
+        umin = fmin(umin, u);
+        umax = fmax(umax, u);
+        vmin = fmin(vmin, w);
+        vmax = fmax(vmax, w);
+    }
+    const double x0 = fmax(floor(umin) - 1.0, 0.0), x1 = fmin(ceil(umax) + 1.0, (double)(v.W - 1));
+    const double y0 = fmax(floor(vmin) - 1.0, 0.0), y1 = fmin(ceil(vmax) + 1.0, (double)(v.H - 1));
+    const double mu = fmax((double)g.mu, g.trunc_d) + 2e-4;
+    if (x1 < x0 || y1 < y0) return true;  /* no voxel projects into the image */
+    const int tx0 = (int)x0 / L3D_DEPTH_TILE, tx1 = (int)x1 / L3D_DEPTH_TILE;
+    const int ty0 = (int)y0 / L3D_DEPTH_TILE, ty1 = (int)y1 / L3D_DEPTH_TILE;
+    if (tx1 - tx0 >= 32 || ty1 - ty0 >= 32) return false;
+    const int tw = (v.W + L3D_DEPTH_TILE - 1) / L3D_DEPTH_TILE;
+    const float* vt = tiles + v.tile_off;
+    float dmax = 0.0f;
+    for (int ty = ty0; ty <= ty1; ty++)
+        for (int tx = tx0; tx <= tx1; tx++) dmax = fmaxf(dmax, __ldg(vt + (long long)ty * tw + tx));
+    return zmin - (double)dmax > mu;
+}
+
+/* Depth tile t of view v (see l3d_launch_depth_tiles). */
+__device__ __forceinline__ void depth_tile(const L3dTsdfView& v, const uint32_t* __restrict__ depth,
+                                           const float* __restrict__ prior, float* __restrict__ tiles,
+                                           long long t) {
+    const int tw = (v.W + L3D_DEPTH_TILE - 1) / L3D_DEPTH_TILE, th = (v.H + L3D_DEPTH_TILE - 1) / L3D_DEPTH_TILE;
+    if (t >= (long long)tw * th) return;
+    const int tx = (int)(t % tw), ty = (int)(t / tw);
+    float m = 0.0f;
+    for (int y = ty * L3D_DEPTH_TILE; y < min(v.H, (ty + 1) * L3D_DEPTH_TILE); y++)
+        for (int x = tx * L3D_DEPTH_TILE; x < min(v.W, (tx + 1) * L3D_DEPTH_TILE); x++) {
+            const long long i = (long long)y * v.W + x;
+            float d = __half2float(__ushort_as_half((unsigned short)(__ldg(depth + i) & 0xffffu)));
+            if (!(d > 0.0f)) d = prior ? __ldg(prior + i) : 0.0f;
+            if (d > m) m = d;  /* NaN never raises the maximum: such a pixel never updates */
+        }
+    tiles[v.tile_off + t] = m;
+}
+
+__global__ void k_depth_tiles(const L3dTsdfView* __restrict__ views, int n_views,
+                              const uint32_t* const* __restrict__ depths, const float* __restrict__ priors,
+                              float* __restrict__ tiles, long long max_tiles) {
+    const int vi = blockIdx.y;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= max_tiles) return;
+    const L3dTsdfView& v = views[vi];
+    depth_tile(v, depths[vi], v.has_prior ? priors + v.prior_off : nullptr, tiles, t);
+}
+
+__global__ void k_depth_tiles_one(const L3dTsdfView v, const uint32_t* __restrict__ depth,
+                                  const float* __restrict__ prior, float* __restrict__ tiles) {
+    depth_tile(v, depth, v.has_prior ? prior : nullptr, tiles, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__global__ void k_visible_depth(const L3dTsdfGrid g, const L3dTsdfView* __restrict__ views, int n_views,
+                                const int32_t* __restrict__ coords, const float* __restrict__ tiles,
+                                uint8_t* __restrict__ mask) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.bricks * n_views) return;
+    int vi = (int)(t / g.bricks);
+    long long b = t - (long long)vi * g.bricks;
+    uint8_t m = brick_visible(g, views[vi], coords, b);
+    if (m && tiles && brick_behind_depths(g, views[vi], coords, tiles, b)) m = 0;
+    mask[t] = m;
+}
+
+__global__ void k_visible_one_depth(const L3dTsdfGrid g, const L3dTsdfView v,
+                                    const int32_t* __restrict__ coords, const float* __restrict__ tiles,
+                                    uint8_t* __restrict__ mask) {
+    long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= g.bricks) return;
+    uint8_t m = brick_visible(g, v, coords, b);
+    if (m && brick_behind_depths(g, v, coords, tiles, b)) m = 0;
+    mask[b] = m;
+}
+
 __global__ void k_visible_one(const L3dTsdfGrid g, const L3dTsdfView v,
                               const int32_t* __restrict__ coords, uint8_t* __restrict__ mask) {
     long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -248,12 +368,16 @@ __global__ void k_visible_one(const L3dTsdfGrid g, const L3dTsdfView v,
     mask[b] = brick_visible(g, v, coords, b);
 }
 
-template <int VEC, bool Q8>
+/* One view per launch.  LUT: the normal of a depth sample comes from the 4096-entry normal
+ * table and a quad's four depth loads are issued together (lut_pixel / lut_observe, the sweep's
+ * path, equal to observe() bit for bit); otherwise observe() decodes each normal. */
+template <int VEC, bool Q8, bool LUT>
 __global__ void __launch_bounds__(256) k_integrate(const L3dTsdfGrid g, const L3dTsdfView v,
                                                    const int32_t* __restrict__ coords,
                                                    const uint8_t* __restrict__ mask,
                                                    const uint32_t* __restrict__ depth,
                                                    const float* __restrict__ prior,
+                                                   const float4* __restrict__ normals,
                                                    float* __restrict__ tsdf, void* __restrict__ weight,
                                                    long long quads) {
     long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -265,10 +389,29 @@ __global__ void __launch_bounds__(256) k_integrate(const L3dTsdfGrid g, const L3
     float obs[VEC], w[VEC];
     bool ok[VEC];
     bool any = false;
+    if (LUT) {
+        const float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
+        const float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
+        const float* pr = v.has_prior ? prior : nullptr;
+        float3 cam[VEC];
+        int pix[VEC];
+        uint32_t packed[VEC];
 #pragma unroll
-    for (int j = 0; j < VEC; j++) {
-        ok[j] = observe(g, v, depth, v.has_prior ? prior : nullptr, gx + j, gy, gz, &obs[j], &w[j]);
-        any |= ok[j];
+        for (int j = 0; j < VEC; j++)
+            ok[j] = lut_pixel(v, fmaf((float)(gx + j) + 0.5f, g.voxel, g.origin[0]), wy, wz, &cam[j], &pix[j]);
+#pragma unroll
+        for (int j = 0; j < VEC; j++) packed[j] = ok[j] ? __ldg(depth + pix[j]) : 0u;
+#pragma unroll
+        for (int j = 0; j < VEC; j++) {
+            ok[j] = ok[j] && lut_observe(g, v, pr, normals, cam[j], pix[j], packed[j], &obs[j], &w[j]);
+            any |= ok[j];
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < VEC; j++) {
+            ok[j] = observe(g, v, depth, v.has_prior ? prior : nullptr, gx + j, gy, gz, &obs[j], &w[j]);
+            any |= ok[j];
+        }
     }
     if (!any) return;
     if (VEC == 4) {
@@ -383,6 +526,52 @@ __global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
         tsdf[idx] = t[0];
         if (Q8) ((uint16_t*)weight)[idx] = (uint16_t)wq[0];
         else ((float*)weight)[idx] = wf[0];
+    }
+}
+
+/* The work of a many-view integration without its writes: per voxel, the views whose brick
+ * culling keeps it (visible) and the views that update it (lut_observe true), summed over the
+ * volume into counts[0] (visible voxel-views) and counts[1] (voxel-updates). */
+template <int VEC>
+__global__ void __launch_bounds__(256) k_count_updates(const L3dTsdfGrid g,
+                                                       const L3dTsdfView* __restrict__ views,
+                                                       int n_views, const int32_t* __restrict__ coords,
+                                                       const uint8_t* __restrict__ mask,
+                                                       const uint32_t* const* __restrict__ depths,
+                                                       const float* __restrict__ priors,
+                                                       const float4* __restrict__ normals,
+                                                       long long quads,
+                                                       unsigned long long* __restrict__ counts) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long vis = 0, upd = 0;
+    int gx, gy, gz;
+    long long idx, brick;
+    if (q < quads && quad_coords<VEC>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) {
+        const float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
+        const float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
+        for (int vi = 0; vi < n_views; vi++) {
+            if (!mask[(long long)vi * g.bricks + brick]) continue;
+            vis += VEC;
+            const L3dTsdfView& v = views[vi];
+            const float* prior = v.has_prior ? priors + v.prior_off : nullptr;
+#pragma unroll
+            for (int j = 0; j < VEC; j++) {
+                float3 cam;
+                int pix;
+                float obs, w;
+                if (lut_pixel(v, fmaf((float)(gx + j) + 0.5f, g.voxel, g.origin[0]), wy, wz, &cam, &pix) &&
+                    lut_observe(g, v, prior, normals, cam, pix, __ldg(depths[vi] + pix), &obs, &w))
+                    upd++;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        vis += __shfl_down_sync(0xffffffffu, vis, o);
+        upd += __shfl_down_sync(0xffffffffu, upd, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (vis || upd)) {
+        atomicAdd(counts, vis);
+        atomicAdd(counts + 1, upd);
     }
 }
 
@@ -566,22 +755,82 @@ cudaError_t l3d_launch_tsdf_visible(const L3dTsdfGrid& g, const L3dTsdfView* vie
     return cudaGetLastError();
 }
 
+long long l3d_depth_tile_count(int W, int H) {
+    return (long long)((W + L3D_DEPTH_TILE - 1) / L3D_DEPTH_TILE) * ((H + L3D_DEPTH_TILE - 1) / L3D_DEPTH_TILE);
+}
+
+cudaError_t l3d_launch_depth_tiles(const L3dTsdfView* views_dev, int n_views,
+                                   const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                   float* tiles, long long max_tiles, cudaStream_t stream) {
+    if (n_views <= 0 || max_tiles <= 0) return cudaSuccess;
+    dim3 grid((unsigned)((max_tiles + 127) / 128), (unsigned)n_views);
+    k_depth_tiles<<<grid, 128, 0, stream>>>(views_dev, n_views, depth_ptrs_dev, priors, tiles, max_tiles);
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_tsdf_visible_depth(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
+                                          const int32_t* coords, const float* tiles, uint8_t* mask,
+                                          cudaStream_t stream) {
+    long long n = g.bricks * n_views;
+    if (n == 0) return cudaSuccess;
+    k_visible_depth<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(g, views_dev, n_views, coords, tiles, mask);
+    return cudaGetLastError();
+}
+
 cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,
                                  uint8_t* mask, const uint32_t* depth, const float* prior,
-                                 float* tsdf, void* weight, int q8, cudaStream_t stream) {
+                                 const float4* normals, float* tiles, float* tsdf, void* weight, int q8,
+                                 cudaStream_t stream) {
     if (g.bricks == 0) return cudaSuccess;
-    k_visible_one<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, v, coords, mask);
+    if (tiles) {
+        const long long nt = l3d_depth_tile_count(v.W, v.H);
+        L3dTsdfView vt = v;
+        vt.tile_off = 0;
+        k_depth_tiles_one<<<(unsigned)((nt + 127) / 128), 128, 0, stream>>>(vt, depth, prior, tiles);
+        k_visible_one_depth<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, vt, coords, tiles, mask);
+    } else {
+        k_visible_one<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, v, coords, mask);
+    }
     const int vec = vec4_ok(g) ? 4 : 1;
     long long quads = quad_count(g, vec);
     if (quads == 0) return cudaSuccess;
     unsigned blocks = (unsigned)((quads + 255) / 256);
-    if (vec == 4) {
-        if (q8) k_integrate<4, true><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, prior, tsdf, weight, quads);
-        else k_integrate<4, false><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, prior, tsdf, weight, quads);
+#define L3D_INTEGRATE(V, Q, L) \
+    k_integrate<V, Q, L><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, prior, normals, tsdf, weight, quads)
+    if (normals) {
+        if (vec == 4) {
+            if (q8) L3D_INTEGRATE(4, true, true);
+            else L3D_INTEGRATE(4, false, true);
+        } else {
+            if (q8) L3D_INTEGRATE(1, true, true);
+            else L3D_INTEGRATE(1, false, true);
+        }
     } else {
-        if (q8) k_integrate<1, true><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, prior, tsdf, weight, quads);
-        else k_integrate<1, false><<<blocks, 256, 0, stream>>>(g, v, coords, mask, depth, prior, tsdf, weight, quads);
+        if (vec == 4) {
+            if (q8) L3D_INTEGRATE(4, true, false);
+            else L3D_INTEGRATE(4, false, false);
+        } else {
+            if (q8) L3D_INTEGRATE(1, true, false);
+            else L3D_INTEGRATE(1, false, false);
+        }
     }
+#undef L3D_INTEGRATE
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_tsdf_count(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
+                                  const int32_t* coords, const uint8_t* mask,
+                                  const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                  const float4* normals, unsigned long long* counts,
+                                  cudaStream_t stream) {
+    const int vec = vec4_ok(g) ? 4 : 1;
+    long long quads = quad_count(g, vec);
+    if (quads == 0 || n_views == 0) return cudaSuccess;
+    unsigned blocks = (unsigned)((quads + 255) / 256);
+    if (vec == 4)
+        k_count_updates<4><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, quads, counts);
+    else
+        k_count_updates<1><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, quads, counts);
     return cudaGetLastError();
 }
 

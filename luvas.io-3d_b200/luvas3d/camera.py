@@ -30,7 +30,7 @@ class Pose:
 
 @dataclass
 class StereoView:
-    """One posed view (mvs/dense-stereo.ts:57-60)."""
+    """One posed view (mvs/dense-stereo.ts:11-14)."""
 
     intrinsics: Intrinsics
     pose: Pose

@@ -3,7 +3,7 @@
 Scratch buffers, point tables and mesh outputs are stream-ordered allocations from a pool that
 keeps up to 16 GB of freed memory mapped for the next call.  The reference's WebGPU buffers
 return their memory when destroyed (fusion/tsdf-volume.ts:279-290,
-mvs/dense-stereo.ts:357-369); `trim_memory` does that on request for the current device.
+mvs/dense-stereo.ts:357-370); `trim_memory` does that on request for the current device.
 """
 from __future__ import annotations
 

@@ -1,4 +1,4 @@
-"""Host-side decoding of the packed depth format (frontend/src/app/vision/mvs/depth-maps.ts:136-177).
+"""Host-side decoding of the packed depth format (frontend/src/app/vision/mvs/depth-maps.ts:57-85).
 
 A packed sample is a u32: bits 0-15 f16 depth, 16-21 and 22-27 the octahedral normal (6 bits
 each), 28-31 the matching cost quantised to 0-15 (mvs/depth-packing.wgsl.ts:21-33).  Zero means
@@ -10,7 +10,7 @@ import numpy as np
 
 
 def half_to_float(bits) -> np.ndarray:
-    """halfToFloat (depth-maps.ts:149-152): IEEE half bits -> float32 (vectorised)."""
+    """halfToFloat (depth-maps.ts:57-60): IEEE half bits -> float32 (vectorised)."""
     return np.asarray(bits, dtype=np.uint32).astype(np.uint16).view(np.float16).astype(np.float32)
 
 
@@ -23,7 +23,7 @@ def unpack_cost(packed) -> np.ndarray:
 
 
 def unpack_samples(packed) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
-    """unpackDepthSample (depth-maps.ts:158-177) over an array, in float64.
+    """unpackDepthSample (depth-maps.ts:66-85) over an array, in float64.
 
     Returns (valid, depth, normal[..., 3]); invalid entries have depth 0 and normal 0.
     """

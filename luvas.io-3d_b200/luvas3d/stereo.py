@@ -21,7 +21,7 @@ MAX_SOURCES = _lib.MAX_SOURCES
 
 @dataclass
 class SolveOptions:
-    """SolveOptions (dense-stereo.ts:62-75)."""
+    """SolveOptions (dense-stereo.ts:16-29)."""
 
     sources: Sequence[int]
     min_depth: float
@@ -35,7 +35,7 @@ class SolveOptions:
 
 @dataclass
 class StereoOptions:
-    """StereoOptions (dense-stereo.ts:84-88) plus the device layout choices of this library."""
+    """StereoOptions (dense-stereo.ts:38-42) plus the device layout choices of this library."""
 
     coarse: "DenseStereo | None" = None
     depth_maps: bool = True
@@ -76,7 +76,7 @@ class _SolveArgs:
 
 
 class DenseStereo:
-    """GPU PatchMatch for every keyframe (DenseStereo, dense-stereo.ts:107-416).
+    """GPU PatchMatch for every keyframe (DenseStereo, dense-stereo.ts:61-370).
 
     All views' images live in one device array and all packed depth maps (u32 per pixel) in one
     device buffer, so the geometric pass and the consistency filter can read any neighbour.
@@ -133,7 +133,7 @@ class DenseStereo:
         return self._handle
 
     def set_image(self, layer: int, gray: np.ndarray) -> None:
-        """setImage (dense-stereo.ts:221-228); u8 (r8unorm), float32, float16 or bfloat16 bits."""
+        """setImage (dense-stereo.ts:175-182); u8 (r8unorm), float32, float16 or bfloat16 bits."""
         a = np.ascontiguousarray(gray)
         h, w = self.shape(layer)
         if a.shape[-2:] != (h, w) and a.size != h * w:
@@ -150,7 +150,7 @@ class DenseStereo:
                                                   C.c_void_p(data_ptr), int(row_stride)))
 
     def solve(self, ref: int, options: SolveOptions) -> None:
-        """solve (dense-stereo.ts:231-285): init, red/black iterations, pack."""
+        """solve (dense-stereo.ts:185-239): init, red/black iterations, pack."""
         h, w = self.shape(ref)
         args = _SolveArgs(options, h * w)
         _lib.check(self._lib.l3d_stereo_solve(self._h(), int(ref), C.byref(args.c)))
@@ -179,7 +179,7 @@ class DenseStereo:
 
     @property
     def hypotheses(self) -> np.ndarray:
-        """The current per-pixel planes (dense-stereo.ts:288-290), read back: (H, W, 4)."""
+        """The current per-pixel planes (dense-stereo.ts:242-244), read back: (H, W, 4)."""
         hyp = np.empty(self.shape(self._hyp_ref) + (4,), dtype=np.float32)
         _lib.check(self._lib.l3d_stereo_read_hyp(self._h(), _lib.ptr(hyp), None))
         return hyp
@@ -211,7 +211,7 @@ class DenseStereo:
         self.synchronize()
 
     def filter(self, ref: int, sources: Sequence[int], needed: int) -> None:
-        """filter (dense-stereo.ts:296-309): consistency check of depths[ref] into `filtered`."""
+        """filter (dense-stereo.ts:250-263): consistency check of depths[ref] into `filtered`."""
         src = (C.c_int32 * max(1, len(sources)))(*[int(s) for s in sources])
         _lib.check(self._lib.l3d_stereo_filter(self._h(), int(ref), src, len(sources), int(needed)))
         self._filtered_ref = int(ref)
@@ -231,7 +231,7 @@ class DenseStereo:
             table.ctypes.data_as(C.POINTER(C.c_int32)), nd.ctypes.data_as(C.POINTER(C.c_int32))))
 
     def filtered_map(self, ref: int, sources: Sequence[int], needed: int) -> np.ndarray:
-        """filteredMap (dense-stereo.ts:347-352): filter, then read back (H, W) u32."""
+        """filteredMap (dense-stereo.ts:301-306): filter, then read back (H, W) u32."""
         self.filter(ref, sources, needed)
         return self.read_filtered()
 
@@ -246,7 +246,7 @@ class DenseStereo:
         return out
 
     def depth_map(self, ref: int) -> np.ndarray:
-        """depthMap (dense-stereo.ts:355-358): raw packed map of one view, (H, W) u32."""
+        """depthMap (dense-stereo.ts:309-312): raw packed map of one view, (H, W) u32."""
         out = np.empty(self.shape(ref), dtype=np.uint32)
         _lib.check(self._lib.l3d_stereo_read_depth(self._h(), int(ref), _lib.ptr(out)))
         return out
@@ -305,7 +305,7 @@ class DenseStereo:
         _lib.check(self._lib.l3d_stereo_synchronize(self._h()))
 
     def destroy(self) -> None:
-        """destroy (dense-stereo.ts:403-416)."""
+        """destroy (dense-stereo.ts:357-370)."""
         if self._handle is not None:
             self._lib.l3d_stereo_destroy(self._handle)
             self._handle = None

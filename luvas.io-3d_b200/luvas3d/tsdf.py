@@ -110,10 +110,10 @@ def _c_view(v: IntegrationView, keep: list):
 
 
 class TsdfVolume:
-    """Truncated signed distance volume on the GPU (TsdfVolume, tsdf-volume.ts:362-496).
+    """Truncated signed distance volume on the GPU (TsdfVolume, tsdf-volume.ts:157-291).
 
     dense=(X, Y, Z) builds a dense grid; otherwise `grid` and `layout` (BrickGrid.build()) give the
-    reference's brick pool.  truncation defaults to 4 voxels (tsdf-volume.ts:384).
+    reference's brick pool.  truncation defaults to 4 voxels (tsdf-volume.ts:179).
     """
 
     def __init__(self, width: int, height: int, voxel: float, origin, *, dense=None,
@@ -166,7 +166,7 @@ class TsdfVolume:
         return int(self._lib.l3d_tsdf_voxels(self._h()))
 
     def integrate(self, view: IntegrationView, depth=None, stereo=None) -> None:
-        """integrate (tsdf-volume.ts:445-473): one packed map, from a host array `depth` (H, W)
+        """integrate (tsdf-volume.ts:240-268): one packed map, from a host array `depth` (H, W)
         u32 or from `stereo`'s filtered map."""
         keep: list = []
         cv = _c_view(view, keep)
@@ -178,6 +178,32 @@ class TsdfVolume:
             keep.append(p)
         if keep:
             self.synchronize()
+
+    def integrate_layer(self, view: IntegrationView, stereo, layer: int) -> None:
+        """integrate (tsdf-volume.ts:240-268) of `stereo`'s filter_all map of `layer`: one view
+        per launch, the reference's form."""
+        keep: list = []
+        cv = _c_view(view, keep)
+        _lib.check(self._lib.l3d_tsdf_integrate_layer(self._h(), stereo._h(), int(layer), C.byref(cv)))
+        if keep:
+            self.synchronize()
+
+    def count_updates(self, views: Sequence[IntegrationView], depths=None, stereo=None,
+                      layers: Sequence[int] | None = None) -> tuple[int, int]:
+        """(visible voxel-views, voxel-updates) that integrating these maps would apply."""
+        keep: list = []
+        arr = (_lib.IntegrationView * len(views))(*[_c_view(v, keep) for v in views])
+        vis, upd = C.c_int64(), C.c_int64()
+        if stereo is not None:
+            lay = np.asarray(layers if layers is not None else range(len(views)), dtype=np.int32)
+            _lib.check(self._lib.l3d_tsdf_count_updates(
+                self._h(), stereo._h(), lay.ctypes.data_as(C.POINTER(C.c_int32)), None,
+                len(views), arr, C.byref(vis), C.byref(upd)))
+        else:
+            p = np.ascontiguousarray(depths, dtype=np.uint32)
+            _lib.check(self._lib.l3d_tsdf_count_updates(self._h(), None, None, _lib.ptr(p), len(views),
+                                                        arr, C.byref(vis), C.byref(upd)))
+        return int(vis.value), int(upd.value)
 
     def integrate_many(self, views: Sequence[IntegrationView], depths=None, stereo=None,
                        layers: Sequence[int] | None = None) -> None:
@@ -231,7 +257,7 @@ class TsdfVolume:
         return tsdf, weight
 
     def read(self) -> tuple[np.ndarray, np.ndarray]:
-        """read (tsdf-volume.ts:475-482): (tsdf f32, weight f32 or uint16 Q8.8)."""
+        """read (tsdf-volume.ts:270-277): (tsdf f32, weight f32 or uint16 Q8.8)."""
         n = self.voxels
         tsdf = np.empty(n, dtype=np.float32)
         weight = np.empty(n, dtype=np.uint16 if self.weight_q8 else np.float32)

@@ -16,7 +16,7 @@
  *   (d, a, b) with n = (sin a cos b, sin b, -cos a cos b); per view an se(3) increment (v, w)
  *   with R = Exp(w) R0, t = Exp(w) t0 + v.
  *
- *   TSDF integration (frontend/src/app/vision/fusion/tsdf-volume.ts:316-358) with the depth of
+ *   TSDF integration (frontend/src/app/vision/fusion/tsdf-volume.ts:111-153) with the depth of
  *   valid pixels taken from a continuous map, differentiated with respect to that depth and the
  *   volume state before the update.
  */

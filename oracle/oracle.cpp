@@ -16,9 +16,9 @@
  * Sources restated (paths inside the reference project):
  *   frontend/src/app/vision/mvs/patchmatch.wgsl.ts:38-469      kernels and helpers
  *   frontend/src/app/vision/mvs/depth-packing.wgsl.ts:3-33     packed depth format
- *   frontend/src/app/vision/mvs/dense-stereo.ts:231-285,360-401 schedule, uniforms, seeds
+ *   frontend/src/app/vision/mvs/dense-stereo.ts:185-239,314-355 schedule, uniforms, seeds
  *   frontend/src/app/vision/geometry/camera.ts:28-36,73-77      scaleIntrinsics, relativePose
- *   frontend/src/app/vision/fusion/tsdf-volume.ts:308-359,425-473 TSDF integrate and culling
+ *   frontend/src/app/vision/fusion/tsdf-volume.ts:103-154,220-268 TSDF integrate and culling
  *
  * Arithmetic contract (where WGSL leaves the order free, this file fixes it and the CUDA
  * kernels follow it):
@@ -51,7 +51,7 @@
 
 namespace {
 
-constexpr int MAX_SOURCES = 8;     /* dense-stereo.ts:90 */
+constexpr int MAX_SOURCES = 8;     /* dense-stereo.ts:44 */
 constexpr int MAX_WINDOW = 121;    /* 11 x 11 samples */
 constexpr uint32_t FILTER_COST = 7u;
 
@@ -126,7 +126,7 @@ template <typename T> struct Src {
     size_t off;                 /* offset of the source's image and depth map */
 };
 
-/* Params of patchmatch.wgsl.ts:12-26 as built by DenseStereo.params (dense-stereo.ts:360-401). */
+/* Params of patchmatch.wgsl.ts:12-26 as built by DenseStereo.params (dense-stereo.ts:314-355). */
 template <typename T> struct Params {
     T k[4];
     T kinv[4];                  /* 1/fx, 1/fy, -cx/fx, -cy/fy in T */
@@ -736,7 +736,7 @@ int kernel_impl(const orc_stereo_args* a, int kernel, int iteration, int phase, 
     double step = std::pow(0.5, iteration);
     Params<T> p;
     if (kernel == ORC_CONSISTENCY) {
-        /* DenseStereo.filter (dense-stereo.ts:296-309): range 0.01-100 m, no flags */
+        /* DenseStereo.filter (dense-stereo.ts:250-263): range 0.01-100 m, no flags */
         p = build_params<T>(a, 0, 0, 0.0, 0, a->needed, 0.01, 100.0);
     } else if (kernel == ORC_PACK) {
         p = build_params<T>(a, 0, 0, 0.0, flags, 0, a->min_depth, a->max_depth);
@@ -750,7 +750,7 @@ int kernel_impl(const orc_stereo_args* a, int kernel, int iteration, int phase, 
 template <typename T>
 int solve_impl(const orc_stereo_args* a, T* hyp, T* cost, uint32_t* depths) {
     if (!valid_args(a)) return 1;
-    if (a->n_sources == 0) return 0;   /* dense-stereo.ts:233 */
+    if (a->n_sources == 0) return 0;   /* dense-stereo.ts:187 */
     int start = (a->from_coarse && a->coarse_hyp) ? ORC_INIT_COARSE : ORC_INIT;
     kernel_impl<T>(a, start, 0, 0, hyp, cost, depths, nullptr);
     for (int it = 0; it < a->iterations; it++)
@@ -788,7 +788,7 @@ int plane_cost_impl(const orc_stereo_args* a, const T* planes, T* cost, T* view_
 
 /* ---------------------------------------------------------------- TSDF -------------------- */
 
-/* visibleBricks (tsdf-volume.ts:425-439) in FP64 with the reference's operation order. */
+/* visibleBricks (tsdf-volume.ts:220-234) in FP64 with the reference's operation order. */
 bool brick_visible(const orc_tsdf_desc* d, const orc_tsdf_view* v, int bx, int by, int bz) {
     double side = d->voxel * 8.0;
     double c[3] = {d->origin[0] + (bx + 0.5) * side, d->origin[1] + (by + 0.5) * side,
@@ -813,7 +813,7 @@ inline void brick_count(const orc_tsdf_desc* d, int* nb) {
     nb[2] = (d->dims[2] + 7) / 8;
 }
 
-/* Per-voxel body of integrate (tsdf-volume.ts:316-358). */
+/* Per-voxel body of integrate (tsdf-volume.ts:111-153). */
 template <typename T, bool Q8>
 inline void integrate_voxel(const orc_tsdf_desc* dsc, const T* tf, const T* kk, int W, int H,
                             const uint32_t* depth, const float* prior, int gx, int gy, int gz,
@@ -879,7 +879,7 @@ int tsdf_impl(const orc_tsdf_desc* d, const orc_tsdf_view* v, const uint32_t* de
               void* weight, int threads) {
     if (!d || !v || !depth || !tsdf || !weight || d->width <= 0 || d->height <= 0) return 1;
     if (d->weight_q8 && sizeof(T) != sizeof(float)) return 1;
-    /* Uniform block of TsdfVolume.integrate (tsdf-volume.ts:449-458), rounded to T. */
+    /* Uniform block of TsdfVolume.integrate (tsdf-volume.ts:244-253), rounded to T. */
     T tf[20];
     for (int i = 0; i < 3; i++) tf[i] = (T)d->origin[i];
     tf[3] = (T)d->voxel;

@@ -49,7 +49,7 @@ typedef struct {
                                   the product's compensated mode); 0: the reference's plain sums */
 } orc_stereo_args;
 
-/* Full schedule of DenseStereo.solve (dense-stereo.ts:231-285) for one reference view. */
+/* Full schedule of DenseStereo.solve (dense-stereo.ts:185-239) for one reference view. */
 int orc32_solve(const orc_stereo_args* a, float* hyp, float* cost, uint32_t* depths);
 int orc64_solve(const orc_stereo_args* a, double* hyp, double* cost, uint32_t* depths);
 
@@ -66,7 +66,7 @@ int orc32_plane_cost(const orc_stereo_args* a, const float* planes, float* cost,
 int orc64_plane_cost(const orc_stereo_args* a, const double* planes, double* cost,
                      double* view_costs);
 
-/* TSDF integration of one packed depth map (tsdf-volume.ts:308-359 and 425-473). */
+/* TSDF integration of one packed depth map (tsdf-volume.ts:103-154 and 425-473). */
 typedef struct {
     double origin[3];
     double voxel;
@@ -94,7 +94,7 @@ int orc32_tsdf_integrate(const orc_tsdf_desc* d, const orc_tsdf_view* v, const u
                          float* tsdf, void* weight, int32_t threads);
 int orc64_tsdf_integrate(const orc_tsdf_desc* d, const orc_tsdf_view* v, const uint32_t* depth,
                          double* tsdf, double* weight, int32_t threads);
-/* Brick visibility of tsdf-volume.ts:425-439 (FP64); out: count (or dense brick count) bytes. */
+/* Brick visibility of tsdf-volume.ts:220-234 (FP64); out: count (or dense brick count) bytes. */
 int orc_tsdf_visible(const orc_tsdf_desc* d, const orc_tsdf_view* v, uint8_t* out);
 
 /* ---- gradients (grad.cpp): forward-mode dual numbers over FP64 restatements ---- */

@@ -4,14 +4,16 @@
 The oracle cannot solve this size in test time, so these check relations that hold at any size:
 the fast form's depth accuracy against the rendered ground truth equals the plain form's, a
 batched solve equals its views solved one by one, the batched consistency filter equals the
-per-view filter, and the many-view TSDF sweep (with and without the overlapped read-back)
-equals the per-view integrations bit for bit.
+per-view filter, the many-view TSDF sweep (with and without the overlapped read-back) and the
+one-view-per-launch integration of the batched maps equal the per-view integrations bit for bit,
+and the equal-accuracy forms (fast form with FP32 gathers, exact form) keep the plain form's
+accuracy against the ground truth, batched or one by one.
 """
 import numpy as np
 import pytest
 
 from helpers import assert_bit_equal
-from luvas3d import (DTYPE_F16, DTYPE_F32, FORM_FAST, FORM_PLAIN, DenseStereo, IntegrationView,
+from luvas3d import (DTYPE_F16, DTYPE_F32, FORM_EXACT, FORM_FAST, FORM_PLAIN, DenseStereo, IntegrationView,
                      SolveOptions, StereoOptions, TsdfVolume, scenes)
 from luvas3d.packing import unpack_depth
 
@@ -102,9 +104,10 @@ def test_tsdf_sweep_equals_per_view_integration(scan, fast):
         return TsdfVolume(w.width, w.height, w.tsdf_voxel, w.tsdf_origin, dense=w.tsdf_dims,
                           truncation=w.tsdf_truncation, weight_q8=True)
 
-    a, b, c = volume(), volume(), volume()
+    a, b, c, d = volume(), volume(), volume(), volume()
     for i, r in enumerate(refs):
         a.integrate(views[i], depth=fast.read_filtered_layer(r))
+        d.integrate_layer(views[i], fast, r)
     b.integrate_many(views, stereo=fast, layers=refs)
     ta, wa = a.read()
     tb, wb = b.read()
@@ -113,6 +116,32 @@ def test_tsdf_sweep_equals_per_view_integration(scan, fast):
     tc, wc = c.integrate_many_read(views, stereo=fast, layers=refs)
     assert_bit_equal(tc, ta, "tsdf (read-back overlapped)")
     assert_bit_equal(wc, wa, "weight (read-back overlapped)")
+    td, wd = d.read()
+    assert_bit_equal(td, ta, "tsdf (one view per launch from the batched maps)")
+    assert_bit_equal(wd, wa, "weight (one view per launch from the batched maps)")
     assert (wa > 0).mean() > 0.05
-    for v in (a, b, c):
+    for v in (a, b, c, d):
         v.destroy()
+
+
+@pytest.mark.parametrize("form,storage,variant", [(FORM_FAST, DTYPE_F32, 30), (FORM_EXACT, DTYPE_F32, 14)])
+def test_equal_accuracy_forms_at_full_size(scan, form, storage, variant):
+    w, refs, opts = scan
+    s = DenseStereo(w.width, w.height, w.views, StereoOptions(storage=storage, form=form))
+    for i, im in enumerate(w.images):
+        s.set_image(i, im)
+    s.variant = variant
+    s.solve_all(refs, opts)
+    v, m, f = accuracy(s, w, refs)
+    print(f"form {form} variant {variant}: valid {v:.4f} median {m:.5f} within1% {f:.4f}")
+    assert m < 0.006 and v > 0.99
+    one = DenseStereo(w.width, w.height, w.views, StereoOptions(storage=storage, form=form))
+    for i, im in enumerate(w.images):
+        one.set_image(i, im)
+    one.variant = variant
+    for r in (5, 30):
+        one.solve_all([r], [opts[r]])
+        assert_bit_equal(one.read_hypotheses_layer(r)[0], s.read_hypotheses_layer(r)[0],
+                         f"view {r} hypotheses")
+    one.destroy()
+    s.destroy()

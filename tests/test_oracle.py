@@ -33,7 +33,7 @@ def test_pcg_known_values():
 
 
 def test_seed_formula_matches_js():
-    """dense-stereo.ts:379: Math.imul(ref + 1, 0x9e3779b1) + iteration*97 + phase*13 + flags*7 >>> 0."""
+    """dense-stereo.ts:333: Math.imul(ref + 1, 0x9e3779b1) + iteration*97 + phase*13 + flags*7 >>> 0."""
     lib = oracle.load()
 
     def js(ref, it, ph, fl):
@@ -299,7 +299,7 @@ def tsdf_hand(tsdf, w0, obs, w):
 def test_single_voxel_tsdf_update_by_hand():
     """One 8^3 brick at the origin, a camera on the -z side looking along +z; a constant packed
     depth of 1.0 facing the camera.  Voxel (3, 4, 5) is checked against the update written out by
-    hand (tsdf-volume.ts:346-357)."""
+    hand (tsdf-volume.ts:141-152)."""
     W, H = 64, 48
     voxel = 0.01
     origin = (-0.04, -0.04, 0.95)
@@ -392,7 +392,7 @@ def test_brick_layout_contract_pool_equals_dense():
 
 
 def test_visible_bricks_cull_behind_and_beyond():
-    """visibleBricks (tsdf-volume.ts:425-439): a camera at the centre of the grid looking along +z
+    """visibleBricks (tsdf-volume.ts:220-234): a camera at the centre of the grid looking along +z
     sees neither the bricks behind it nor those beyond max_depth."""
     W, H = 96, 72
     o = oracle.Tsdf(W, H, 0.05, (-1.2, -1.2, -1.2), 0.2, dense=(48, 48, 48))

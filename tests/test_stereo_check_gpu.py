@@ -1,6 +1,6 @@
 """The reference's own stereo self-test, restated on this repository's synthetic scene.
 
-frontend/tools/verify/stereo-check.ts:11-77 renders five views 10 degrees apart on a ring around
+frontend/tools/verify/stereo-check.ts:11-74 renders five views 10 degrees apart on a ring around
 its scene (640x360), solves the middle view against the other four (depths 0.1-2 m, 5
 iterations, no prior, photometric pass) and requires more than 60 % of the surface pixels to
 keep a packed depth with a median relative error under 0.4 %.  Its scene needs WebGL; here the

@@ -188,3 +188,51 @@ def test_reset_and_empty_maps(scene):
     g.reset()
     t, w = g.read()
     assert np.all(t == 1.0) and np.all(w == 0)
+
+
+def test_update_count_matches_the_oracle(scene):
+    """l3d_tsdf_count_updates: the voxel-updates of integrating the maps equal, per view, the
+    voxels whose f32 weight the oracle's integration raises (weights stay below the maximum)."""
+    views, maps = scene
+    W, H = 120, 90
+    dims, voxel, origin, mu = (64, 48, 56), 0.04, (-1.28, -1.1, -1.1), 0.12
+    o = oracle.Tsdf(W, H, voxel, origin, mu, dense=dims)
+    want = 0
+    for v, m in zip(views, maps):
+        before = o.weight.copy()
+        o.integrate(view_kw(v), m)
+        want += int((o.weight != before).sum())
+    g = TsdfVolume(W, H, voxel, origin, dense=dims, truncation=mu)
+    visible, updates = g.count_updates([gpu_view(v) for v in views], depths=np.stack(maps))
+    assert updates == want
+    assert want > 5000
+    assert visible >= updates
+    assert visible <= len(views) * int(np.prod(dims))
+    t, w = g.read()  # counting leaves the volume untouched
+    assert np.all(w == 0) and np.all(t == 1)
+
+
+@pytest.mark.parametrize("q8", [False, True])
+def test_sweep_with_prior_and_depth_cull_bit_exact(scene, q8):
+    """The sweep and the per-view launches cull bricks by depth (a brick provably behind every
+    depth of its footprint by more than the truncation band is skipped); with a phone prior
+    filling the holes of one map and a narrow truncation band, both still equal the oracle, which
+    visits every voxel of every visible brick."""
+    views, maps = scene
+    W, H = 120, 90
+    dims, voxel, origin, mu = (64, 48, 56), 0.04, (-1.28, -1.1, -1.1), 0.05
+    prior = np.where(maps[2] == 0, 1.9, 0.0).astype(np.float32)
+    o = oracle.Tsdf(W, H, voxel, origin, mu, dense=dims, weight_q8=q8)
+    a = TsdfVolume(W, H, voxel, origin, dense=dims, truncation=mu, weight_q8=q8)
+    b = TsdfVolume(W, H, voxel, origin, dense=dims, truncation=mu, weight_q8=q8)
+    gv = []
+    for i, (v, m) in enumerate(zip(views, maps)):
+        pr = prior if i == 2 else None
+        o.integrate(view_kw(v, prior=pr), m)
+        a.integrate(gpu_view(v, prior=pr), depth=m)
+        gv.append(gpu_view(v, prior=pr))
+    b.integrate_many(gv, depths=np.stack(maps))
+    for g, what in ((a, "per view"), (b, "sweep")):
+        t, w = g.read()
+        assert_bit_equal(t.reshape(-1), o.tsdf, f"tsdf ({what})")
+        assert_bit_equal(w.reshape(-1), o.weight, f"weight ({what})")
