@@ -18,6 +18,7 @@ tests run the same functions over gloo on the CPU.
 """
 from __future__ import annotations
 
+import contextlib
 from typing import Sequence
 
 import numpy as np
@@ -124,3 +125,114 @@ def pool_to_dense(values: np.ndarray, coords: np.ndarray, dims: Sequence[int],
         x0, y0, z0 = bx * 8, by * 8, bz * 8
         x1, y1, z1 = min(x0 + 8, X), min(y0 + 8, Y), min(z0 + 8, Z)
         out[z0:z1, y0:y1, x0:x1] = v[b, :z1 - z0, :y1 - y0, :x1 - x0]
+
+
+def slab_pool(dims: Sequence[int], rank: int, world: int) -> np.ndarray | None:
+    """The brick-pool coordinates of rank's z-slab, or None when the slab is empty (more ranks
+    than brick rows along z: such a rank integrates nothing)."""
+    z0, z1 = slab_bricks(dims, world)[rank]
+    return slab_layout(dims, z0, z1) if z1 > z0 else None
+
+
+class ScanSplit:
+    """One scan split over the ranks of a process group: the photometric solve of this rank's
+    views (shard_views), one all-gather of every view's packed depth map, the consistency filter
+    of every view on every rank (cheap, and it needs every map), and the TSDF integration of
+    every view into this rank's z-slab of bricks.  Each rank's slab equals the same bricks of a
+    single-GPU volume bit for bit, and every rank's packed and filtered maps equal the single-GPU
+    maps bit for bit (the batched photometric solve of a subset of views equals its views solved
+    alone).
+
+    `backend` does the device work:
+      solve(views)              photometric solve of the given reference views;
+      packed_maps(views)        {view: that view's packed map (H, W) or flat}, 4-byte integers;
+      set_packed_maps(full)     every view's packed map, concatenated in view order (flat);
+      filter_all()              consistency filter of every view;
+      integrate()               TSDF integration of every view into the rank's slab."""
+
+    def __init__(self, backend, sizes: Sequence[tuple[int, int]], rank: int, world: int,
+                 group=None, device=None):
+        self.backend = backend
+        self.sizes = [(int(a), int(b)) for a, b in sizes]
+        self.rank, self.world = int(rank), int(world)
+        self.group, self.device = group, device
+        self.shards = shard_views(self.sizes, self.world)
+        self.views = self.shards[self.rank]
+
+    def solve(self) -> None:
+        if self.views:
+            self.backend.solve(self.views)
+
+    def exchange(self) -> None:
+        ctx = getattr(self.backend, "context", None)
+        with (ctx() if ctx else contextlib.nullcontext()):
+            local = self.backend.packed_maps(self.views)
+            full = gather_packed_maps(local, self.sizes, self.shards, self.rank, self.group,
+                                      self.device)
+            self.backend.set_packed_maps(full)
+
+    def filter(self) -> None:
+        self.backend.filter_all()
+
+    def integrate(self) -> None:
+        self.backend.integrate()
+
+    def step(self) -> None:
+        self.solve()
+        self.exchange()
+        self.filter()
+        self.integrate()
+
+
+class _DeviceArray:
+    """A device buffer seen through the CUDA array interface (zero-copy torch views)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str = "<i4"):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3, "strides": None}
+
+
+def device_view(ptr: int, n: int):
+    """A flat int32 torch tensor over n 4-byte integers of device memory at ptr (no copy)."""
+    import torch
+
+    return torch.as_tensor(_DeviceArray(ptr, n), device="cuda")
+
+
+class DeviceScan:
+    """ScanSplit backend over the library's handles: a DenseStereo holding every view's image
+    and packed map, and (for a rank with a non-empty slab) a brick-pool TsdfVolume of the slab.
+    The exchange (copies and the all-gather) runs on the stereo handle's stream (context())."""
+
+    def __init__(self, stereo, tsdf, options, sources, needed, iviews):
+        import torch
+
+        self.stereo, self.tsdf = stereo, tsdf
+        self.options, self.sources, self.needed, self.iviews = options, sources, needed, iviews
+        self.refs = list(range(len(iviews)))
+        self.stream = torch.cuda.ExternalStream(stereo.stream)
+        sizes = stereo.sizes
+        self.off = _offsets(sizes)
+        self.maps = device_view(stereo.buffers().depths, int(self.off[-1]))
+
+    def solve(self, views):
+        self.stereo.solve_all(views, [self.options[v] for v in views])
+
+    def packed_maps(self, views):
+        return {v: self.maps[int(self.off[v]):int(self.off[v + 1])] for v in views}
+
+    def context(self):
+        """The exchange runs on the stereo handle's stream, ordered after its solves."""
+        import torch
+
+        return torch.cuda.stream(self.stream)
+
+    def set_packed_maps(self, full):
+        self.maps.copy_(full)
+
+    def filter_all(self):
+        self.stereo.filter_all(self.refs, self.sources, self.needed)
+
+    def integrate(self):
+        if self.tsdf is not None:
+            self.tsdf.integrate_many(self.iviews, stereo=self.stereo, layers=self.refs)

@@ -111,3 +111,117 @@ def test_slab_brick_pools_equal_the_dense_volume():
     assert (w_d > 0).sum() > 1000
     np.testing.assert_array_equal(got_t.view(np.uint32), t_d.view(np.uint32))
     np.testing.assert_array_equal(got_w, w_d)
+
+
+class OracleScan:
+    """ScanSplit backend on the CPU: the FP32 oracle stands in for the device kernels (which
+    equal it bit for bit), so the split's host logic runs end to end over gloo ranks."""
+
+    def __init__(self, w, dims, voxel, origin, coords):
+        self.w, self.dims, self.voxel, self.origin, self.coords = w, dims, voxel, origin, coords
+        self.o = oracle.Stereo(w.width, w.height, w.views, w.images, 32, threads=1)
+        self.filtered = {}
+        self.pool = None
+
+    def solve(self, views):
+        for v in views:
+            self.o.solve(v, self.w.sources[v], min_depth=self.w.ranges[v][0],
+                         max_depth=self.w.ranges[v][1], iterations=self.w.iterations)
+
+    def packed_maps(self, views):
+        return {v: self.o.depths[v] for v in views}
+
+    def set_packed_maps(self, full):
+        self.o._depths[:] = full.numpy().view(np.uint32)
+
+    def filter_all(self):
+        self.filtered = {v: self.o.filter(v, self.w.sources[v], self.w.needed[v])
+                         for v in range(len(self.w.views))}
+
+    def integrate(self):
+        if self.coords is None:
+            return
+        self.pool = oracle.Tsdf(self.w.width, self.w.height, self.voxel, self.origin, 4 * self.voxel,
+                                coords=self.coords, weight_q8=True, threads=1)
+        for i, v in enumerate(self.w.views):
+            k = v.intrinsics
+            self.pool.integrate(dict(k=(k.fx, k.fy, k.cx, k.cy), R=v.pose.R, t=v.pose.t,
+                                     max_depth=self.w.ranges[i][1]), self.filtered[i])
+
+
+SPLIT_DIMS, SPLIT_VOXEL, SPLIT_ORIGIN = (48, 40, 20), 0.03, (-0.72, -0.6, 0.3)
+
+
+def _arc_scan():
+    """Five views 5 degrees apart on the sphere scene, 72 x 54, each against the other four."""
+    from types import SimpleNamespace
+
+    views, imgs, truth, srcs = arc_workload(n=5, W=72, H=54, f=63.0, step_deg=5.0, seed=9)
+    return SimpleNamespace(width=72, height=54, views=views, images=imgs, sources=srcs,
+                           ranges=[(0.5, 5.0)] * 5, iterations=3, needed=[2] * 5)
+
+
+def _split_worker(rank, world, port, out_dir):
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        w = _arc_scan()
+        coords = shard.slab_pool(SPLIT_DIMS, rank, world)
+        backend = OracleScan(w, SPLIT_DIMS, SPLIT_VOXEL, SPLIT_ORIGIN, coords)
+        split = shard.ScanSplit(backend, [(w.width, w.height)] * len(w.views), rank, world)
+        split.step()
+        np.save(os.path.join(out_dir, f"w{world}_filtered{rank}.npy"),
+                np.stack([backend.filtered[v] for v in range(len(w.views))]))
+        np.save(os.path.join(out_dir, f"w{world}_views{rank}.npy"), np.array(split.views + [-1]))
+        if coords is not None:
+            t = np.full((SPLIT_DIMS[2], SPLIT_DIMS[1], SPLIT_DIMS[0]), np.nan, dtype=np.float32)
+            wt = np.zeros_like(t, dtype=np.uint16)
+            shard.pool_to_dense(backend.pool.tsdf, coords, SPLIT_DIMS, t)
+            shard.pool_to_dense(backend.pool.weight, coords, SPLIT_DIMS, wt)
+            np.save(os.path.join(out_dir, f"w{world}_tsdf{rank}.npy"), t)
+            np.save(os.path.join(out_dir, f"w{world}_weight{rank}.npy"), wt)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_scan_split_over_two_and_three_gloo_ranks_equals_one_rank():
+    """ScanSplit end to end (solve of each rank's views, the all-gather of packed maps, every
+    view's filter on every rank, the z-slab TSDF), on 1, 2 and 3 gloo ranks: every rank's
+    filtered maps and the slabs put together equal the one-rank result bit for bit.  Three ranks
+    over a grid of three brick rows, and four views of five dealt by pixel count."""
+    import torch.multiprocessing as mp
+
+    with tempfile.TemporaryDirectory() as d:
+        for world in (1, 2, 3):
+            mp.start_processes(_split_worker, args=(world, _free_port(), d), nprocs=world,
+                               join=True, start_method="spawn")
+        want_f = np.load(os.path.join(d, "w1_filtered0.npy"))
+        want_t = np.load(os.path.join(d, "w1_tsdf0.npy"))
+        want_w = np.load(os.path.join(d, "w1_weight0.npy"))
+        assert (want_f != 0).mean() > 0.05 and (want_w > 0).sum() > 100
+        for world in (2, 3):
+            t = np.full_like(want_t, np.nan)
+            wt = np.zeros_like(want_w)
+            views = []
+            for r in range(world):
+                np.testing.assert_array_equal(np.load(os.path.join(d, f"w{world}_filtered{r}.npy")), want_f)
+                views += [v for v in np.load(os.path.join(d, f"w{world}_views{r}.npy")) if v >= 0]
+                p = os.path.join(d, f"w{world}_tsdf{r}.npy")
+                if os.path.exists(p):
+                    rt, rw = np.load(p), np.load(os.path.join(d, f"w{world}_weight{r}.npy"))
+                    m = ~np.isnan(rt)
+                    t[m], wt[m] = rt[m], rw[m]
+            assert sorted(views) == list(range(5))
+            np.testing.assert_array_equal(t.view(np.uint32), want_t.view(np.uint32))
+            np.testing.assert_array_equal(wt, want_w)
+
+
+def test_empty_slab_ranks_integrate_nothing():
+    dims = (16, 16, 16)  # two brick rows along z
+    assert shard.slab_pool(dims, 2, 3) is None
+    assert shard.slab_pool(dims, 0, 3).shape == (4, 4)
+    assert [shard.slab_bricks(dims, 3)[r] for r in range(3)] == [(0, 1), (1, 2), (2, 2)]
