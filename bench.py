@@ -1,6 +1,7 @@
 """Benchmark of the dense-reconstruction path: PatchMatch px-iters/s and TSDF voxel-updates/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form plain|fast]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--form auto|plain|fast|exact] [--workload scan|room|polish|fusion]
 
 Workload (the scan-scale configuration): 48 synthetic views of 640x480 (sphere-on-plane scene,
 3-octave value noise, helical camera path, 2 mm / 0.1 deg pose noise, pixel noise 0.01), 8
@@ -10,13 +11,20 @@ every view; TSDF 512^3 at 4 mm, truncation 2 cm, f32 tsdf + uint16 Q8.8 weights.
 One step = the photometric PatchMatch stage over all 48 views + the consistency filter of all
 views + TSDF integration of all 48 filtered maps.  `value` is the PatchMatch px-iters/s of the
 step (px-iter = one pixel updated in one red/black iteration: 48 * 307200 * 5 per step) timed on
-the PatchMatch stage; the TSDF stage gives voxel-updates/s (134M voxels * 48 views per step).
-Inputs are resident in HBM for `value`; `e2e` repeats the step through the C ABI with the images
-copied from pinned host memory every step and the filtered maps and the TSDF volume read back.
-L2 is flushed (a 256 MB write) before every timed step.
+the PatchMatch stage, in the fast form (FP16 texels) unless --form says otherwise; the plain FP32
+form runs beside it, and the forms at the plain form's FP64 accuracy (the fast form with FP32
+texels read through gathers with exact weights, and the exact form) are timed on the PatchMatch
+stage.  The TSDF stage gives voxel-updates/s (134M voxels * 48 views per step); the reference's
+one-view-per-launch form is timed on the same maps.  Inputs are resident in HBM for `value`;
+`e2e` repeats the step through the C ABI with the images copied from pinned host memory every
+step and the filtered maps and the TSDF volume read back.  L2 is flushed (a 256 MB write) before
+every timed step.  The default run also times the batching configuration (room: 96 views of
+mixed sizes, TSDF 768^3) and the differentiation configuration (polish: the NCC adjoint over 24
+views of 640x480), and the CPU sample of the reference algorithm.
 
-Multi-GPU: the path shards by reference view with no data-path collective in the photometric
-stage; each rank runs an independent replica of the workload ("scaling": "weak").
+Multi-GPU (--gpus N, or N ranks under torch.distributed.run): one scan split over the GPUs, views
+dealt by pixel count, one NCCL all-gather of the packed depth maps per step, TSDF z-slabs per
+GPU ("scaling": "strong": the scan is the same at every N).
 """
 from __future__ import annotations
 
@@ -142,85 +150,127 @@ def scene_conventions(w) -> dict:
                                     "seed = (ref + 1) 0x9e3779b1 + 97 iter + 13 phase + 7 flags"}}
 
 
-def cpu_baseline(w, threads: int, budget_s: float = 20.0) -> dict:
-    """The FP32 oracle on the host cores: one reference view's init + 1 red/black iteration at
-    full resolution with the workload's sources, and one TSDF view integration of the full
-    volume.  px-iters/s and voxel-updates/s of that bounded sample."""
+class CpuSample:
+    """The bounded CPU sample of the workload: the FP32 oracle (the reference algorithm restated
+    in C++) on the host cores, for one reference view (the middle one) at full resolution with
+    its sources.  One sample runs init + iteration 0 (both red/black colours) from scratch and
+    iteration 4 (both colours) from the planes of four iterations, so the rate covers the
+    random planes of the first iteration and the converged planes of the last: 2 x W x H
+    px-iters per sample.  The TSDF sample integrates that view's packed map into the full
+    volume."""
+
+    def __init__(self, w, threads: int):
+        import oracle
+
+        self.w, self.threads = w, threads
+        self.ref = len(w.views) // 2
+        r = self.ref
+        self.kw = dict(min_depth=w.ranges[r][0], max_depth=w.ranges[r][1])
+        self.o = oracle.Stereo(w.width, w.height, w.views, w.images, 32, threads=threads)
+        self.o.solve(r, w.sources[r], iterations=4, **self.kw)
+        self.hyp4, self.cost4 = self.o.hyp.copy(), self.o.cost.copy()
+        self.px = w.images[r].size
+
+    def stereo(self) -> float:
+        """Seconds of one sample (2 x W x H px-iters)."""
+        import oracle
+
+        o, r, src = self.o, self.ref, self.w.sources[self.ref]
+        t0 = time.perf_counter()
+        o.kernel(oracle.INIT, r, src, **self.kw)
+        for phase in (0, 1):
+            o.kernel(oracle.PROPAGATE, r, src, iteration=0, phase=phase, **self.kw)
+        o.hyp, o.cost = self.hyp4, self.cost4
+        for phase in (0, 1):
+            o.kernel(oracle.PROPAGATE, r, src, iteration=4, phase=phase, **self.kw)
+        return time.perf_counter() - t0
+
+    def tsdf(self) -> float:
+        """Seconds of one view integrated into the full volume."""
+        import oracle
+
+        w, r = self.w, self.ref
+        self.o.kernel(oracle.PACK, r, w.sources[r], **self.kw)
+        v = w.views[r]
+        k = v.intrinsics
+        h0, w0 = w.images[r].shape
+        ot = oracle.Tsdf(w0, h0, w.tsdf_voxel, w.tsdf_origin, w.tsdf_truncation,
+                         dense=w.tsdf_dims, weight_q8=True, threads=self.threads)
+        t0 = time.perf_counter()
+        ot.integrate(dict(k=(k.fx, k.fy, k.cx, k.cy), R=v.pose.R, t=v.pose.t,
+                          max_depth=w.ranges[r][1]), self.o.depths[r])
+        return time.perf_counter() - t0
+
+    def describe(self, stereo_s: float, tsdf_s: float) -> str:
+        h0, w0 = self.w.images[self.ref].shape
+        return (f"FP32 oracle, reference view {self.ref} at {w0}x{h0} with "
+                f"{len(self.w.sources[self.ref])} sources: init + iteration 0 from scratch and "
+                f"iteration 4 from four iterations' planes, both colours each ({stereo_s:.2f} s); "
+                f"TSDF 1 view into {self.w.tsdf_dims[0]}^3 ({tsdf_s:.2f} s)")
+
+
+def cpu_baseline(w, threads: int) -> dict:
+    """One CPU sample (CpuSample) on `threads` host threads, and the stereo sample's iteration 0
+    on one thread."""
     import oracle
 
-    o = oracle.Stereo(w.width, w.height, w.views, w.images, 32, threads=threads)
-    h0, w0 = w.images[0].shape
+    smp = CpuSample(w, threads)
+    t_pm = smp.stereo()
+    t_ts = smp.tsdf()
+    one = oracle.Stereo(w.width, w.height, w.views, w.images, 32, threads=1)
+    r = smp.ref
+    one.kernel(oracle.INIT, r, w.sources[r], **smp.kw)
     t0 = time.perf_counter()
-    o.kernel(oracle.INIT, 0, w.sources[0], min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
-    t_init = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    for phase in (0, 1):
-        o.kernel(oracle.PROPAGATE, 0, w.sources[0], iteration=0, phase=phase,
-                 min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
-    t_prop = time.perf_counter() - t0
-    pm = w.images[0].size / t_prop
-    # TSDF: one view into the full volume
-    o.kernel(oracle.PACK, 0, w.sources[0], min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
-    v = w.views[0]
-    k = v.intrinsics
-    ot = oracle.Tsdf(w0, h0, w.tsdf_voxel, w.tsdf_origin, w.tsdf_truncation,
-                     dense=w.tsdf_dims, weight_q8=True, threads=threads)
-    t0 = time.perf_counter()
-    ot.integrate(dict(k=(k.fx, k.fy, k.cx, k.cy), R=v.pose.R, t=v.pose.t,
-                      max_depth=w.ranges[0][1]), o.depths[0])
-    t_tsdf = time.perf_counter() - t0
-    vox = int(np.prod(w.tsdf_dims))
-    # one thread: one colour of the same iteration (half the pixels updated)
-    o1 = oracle.Stereo(w.width, w.height, w.views, w.images, 32, threads=1)
-    o1.kernel(oracle.INIT, 0, w.sources[0], min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
-    t0 = time.perf_counter()
-    o1.kernel(oracle.PROPAGATE, 0, w.sources[0], iteration=0, phase=0,
-              min_depth=w.ranges[0][0], max_depth=w.ranges[0][1])
+    one.kernel(oracle.PROPAGATE, r, w.sources[r], iteration=0, phase=0, **smp.kw)
     t_one = time.perf_counter() - t0
-    return {"value": pm, "unit": "px-iters/s", "cores": threads, "kind": "port",
-            "single_thread_px_iters_per_s": (w.images[0].size / 2) / t_one,
-            "sample": (f"FP32 oracle: 1 reference view x 1 red/black iteration at "
-                       f"{w0}x{h0}, {len(w.sources[0])} sources "
-                       f"({t_prop:.2f} s); TSDF 1 view into {w.tsdf_dims[0]}^3 ({t_tsdf:.2f} s)"),
-            "tsdf_voxel_updates_per_s": vox / t_tsdf, "seconds": t_prop + t_tsdf}
+    vox = int(np.prod(w.tsdf_dims))
+    return {"value": 2 * smp.px / t_pm, "unit": "px-iters/s", "cores": threads, "kind": "port",
+            "single_thread_px_iters_per_s": (smp.px / 2) / t_one,
+            "sample": smp.describe(t_pm, t_ts), "tsdf_voxel_updates_per_s": vox / t_ts}
 
 
 def run_reference(args, rank: int, world: int) -> None:
     """--impl reference: the CPU restatement of the path on the host cores (the reference has no
-    CPU implementation of these stages; its WGSL needs WebGPU, unavailable on this box)."""
+    CPU implementation of these stages; its WGSL needs WebGPU, unavailable on this box).  Each
+    timed step is one bounded sample (CpuSample); ms_per_step is its measured duration."""
     if rank != 0:
         return
     w = build_workload(args)
     threads = os.cpu_count() or 1
-    vals, tv, secs = [], [], []
+    smp = CpuSample(w, threads)
+    secs, tsecs = [], []
     for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        r = cpu_baseline(w, threads)
+        t_pm = smp.stereo()
+        t_ts = smp.tsdf() if i in (0, args.warmup) else None
         if i >= args.warmup:
-            vals.append(r["value"])
-            tv.append(r["tsdf_voxel_updates_per_s"])
-            secs.append(time.perf_counter() - t0)
-    v = statistics.median(vals)
+            secs.append(t_pm)
+            if t_ts is not None:
+                tsecs.append(t_ts)
+    sec = statistics.median(secs)
+    v = 2 * smp.px / sec
+    vox = int(np.prod(w.tsdf_dims))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "px-iters/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * w.pixels * w.iterations / v,
-        "ms_per_step_basis": "one full step of the workload at the sampled rate; each timed step "
-                             "runs the bounded sample only",
-        "sample_seconds_per_step": statistics.median(secs), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name(w), "sample": r["sample"]},
+        "ms_per_step": sec * 1e3,
+        "ms_per_step_basis": "measured: one bounded sample per timed step (median)",
+        "full_step_ms_extrapolated": 1e3 * w.pixels * w.iterations / v,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": workload_name(w), "sample": smp.describe(sec, tsecs[0])},
         "scene": scene_conventions(w),
-        "tsdf_voxel_updates_per_s": statistics.median(tv),
+        "tsdf_voxel_updates_per_s": vox / tsecs[0],
         "cpu_baseline": {"value": v, "unit": "px-iters/s", "cores": threads, "kind": "port",
-                         "sample": r["sample"],
-                         "single_thread_px_iters_per_s": r["single_thread_px_iters_per_s"]},
+                         "sample": smp.describe(sec, tsecs[0])},
         "e2e": {"value": v, "unit": "px-iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 def run_polish(args) -> None:
+    print(json.dumps(polish_measure(args.views or 24, args.steps, args.warmup)), flush=True)
+
+
+def polish_measure(n_views: int, steps: int, warmup: int, geometry: bool = True) -> dict:
     """Differentiation configuration: 24 views of 640x480 of the sphere scene with poses perturbed
     by 5 mm / 0.3 deg.  PatchMatch (fast form) on the perturbed poses gives the starting planes;
     then 20 Adam steps polish every view's planes and pose increment against the summed NCC
@@ -232,7 +282,7 @@ def run_polish(args) -> None:
     from luvas3d import DTYPE_F16, FORM_FAST, DenseStereo, SolveOptions, StereoOptions, scenes
     from luvas3d import grad as G
 
-    w = scenes.polish(n_views=args.views or 24)
+    w = scenes.polish(n_views=n_views)
     V = len(w.views)
     refs = list(range(V))
     opts = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=w.iterations)
@@ -266,11 +316,11 @@ def run_polish(args) -> None:
         for r in refs:
             G.ncc_value_and_grad(st, r, w.sources[r], planes[r], deltas, weights[r], gd)
 
-    for _ in range(max(3, args.warmup)):
+    for _ in range(max(3, warmup)):
         grad_pass()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     times = []
-    for _ in range(max(1, args.steps)):
+    for _ in range(max(1, steps)):
         flush.fill_(1)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
@@ -295,12 +345,14 @@ def run_polish(args) -> None:
     # (1) planes from PatchMatch on the perturbed poses; (2) planes of the true geometry (solved
     # with the true poses, as a depth prior would give), poses still perturbed
     from_pm = run(planes, weights)
-    true_planes, true_weights = starting_planes(w.true_views)
-    from_geometry = run(true_planes, true_weights)
+    from_geometry = None
+    if geometry:
+        true_planes, true_weights = starting_planes(w.true_views)
+        from_geometry = run(true_planes, true_weights)
     line = {
         "metric": "NCC adjoint pixel-sources/s (cost + plane + se(3) pose gradient)",
         "value": units / (grad_ms / 1e3), "unit": "pixel-sources/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": grad_ms,
+        "steps": steps, "warmup": warmup, "ms_per_step": grad_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 images, f32 arithmetic, FP64 pose composition and pose-gradient sums",
         "data": "synthetic (seeded sphere-on-plane scene, value-noise texture)",
@@ -312,8 +364,8 @@ def run_polish(args) -> None:
         "pose_errors": "relative to view 0 (held fixed), mean over the other views: [before, after]",
         "gpu_launches": 3 * V,
     }
-    print(json.dumps(line), flush=True)
     st.destroy()
+    return line
 
 
 def run_fusion(args):
@@ -550,52 +602,148 @@ def run_fusion(args):
         h.destroy()
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="auto", choices=["auto", "plain", "fast"])
-    ap.add_argument("--workload", default="scan", choices=["scan", "room", "polish", "fusion"])
-    ap.add_argument("--views", type=int, default=0)
-    ap.add_argument("--width", type=int, default=640)
-    ap.add_argument("--height", type=int, default=480)
-    ap.add_argument("--tsdf-dim", type=int, default=0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--storage", default="f16", choices=["f16", "u8", "f32", "bf16"],
-                    help="fast-form image storage")
-    ap.add_argument("--variant", type=int, default=-1,
-                    help="fast-form kernel variant; default: the autotuner's choice")
-    args = ap.parse_args()
+def _free_port() -> int:
+    import socket
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        run_reference(args, rank, world)
-        return
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
 
-    import torch
-    import torch.distributed as dist
 
-    torch.cuda.set_device(local)
-    if args.workload == "polish":
-        if rank == 0:
-            run_polish(args)
-        return
-    if args.workload == "fusion":
-        if rank == 0:
-            run_fusion(args)
-        return
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+def relaunch(n: int) -> int:
+    """`--gpus N` without a launcher: one process per GPU under torch.distributed.run."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={_free_port()}", os.path.abspath(__file__),
+           *sys.argv[1:]]
+    return subprocess.run(cmd, timeout=3600).returncode
 
-    from luvas3d import (DTYPE_BF16, DTYPE_F16, DTYPE_F32, DTYPE_U8, FORM_FAST, FORM_PLAIN,
-                         DenseStereo, IntegrationView, SolveOptions, StereoOptions, TsdfVolume)
+
+class Stage:
+    """CUDA events on one stream around the stages of a step."""
+
+    def __init__(self, stream, names):
+        import torch
+
+        self.stream, self.names = stream, list(names)
+        self.ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)]
+        self.i = 0
+
+    def mark(self):
+        import torch
+
+        with torch.cuda.stream(self.stream):
+            self.ev[self.i].record(self.stream)
+        self.i += 1
+
+    def ms(self) -> dict:
+        out = {n: self.ev[k].elapsed_time(self.ev[k + 1]) for k, n in enumerate(self.names)}
+        out["step"] = self.ev[0].elapsed_time(self.ev[-1])
+        return out
+
+
+def make_stereo(w, form, storage, stream, refs, opts, variant=None, gather=False, compensated=False):
+    """A stereo handle with every view's image; for the batched forms the kernel variant is
+    `variant`, or the autotuner's pick over `refs` (with `gather`, among the variants that read
+    the texture through gathers with exact weights), and batched solves replay CUDA graphs."""
+    from luvas3d import FORM_PLAIN, DenseStereo, StereoOptions
+
+    st = DenseStereo(w.width, w.height, w.views,
+                     StereoOptions(storage=storage, form=form, stream=stream, compensated=compensated),
+                     sizes=w.sizes or [(w.width, w.height)] * len(w.views))
+    for i, im in enumerate(w.images):
+        st.set_image(i, im)
+    tuned = {"variant": None, "ms": None}
+    if form != FORM_PLAIN:
+        if variant is not None:
+            st.variant = variant
+            tuned["variant"] = variant
+        else:
+            if gather:
+                st.variant = 30
+            tuned["variant"], tuned["ms"] = st.autotune(refs, opts)
+        st.set_graphs(True)
+    return st, tuned
+
+
+def depth_accuracy(st, w, refs) -> dict:
+    """Packed depth maps of the last solve against the rendered ground truth, scored like the
+    reference's stereo self-test (frontend/tools/verify/stereo-check.ts:56-73): surface pixels
+    (truth > 0) with a non-zero packed entry count as valid; relative error of the packed half
+    depth, median and p90, over the given views."""
     from luvas3d.packing import unpack_depth
+
+    errs, surf, valid = [], 0, 0
+    for r in refs:
+        packed = st.depth_map(r)
+        t = w.truth[r]
+        m = t > 0
+        ok = m & (packed != 0)
+        surf += int(m.sum())
+        valid += int(ok.sum())
+        errs.append(np.abs(unpack_depth(packed[ok]) - t[ok]) / t[ok])
+    e = np.concatenate(errs)
+    return {"valid_fraction": round(valid / max(1, surf), 4),
+            "median_rel_err": float(np.percentile(e, 50)),
+            "p90_rel_err": float(np.percentile(e, 90))}
+
+
+def time_solves(st, refs, opts, stream, flush, steps: int, warmup: int) -> list:
+    """PatchMatch stage alone (solve_all of refs), L2 flushed before each, CUDA events."""
+    import torch
+
+    out = []
+    for i in range(warmup + steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        g = Stage(stream, ["patchmatch"])
+        g.mark()
+        st.solve_all(refs, opts)
+        g.mark()
+        torch.cuda.synchronize()
+        if i >= warmup:
+            out.append(g.ms()["patchmatch"])
+    return out
+
+
+def propagate_launch_ms(st, w, refs, stream, per_view_launches: bool) -> float:
+    """One propagate launch: (solve with all iterations - solve with none) / propagate launches,
+    CUDA events on the handle's stream."""
+    import torch
+
+    from luvas3d import SolveOptions
+
+    per = {}
+    for its in (0, w.iterations):
+        o2 = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=its)
+              for r in refs]
+        g = Stage(stream, ["solve"])
+        g.mark()
+        for _ in range(2):
+            st.solve_all(refs, o2)
+        g.mark()
+        torch.cuda.synchronize()
+        per[its] = g.ms()["solve"] / 2
+    return (per[w.iterations] - per[0]) / (2 * w.iterations * (len(refs) if per_view_launches else 1))
+
+
+def fetch_rate(dtype, mode) -> float:
+    """Measured bilinear samples/s of the texture unit (l3d_measure_fetch_rate, one colour)."""
+    import ctypes as C
+
+    from luvas3d import _lib
+
+    rate = C.c_double()
+    _lib.check(_lib.load().l3d_measure_fetch_rate(dtype, 1, mode, C.byref(rate)))
+    return rate.value
+
+
+def run_scan(args) -> None:
+    """One GPU: the scan (or room) workload through every form, with the rooflines, the end-to-end
+    run through the C ABI, the batching and differentiation configurations and the CPU sample."""
+    import torch
+
+    from luvas3d import (DTYPE_BF16, DTYPE_F16, DTYPE_F32, DTYPE_U8, FETCH_FILTERED, FETCH_GATHER,
+                         FORM_EXACT, FORM_FAST, FORM_PLAIN, IntegrationView, SolveOptions, TsdfVolume)
 
     w = build_workload(args)
     V = len(w.views)
@@ -610,187 +758,159 @@ def main():
     vox = int(np.prod(w.tsdf_dims))
     px_iters_step = w.pixels * w.iterations
     tsdf = TsdfVolume(max(s[0] for s in sizes), max(s[1] for s in sizes), w.tsdf_voxel,
-                      w.tsdf_origin, dense=w.tsdf_dims,
-                      truncation=w.tsdf_truncation, weight_q8=True, stream=sptr)
-    mk = lambda n=4: [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+                      w.tsdf_origin, dense=w.tsdf_dims, truncation=w.tsdf_truncation,
+                      weight_q8=True, stream=sptr)
+    storage = {"f16": DTYPE_F16, "u8": DTYPE_U8, "f32": DTYPE_F32, "bf16": DTYPE_BF16}[args.storage]
+    fixed = args.variant if args.variant >= 0 else None
 
-    def rec(ev):
-        with torch.cuda.stream(stream):
-            ev.record(stream)
-
-    tuned = {}
-
-    def make_stereo(form):
-        storage = {"f16": DTYPE_F16, "u8": DTYPE_U8, "f32": DTYPE_F32, "bf16": DTYPE_BF16}[args.storage] \
-            if form == FORM_FAST else DTYPE_F32
-        st = DenseStereo(w.width, w.height, w.views,
-                         StereoOptions(storage=storage, form=form, stream=sptr), sizes=sizes)
-        for i, im in enumerate(w.images):
-            st.set_image(i, im)
-        if form == FORM_FAST:
-            # kernel variant picked by timing one iteration of this batch, then graph replay
-            if args.variant >= 0:
-                st.variant = args.variant
-                tuned["variant"], tuned["ms"] = args.variant, None
-            else:
-                tuned["variant"], tuned["ms"] = st.autotune(refs, opts)
-            st.set_graphs(True)
-        return st
-
-    def step(st, evs):
+    def step(st, g):
         with torch.cuda.stream(stream):
             flush.fill_(1)
-        rec(evs[0])
+        g.mark()
         st.solve_all(refs, opts)
-        rec(evs[1])
+        g.mark()
         tsdf.reset()  # a fresh volume per scan (tsdf 1, weight 0), outside the timed TSDF stage
         st.filter_all(refs, w.sources, w.needed)
-        rec(evs[2])
+        g.mark()
         tsdf.integrate_many(iviews, stereo=st, layers=refs)
-        rec(evs[3])
+        g.mark()
 
-    def time_form(form, steps, warmup, sample_clocks):
-        st = make_stereo(form)
+    def time_form(form, stor, steps, warmup, sample_clocks, variant):
+        st, tuned = make_stereo(w, form, stor, sptr, refs, opts, variant=variant)
         for _ in range(warmup):
-            step(st, mk())
+            step(st, Stage(stream, ["patchmatch", "filter", "tsdf"]))
         torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
         l0 = st.launches + tsdf.launches
-        clocks = ClockSampler(local) if sample_clocks else None
+        clocks = ClockSampler(torch.cuda.current_device()) if sample_clocks else None
         if clocks:
             clocks.start()
-        all_evs = []
+        gs = []
         for _ in range(steps):
-            evs = mk()
-            step(st, evs)
-            all_evs.append(evs)
+            g = Stage(stream, ["patchmatch", "filter", "tsdf"])
+            step(st, g)
+            gs.append(g)
         torch.cuda.synchronize()
-        launches = st.launches + tsdf.launches - l0
-        if world > 1:
-            dist.barrier()
         clk = clocks.stop() if clocks else None
-        ms = {k: [e[a].elapsed_time(e[b]) for e in all_evs]
-              for k, (a, b) in {"patchmatch": (0, 1), "filter": (1, 2), "tsdf": (2, 3),
-                                "step": (0, 3)}.items()}
-        tot = torch.tensor([sum(ms["patchmatch"]), sum(ms["tsdf"]), sum(ms["step"])],
-                           dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-        pm_s, ts_s, st_s = (float(x) / 1e3 for x in tot.tolist())
-        # propagate launches alone: solve with 5 iterations minus solve with 0 (init + pack)
-        per = {}
-        for its in (0, w.iterations):
-            o2 = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=its)
-                  for r in refs]
-            a, b = mk(2)
-            rec(a)
-            for _ in range(2):
-                st.solve_all(refs, o2)
-            rec(b)
-            torch.cuda.synchronize()
-            per[its] = a.elapsed_time(b) / 2
-        n_prop = 2 * w.iterations * (1 if form == FORM_FAST else V)
-        prop_ms = (per[w.iterations] - per[0]) / n_prop
-        return st, {"pm_s": pm_s, "ts_s": ts_s, "st_s": st_s, "ms": ms, "clk": clk,
-                    "launches": launches, "prop_ms": prop_ms,
-                    "px_iters_per_s": px_iters_step * steps * world / pm_s}
+        ms = [g.ms() for g in gs]
+        stage = {k: sum(m[k] for m in ms) / len(ms) for k in ms[0]}
+        r = {"stage_ms": stage, "clk": clk, "launches": st.launches + tsdf.launches - l0,
+             "px_iters_per_s": px_iters_step / (stage["patchmatch"] / 1e3), "tuned": tuned,
+             "prop_ms": propagate_launch_ms(st, w, refs, stream, form == FORM_PLAIN),
+             "accuracy": depth_accuracy(st, w, refs)}
+        return st, r
 
-    def accuracy(st) -> dict:
-        """Packed depth maps of the last full solve against the rendered ground truth, scored
-        like the reference's stereo self-test (frontend/tools/verify/stereo-check.ts:56-73):
-        surface pixels (truth > 0) with a non-zero packed entry count as valid; relative error of
-        the packed half depth, median and p90, over all views of this rank."""
-        errs, surf, valid = [], 0, 0
-        for r in refs:
-            packed = st.depth_map(r)
-            t = w.truth[r]
-            m = t > 0
-            ok = m & (packed != 0)
-            surf += int(m.sum())
-            valid += int(ok.sum())
-            errs.append(np.abs(unpack_depth(packed[ok]) - t[ok]) / t[ok])
-        e = np.concatenate(errs)
-        return {"valid_fraction": round(valid / max(1, surf), 4),
-                "median_rel_err": float(np.percentile(e, 50)),
-                "p90_rel_err": float(np.percentile(e, 90))}
-
-    plain_steps = max(1, min(args.steps, 2)) if args.form == "auto" else args.steps
+    chosen = {"auto": FORM_FAST, "fast": FORM_FAST, "plain": FORM_PLAIN, "exact": FORM_EXACT}[args.form]
+    chosen_storage = DTYPE_F32 if chosen in (FORM_PLAIN, FORM_EXACT) else storage
     res = {}
-    acc = {}
-    stereo = None
-    forms = {"auto": [FORM_PLAIN, FORM_FAST], "plain": [FORM_PLAIN], "fast": [FORM_FAST]}[args.form]
-    for form in forms:
-        chosen = form == forms[-1]
-        st, r = time_form(form, args.steps if chosen else plain_steps, args.warmup, chosen)
-        res[form] = r
-        acc["fast" if form == FORM_FAST else "plain"] = accuracy(st)
-        if chosen:
-            stereo = st
-        else:
-            st.destroy()
-    chosen_form = forms[-1]
-    R = res[chosen_form]
-    clk = R["clk"]
+    if args.form == "auto":
+        st, res["plain"] = time_form(FORM_PLAIN, DTYPE_F32, max(1, min(args.steps, 2)),
+                                     min(args.warmup, 3), False, None)
+        st.destroy()
+    stereo, R = time_form(chosen, chosen_storage, args.steps, args.warmup, True, fixed)
+    plain = res.get("plain")
     value = R["px_iters_per_s"]
-    voxel_updates = vox * V * args.steps * world
-
-    # ---- roofline of the dominant kernel (red/black propagate) ------------------------------
-    peaks, peak_kind = _peaks()
     S = len(w.sources[0])
+    pix_colour = w.pixels / V / 2
+    views_launch = 1 if chosen == FORM_PLAIN else V
+
+    # ---- rooflines of the propagate kernel ------------------------------------------------
+    peaks, peak_kind = _peaks()
+    samples = 14 * S * 36 * pix_colour * views_launch
     flop_per_px_phase = 14 * S * (18 + 36 * 37 + 15) + 36 * 26
-    views_per_launch = V if chosen_form == FORM_FAST else 1
-    prop_flops = flop_per_px_phase * (w.pixels / V / 2) * views_per_launch
-    achieved = prop_flops / (R["prop_ms"] / 1e3) / 1e12
-    sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+    prop_flops = flop_per_px_phase * pix_colour * views_launch
+    sm_mhz = (R["clk"] or {}).get("sm_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
-    roof_fp32 = {"kernel": (f"k_fast_propagate (all {V} views, one colour)"
-                            if chosen_form == FORM_FAST else "k_propagate (one view, one colour)"),
-                 "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                 "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
-                 "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 flops) at "
-                                "the sampled median SM clock",
+    kname = (f"k_fast_propagate (all {V} views, one colour)" if chosen != FORM_PLAIN
+             else "k_propagate (one view, one colour)")
+    roof_fp32 = {"kernel": kname, "bound": "fp32", "achieved": prop_flops / (R["prop_ms"] / 1e3) / 1e12,
+                 "peak": fp32_peak, "unit": "TFLOP/s", "traffic": None,
+                 "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 flops) at the "
+                                "sampled median SM clock",
                  "launch_ms": R["prop_ms"], "flop_per_launch": prop_flops,
-                 "flop_model": "14 candidates x sources x (18 + 36 x 37 + 15) + 936 per "
-                               "pixel of the colour"}
-    # the fast propagate kernel is bound by the texture data pipe: quote its bilinear samples
-    # against the rate a probe kernel with the same thread layout measures on this GPU
+                 "flop_model": "14 candidates x sources x (18 + 36 x 37 + 15) + 936 per pixel of "
+                               "the colour"}
+    roof_fp32["frac"] = roof_fp32["achieved"] / fp32_peak
+    sample_model = ("14 candidates x sources x 36 bilinear samples per pixel of the colour (the "
+                    "reference's count; sources the corner test rejects are counted although not "
+                    "sampled)")
+
+    def tex_roof(kernel, launch_ms, dtype, mode, name):
+        peak = fetch_rate(dtype, mode) / 1e9
+        got = samples / (launch_ms / 1e3) / 1e9
+        return {"kernel": kernel, "bound": "texture", "achieved": got, "peak": peak,
+                "unit": "Gsample/s", "frac": got / peak, "traffic": None,
+                "peak_source": f"measured: l3d_measure_fetch_rate({name}), bilinear samples/s of a "
+                               "2048x2048 texture, one red/black colour",
+                "launch_ms": launch_ms, "samples_per_launch": samples, "sample_model": sample_model}
+
     roof_tex = None
-    if chosen_form == FORM_FAST and args.storage != "bf16":
-        import ctypes as C
-        from luvas3d import _lib
-        rate = C.c_double()
-        dt = {"f16": DTYPE_F16, "u8": DTYPE_U8, "f32": DTYPE_F32}[args.storage]
-        _lib.check(_lib.load().l3d_measure_texture_rate(dt, 1, C.byref(rate)))
-        samples = 14 * S * 36 * (w.pixels / V / 2) * views_per_launch
-        got = samples / (R["prop_ms"] / 1e3) / 1e9
-        peak_tex = rate.value / 1e9
-        # DRAM traffic of one launch: the ncu capture of the 8-view launch of this kernel (F16
-        # images, variant 14: 54.13 MB read + 1.90 MB written for 8 x 153 600 pixels of one
-        # colour) scaled by the pixels this launch processes; hyp, cost and images all grow
-        # with the views in the launch
-        traffic = None
-        if args.storage == "f16":
-            traffic = (54.13248e6 + 1.896704e6) / (8 * 153600) * (w.pixels / V / 2) * views_per_launch
-        roof_tex = {"kernel": roof_fp32["kernel"], "bound": "texture", "achieved": got,
-                    "peak": peak_tex, "unit": "Gsample/s", "frac": got / peak_tex, "traffic": traffic,
-                    "traffic_unit": "DRAM bytes per launch",
-                    "traffic_source": "profiles/k_fast_propagate_scan8.md (8-view capture, "
-                                      "scaled by the pixels per launch)" if traffic else None,
-                    "peak_source": f"measured: l3d_measure_texture_rate({args.storage}, one "
-                                   "red/black colour), bilinear samples/s of a 2048x2048 texture",
-                    "launch_ms": R["prop_ms"], "samples_per_launch": samples,
-                    "sample_model": "14 candidates x sources x 36 bilinear samples per pixel of "
-                                    "the colour (the reference's count; sources the corner test "
-                                    "rejects are counted although not sampled)"}
-    tsdf_ms = sum(R["ms"]["tsdf"]) / len(R["ms"]["tsdf"])
-    tsdf_bytes = vox * 12
-    tsdf_gbs = tsdf_bytes / (tsdf_ms / 1e3) / 1e9
+    if chosen == FORM_FAST and args.storage != "bf16":
+        roof_tex = tex_roof(kname, R["prop_ms"], chosen_storage, FETCH_FILTERED,
+                            f"{args.storage}, filtered")
+    elif chosen == FORM_EXACT:
+        roof_tex = tex_roof(kname, R["prop_ms"], DTYPE_F32, FETCH_GATHER, "f32, gather")
+
+    # ---- the forms at the plain form's FP64 accuracy: PatchMatch stage alone ---------------
+    equal = {}
+    if args.workload == "scan" and not args.no_extras:
+        for name, form, gather in (("fast f32 gather", FORM_FAST, True), ("exact", FORM_EXACT, False)):
+            st, tuned = make_stereo(w, form, DTYPE_F32, sptr, refs, opts, gather=gather)
+            n_steps = max(2, min(args.steps, 5)) if form == FORM_FAST else 2
+            t = time_solves(st, refs, opts, stream, flush, n_steps, 2)
+            pms = sum(t) / len(t)
+            e = {"form": name, "storage": "f32", "variant": tuned["variant"],
+                 "px_iters_per_s": px_iters_step / (pms / 1e3), "patchmatch_ms": pms,
+                 "accuracy": depth_accuracy(st, w, refs)}
+            if plain:
+                e["speedup_vs_plain"] = e["px_iters_per_s"] / plain["px_iters_per_s"]
+            lm = propagate_launch_ms(st, w, refs, stream, False)
+            e["roofline"] = tex_roof(kname, lm, DTYPE_F32, FETCH_GATHER, "f32, gather")
+            equal[name] = e
+            st.destroy()
+
+    # ---- TSDF: the sweep of the step, and the reference's one-view-per-launch form ---------
+    stereo.solve_all(refs, opts)
+    stereo.filter_all(refs, w.sources, w.needed)
+    visible, updates = tsdf.count_updates(iviews, stereo=stereo, layers=refs)
+    pv = []
+    for i in range(4):
+        tsdf.reset()
+        g = Stage(stream, ["tsdf"])
+        g.mark()
+        for k, r in enumerate(refs):
+            tsdf.integrate_layer(iviews[k], stereo, r)
+        g.mark()
+        torch.cuda.synchronize()
+        if i:
+            pv.append(g.ms()["tsdf"])
+    per_view_ms = sum(pv) / len(pv)
+    sweep_ms = R["stage_ms"]["tsdf"]
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    roof_tsdf = {"kernel": f"k_integrate_many ({V} views per sweep)", "bound": "hbm",
+                 "achieved": vox * 12 / (sweep_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                 "peak_source": peak_kind, "bytes_per_launch": vox * 12,
+                 "bytes_model": "12 B per voxel per sweep (f32 tsdf and Q8.8 weight, read and written)",
+                 "voxel_updates": updates, "visible_voxel_views": visible,
+                 "launch_ms": sweep_ms,
+                 # the one-view-per-pass form moves 12 B per voxel-update it applies; the sweep's
+                 # time against those bytes is its HBM-equivalent rate
+                 "per_view_form_equivalent_frac": updates * 12 / (sweep_ms / 1e3) / 1e9 / hbm}
+    roof_tsdf["frac"] = roof_tsdf["achieved"] / hbm
+    roof_tsdf_view = {"kernel": f"k_integrate ({V} launches, one view each)", "bound": "hbm",
+                      "achieved": updates * 12 / (per_view_ms / 1e3) / 1e9, "peak": hbm,
+                      "unit": "GB/s", "peak_source": peak_kind, "traffic": None,
+                      "bytes_model": "12 B per voxel-update applied (f32 tsdf and Q8.8 weight, "
+                                     "read and written), counted by l3d_tsdf_count_updates",
+                      "bytes_per_step": updates * 12, "voxel_updates": updates,
+                      "visible_voxel_views": visible, "ms_per_step": per_view_ms,
+                      "voxel_updates_per_s": vox * V / (per_view_ms / 1e3)}
+    roof_tsdf_view["frac"] = roof_tsdf_view["achieved"] / hbm
 
     # ---- end to end through the C ABI with pinned host buffers ------------------------------
     e2e = None
     if not args.no_e2e:
         import ctypes as C
+
         from luvas3d import _lib
         lib = _lib.load()
         pinned = [torch.from_numpy(np.ascontiguousarray(im)).pin_memory() for im in w.images]
@@ -813,76 +933,322 @@ def main():
 
         e2e_step()
         torch.cuda.synchronize()
-        ea, eb = mk(2)
-        rec(ea)
+        g = Stage(stream, ["e2e"])
+        g.mark()
         for _ in range(args.steps):
             e2e_step()
-        rec(eb)
+        g.mark()
         torch.cuda.synchronize()
-        e2e_s = torch.tensor([ea.elapsed_time(eb) / 1e3], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
-        e2e = {"value": px_iters_step * args.steps * world / float(e2e_s.item()),
-               "unit": "px-iters/s", "h2d_bytes_per_step": w.pixels * 4,
-               "d2h_bytes_per_step": w.pixels * 4 + vox * 6,
-               "ms_per_step": float(e2e_s.item()) * 1e3 / args.steps,
-               "includes": "image upload from pinned host memory, PatchMatch, filter, "
-                           "read-back of the filtered maps, TSDF sweep with the volume's "
-                           "read-back overlapped (l3d_tsdf_integrate_many_read)"}
+        e2e_s = g.ms()["e2e"] / 1e3
+        e2e = {"value": px_iters_step * args.steps / e2e_s, "unit": "px-iters/s",
+               "h2d_bytes_per_step": w.pixels * 4, "d2h_bytes_per_step": w.pixels * 4 + vox * 6,
+               "ms_per_step": e2e_s * 1e3 / args.steps,
+               "includes": "image upload from pinned host memory, PatchMatch, filter, read-back of "
+                           "the filtered maps, TSDF sweep with the volume's read-back overlapped "
+                           "(l3d_tsdf_integrate_many_read)"}
+    stereo.destroy()
+    tsdf.destroy()
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w, os.cpu_count() or 1)
-        cpu.pop("seconds", None)
+    # ---- the batching (room) and differentiation (polish) configurations ------------------
+    extras = {}
+    if args.workload == "scan" and not args.no_extras:
+        from luvas3d import scenes
 
-    def stage(r):
-        return {k: sum(v) / len(v) for k, v in r["ms"].items()}
+        wr = scenes.room()
+        Vr = len(wr.views)
+        refs_r = list(range(Vr))
+        opts_r = [SolveOptions(wr.sources[r], wr.ranges[r][0], wr.ranges[r][1],
+                               iterations=wr.iterations) for r in refs_r]
+        iv_r = [IntegrationView(v.intrinsics, v.pose, wr.ranges[i][1]) for i, v in enumerate(wr.views)]
+        st, tuned = make_stereo(wr, FORM_FAST, storage, sptr, refs_r, opts_r)
+        vol = TsdfVolume(max(s[0] for s in wr.sizes), max(s[1] for s in wr.sizes), wr.tsdf_voxel,
+                         wr.tsdf_origin, dense=wr.tsdf_dims, truncation=wr.tsdf_truncation,
+                         weight_q8=True, stream=sptr)
+        ms = []
+        for i in range(4):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            g = Stage(stream, ["patchmatch", "filter", "tsdf"])
+            g.mark()
+            st.solve_all(refs_r, opts_r)
+            g.mark()
+            vol.reset()
+            st.filter_all(refs_r, wr.sources, wr.needed)
+            g.mark()
+            vol.integrate_many(iv_r, stereo=st, layers=refs_r)
+            g.mark()
+            torch.cuda.synchronize()
+            if i >= 2:
+                ms.append(g.ms())
+        stage = {k: sum(m[k] for m in ms) / len(ms) for k in ms[0]}
+        vox_r = int(np.prod(wr.tsdf_dims))
+        extras["room"] = {
+            "workload": workload_name(wr), "form": "fast", "storage": args.storage,
+            "variant": tuned["variant"], "graphs": True, "steps": len(ms), "warmup": 2,
+            "px_iters_per_s": wr.pixels * wr.iterations / (stage["patchmatch"] / 1e3),
+            "tsdf_voxel_updates_per_s": vox_r * Vr / (stage["tsdf"] / 1e3),
+            "stage_ms": stage, "depth_accuracy": depth_accuracy(st, wr, refs_r)}
+        st.destroy()
+        vol.destroy()
+        p = polish_measure(24, 5, 3, geometry=False)
+        extras["polish"] = {
+            "workload": p["config"]["workload"], "grad_pass_ms": p["ms_per_step"],
+            "pixel_sources_per_s": p["value"],
+            "polish_ms_per_adam_step": p["polish_from_patchmatch_planes"]["ms_per_step"],
+            "polish_from_patchmatch_planes": p["polish_from_patchmatch_planes"]}
 
+    cpu = None if args.no_cpu_baseline else cpu_baseline(w, os.cpu_count() or 1)
+    eq = equal.get("fast f32 gather")
     line = {
-        "metric": METRIC, "value": value, "unit": "px-iters/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": R["st_s"] * 1e3 / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": f"{args.storage} images, f32 arithmetic" if chosen_form == FORM_FAST else "f32",
+        "metric": METRIC, "value": value, "unit": "px-iters/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": R["stage_ms"]["step"], "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": (f"{args.storage} images, f32 arithmetic" if chosen == FORM_FAST else "f32"),
         "data": ("synthetic (seeded room scene with cuboids, value-noise texture)" if w.name == "room"
                  else "synthetic (seeded sphere-on-plane scene, value-noise texture)"),
         "scene": scene_conventions(w),
         "config": {"workload": workload_name(w),
-                   "form": "fast" if chosen_form == FORM_FAST else "plain",
-                   "variant": tuned.get("variant"),
-                   "graphs": chosen_form == FORM_FAST,
-                   "l2": "flushed (256 MB write) before every step",
-                   "parallelism": f"replica x{world}"},
-        "tsdf_voxel_updates_per_s": voxel_updates / R["ts_s"],
-        "stage_ms": stage(R),
-        "depth_accuracy": acc,
-        "plain": ({"px_iters_per_s": res[FORM_PLAIN]["px_iters_per_s"],
-                   "stage_ms": stage(res[FORM_PLAIN]),
-                   "propagate_launch_ms": res[FORM_PLAIN]["prop_ms"]}
-                  if FORM_PLAIN in res else None),
-        "speedup_vs_plain": (value / res[FORM_PLAIN]["px_iters_per_s"]
-                             if FORM_PLAIN in res and chosen_form != FORM_PLAIN else None),
+                   "form": {FORM_FAST: "fast", FORM_PLAIN: "plain", FORM_EXACT: "exact"}[chosen],
+                   "variant": R["tuned"]["variant"], "graphs": chosen != FORM_PLAIN,
+                   "l2": "flushed (256 MB write) before every step", "parallelism": "1 GPU"},
+        "tsdf_voxel_updates_per_s": vox * V / (R["stage_ms"]["tsdf"] / 1e3),
+        "stage_ms": R["stage_ms"],
+        "depth_accuracy": {"plain": plain["accuracy"] if plain else None, "chosen": R["accuracy"]},
+        "plain": ({"px_iters_per_s": plain["px_iters_per_s"], "stage_ms": plain["stage_ms"],
+                   "propagate_launch_ms": plain["prop_ms"]} if plain else None),
+        "speedup_vs_plain": value / plain["px_iters_per_s"] if plain else None,
+        "equal_fp64_accuracy_forms": equal or None,
+        "speedup_vs_plain_at_equal_fp64_accuracy": eq.get("speedup_vs_plain") if eq else None,
+        "fp64_accuracy_basis": ("depth within 1e-3 relative of the FP64 oracle's solve and plane "
+                                "costs within 1e-4 at p99, per form, on the scan subset and the "
+                                "small workload: tests/test_precision_gpu.py"),
         "roofline": roof_tex or roof_fp32,
         "roofline_fp32": roof_fp32,
-        "roofline_tsdf": {"kernel": f"k_integrate_many ({V} views per sweep)", "bound": "hbm",
-                          "achieved": tsdf_gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-                          "frac": tsdf_gbs / peaks.get("hbm_gbs", 6650.0),
-                          "peak_source": peak_kind, "bytes_per_launch": tsdf_bytes,
-                          # the one-view-per-pass form streams 12 B per voxel-update; the sweep's
-                          # time against that form's bytes is its HBM-equivalent rate
-                          "per_view_form_bytes": vox * V * 12,
-                          "per_view_form_equivalent_frac":
-                              vox * V * 12 / (tsdf_ms / 1e3) / 1e9 / peaks.get("hbm_gbs", 6650.0)},
-        "clocks": clk,
+        "roofline_tsdf": roof_tsdf,
+        "roofline_tsdf_per_view": roof_tsdf_view,
+        "clocks": R["clk"],
         "gpu_launches": R["launches"],
         "e2e": e2e,
+        "batching_room": extras.get("room"),
+        "differentiation_polish": extras.get("polish"),
         "cpu_baseline": cpu,
     }
+    print(json.dumps(line), flush=True)
+
+
+def run_split(args, rank: int, world: int, local: int) -> None:
+    """N GPUs, one process each: one scan split over the ranks (luvas3d.shard.ScanSplit): each
+    rank solves its share of the reference views (dealt by pixel count), one NCCL all-gather
+    gives every rank every view's packed depth map, every rank filters every view, and each
+    rank integrates every view into its z-slab of the TSDF volume (a brick pool).  The split
+    equals the one-GPU scan bit for bit (tests/test_shard.py runs the same driver on gloo ranks);
+    the whole-job rate is the scan's px-iters over the slowest rank's time."""
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    from luvas3d import (DTYPE_BF16, DTYPE_F16, DTYPE_F32, DTYPE_U8, FORM_FAST, IntegrationView,
+                         SolveOptions, TsdfVolume, shard)
+
+    # communicator set-up lines in the log (ranks, transport) without per-call chatter
+    os.environ.setdefault("NCCL_DEBUG", "INFO")
+    os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+    device = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
+    w = build_workload(args)
+    V = len(w.views)
+    sizes = w.sizes or [(w.width, w.height)] * V
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    refs = list(range(V))
+    opts = [SolveOptions(w.sources[r], w.ranges[r][0], w.ranges[r][1], iterations=w.iterations)
+            for r in refs]
+    iviews = [IntegrationView(v.intrinsics, v.pose, w.ranges[i][1]) for i, v in enumerate(w.views)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    storage = {"f16": DTYPE_F16, "u8": DTYPE_U8, "f32": DTYPE_F32, "bf16": DTYPE_BF16}[args.storage]
+    mine = shard.shard_views(sizes, world)[rank]
+    st, tuned = make_stereo(w, FORM_FAST, storage, sptr, mine or refs[:1],
+                            [opts[v] for v in (mine or refs[:1])],
+                            variant=args.variant if args.variant >= 0 else None)
+    coords = shard.slab_pool(w.tsdf_dims, rank, world)
+    vol = None
+    if coords is not None:
+        vol = TsdfVolume(max(s[0] for s in sizes), max(s[1] for s in sizes), w.tsdf_voxel,
+                         w.tsdf_origin, layout=(coords,), truncation=w.tsdf_truncation,
+                         weight_q8=True, stream=sptr)
+    split = shard.ScanSplit(shard.DeviceScan(st, vol, opts, w.sources, w.needed, iviews), sizes,
+                            rank, world, device=device)
+    names = ["patchmatch", "exchange", "filter", "tsdf"]
+
+    def step(g):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        g.mark()
+        split.solve()
+        g.mark()
+        split.exchange()
+        g.mark()
+        if vol is not None:
+            vol.reset()
+        split.filter()
+        g.mark()
+        split.integrate()
+        g.mark()
+
+    for _ in range(args.warmup):
+        step(Stage(stream, names))
+    torch.cuda.synchronize()
+    dist.barrier()
+    launches0 = st.launches + (vol.launches if vol else 0)
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    gs = []
+    for _ in range(args.steps):
+        g = Stage(stream, names)
+        step(g)
+        gs.append(g)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop() if clocks else None
+    launches = st.launches + (vol.launches if vol else 0) - launches0
+    ms = [g.ms() for g in gs]
+    stage = {k: sum(m[k] for m in ms) / len(ms) for k in ms[0]}
+    tot = torch.tensor([sum(m["patchmatch"] for m in ms), sum(m["tsdf"] for m in ms),
+                        sum(m["step"] for m in ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    pm_s, ts_s, st_s = (float(x) / 1e3 for x in tot.tolist())
+    px_iters_step = w.pixels * w.iterations
+    vox = int(np.prod(w.tsdf_dims))
+
+    # end to end: every rank uploads every image from pinned host memory (each holds all the
+    # sources), runs the split step and reads back its views' filtered maps and its slab
+    e2e = None
+    if not args.no_e2e:
+        import ctypes as C
+
+        from luvas3d import _lib
+        lib = _lib.load()
+        pinned = [torch.from_numpy(np.ascontiguousarray(im)).pin_memory() for im in w.images]
+        f_off = np.concatenate([[0], np.cumsum([a * b for a, b in sizes])])
+        out_f = torch.empty(w.pixels, dtype=torch.int32).pin_memory()
+        nvox = 0 if vol is None else vol.voxels
+        out_t = torch.empty(max(1, nvox), dtype=torch.float32).pin_memory()
+        out_w = torch.empty(max(1, nvox), dtype=torch.int16).pin_memory()
+
+        def e2e_step():
+            for i, im in enumerate(pinned):
+                st.set_image_device(i, im.data_ptr(), DTYPE_F32)
+            split.solve()
+            split.exchange()
+            if vol is not None:
+                vol.reset()
+            split.filter()
+            for r in mine:
+                _lib.check(lib.l3d_stereo_read_filtered_layer(
+                    st._h(), r, C.c_void_p(out_f[int(f_off[r]):].data_ptr())))
+            if vol is not None:
+                vol.integrate_many_read(iviews, stereo=st, layers=refs, out=(out_t, out_w))
+
+        e2e_step()
+        torch.cuda.synchronize()
+        dist.barrier()
+        g = Stage(stream, ["e2e"])
+        g.mark()
+        for _ in range(args.steps):
+            e2e_step()
+        g.mark()
+        torch.cuda.synchronize()
+        e2e_s = shard.max_over_ranks(g.ms()["e2e"] / 1e3, device=device)
+        e2e = {"value": px_iters_step * args.steps / e2e_s, "unit": "px-iters/s",
+               "h2d_bytes_per_step": world * w.pixels * 4, "d2h_bytes_per_step": w.pixels * 4 + vox * 6,
+               "ms_per_step": e2e_s * 1e3 / args.steps,
+               "includes": "every rank: every image uploaded from pinned host memory, its views' "
+                           "PatchMatch, the all-gather of packed maps, every view's filter, the "
+                           "read-back of its views' filtered maps, the sweep of its slab with the "
+                           "slab's read-back overlapped"}
     if rank == 0:
+        line = {
+            "metric": METRIC, "value": px_iters_step * args.steps / pm_s, "unit": "px-iters/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": st_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": f"{args.storage} images, f32 arithmetic",
+            "data": "synthetic (seeded sphere-on-plane scene, value-noise texture)",
+            "scene": scene_conventions(w),
+            "config": {"workload": workload_name(w), "form": "fast", "variant": tuned["variant"],
+                       "graphs": True, "l2": "flushed (256 MB write) before every step",
+                       "parallelism": (f"split over {world} GPUs: reference views dealt by pixel "
+                                       "count, one NCCL all-gather of the packed depth maps per "
+                                       "step, TSDF z-slabs of bricks per GPU")},
+            "tsdf_voxel_updates_per_s": vox * V * args.steps / ts_s,
+            "stage_ms_rank0": stage,
+            "views_rank0": len(mine),
+            "clocks": clk,
+            "gpu_launches": launches,
+            "e2e": e2e,
+            "cpu_baseline": None,
+        }
         print(json.dumps(line), flush=True)
-    stereo.destroy()
-    tsdf.destroy()
-    if world > 1:
-        dist.destroy_process_group()
+    st.destroy()
+    if vol is not None:
+        vol.destroy()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="auto", choices=["auto", "plain", "fast", "exact"])
+    ap.add_argument("--workload", default="scan", choices=["scan", "room", "polish", "fusion"])
+    ap.add_argument("--views", type=int, default=0)
+    ap.add_argument("--width", type=int, default=640)
+    ap.add_argument("--height", type=int, default=480)
+    ap.add_argument("--tsdf-dim", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the equal-accuracy forms and the room / polish configurations")
+    ap.add_argument("--split", action="store_true",
+                    help="run the multi-GPU split path even on one GPU (a one-rank communicator)")
+    ap.add_argument("--storage", default="f16", choices=["f16", "u8", "f32", "bf16"],
+                    help="fast-form image storage")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="fast-form kernel variant; default: the autotuner's choice")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(relaunch(args.gpus))
+
+    import torch
+
+    torch.cuda.set_device(local)
+    if args.workload == "polish":
+        if rank == 0:
+            run_polish(args)
+        return
+    if args.workload == "fusion":
+        if rank == 0:
+            run_fusion(args)
+        return
+    if world > 1 or args.split:
+        if "WORLD_SIZE" not in os.environ:
+            os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(_free_port()), RANK="0",
+                              WORLD_SIZE="1", LOCAL_RANK="0")
+        run_split(args, rank, world, local)
+        return
+    run_scan(args)
 
 
 if __name__ == "__main__":
