@@ -1789,13 +1789,16 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
             for (cudaEvent_t& ev : t->slab_done)
                 L3D_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event creation");
         }
-        int vpu = 1;
-        const long long units = l3d_tsdf_sweep_units(t->g, &vpu);
-        const long long per = (units + L3D_TSDF_READ_SLABS - 1) / L3D_TSDF_READ_SLABS;
+        long long lu = 1, lv = 1;
+        const long long units = l3d_tsdf_sweep_units(t->g, &lu, &lv);
+        const long long layers = units / lu;
+        const long long per = (layers + L3D_TSDF_READ_SLABS - 1) / L3D_TSDF_READ_SLABS;
         /* every launch first, so that a copy into pageable memory (which blocks the host until
-         * it is done) does not hold back the next launch */
+         * it is done) does not hold back the next launch; each slab is whole layers, so its
+         * voxels are one contiguous range */
         for (int i = 0; i < L3D_TSDF_READ_SLABS; i++) {
-            const long long q0 = std::min(units, i * per), q1 = std::min(units, q0 + per);
+            const long long q0 = std::min(layers, i * per) * lu;
+            const long long q1 = std::min(layers, i * per + per) * lu;
             e = l3d_launch_tsdf_many_range(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs,
                                            t->priors, t->normals, t->tsdf, t->weight, t->q8, q0, q1,
                                            t->stream);
@@ -1805,8 +1808,8 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
         }
         const size_t wsize = t->q8 ? 2 : 4;
         for (int i = 0; i < L3D_TSDF_READ_SLABS; i++) {
-            const long long v0 = std::min(units, i * per) * vpu;
-            const long long v1 = std::min(units, i * per + per) * vpu;
+            const long long v0 = std::min(t->voxels, std::min(layers, i * per) * lv);
+            const long long v1 = std::min(t->voxels, std::min(layers, i * per + per) * lv);
             if (v1 <= v0) continue;
             L3D_CUDA(cudaStreamWaitEvent(t->copy, t->slab_done[i], 0), "stream wait");
             if (tsdf_out)

@@ -208,9 +208,12 @@ cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_
                                  const uint32_t* const* depth_ptrs_dev, const float* priors,
                                  const float4* normals, float* tsdf, void* weight, int q8,
                                  cudaStream_t stream);
-/* The sweep's work units (voxel runs of *voxels_per_unit along x, in voxel-index order) and a
- * sweep over units [q_begin, q_end) only: voxels [q_begin, q_end) * voxels_per_unit. */
-long long l3d_tsdf_sweep_units(const L3dTsdfGrid& g, int* voxels_per_unit);
+/* The sweep's work units in launch order (brick-major quads).  They come in layers: a layer is
+ * *layer_units units (dense grid: one z-row of bricks; brick pool: one brick) and covers the
+ * contiguous voxel-index range of *layer_voxels voxels after the layers before it (the last
+ * dense layer may be shorter).  A sweep over units [q_begin, q_end) only (l3d_launch_tsdf_many_
+ * range) with whole layers therefore integrates one contiguous voxel range. */
+long long l3d_tsdf_sweep_units(const L3dTsdfGrid& g, long long* layer_units, long long* layer_voxels);
 cudaError_t l3d_launch_tsdf_many_range(const L3dTsdfGrid& g, const L3dTsdfView* views_dev,
                                        int n_views, const int32_t* coords, const uint8_t* mask,
                                        const uint32_t* const* depth_ptrs_dev, const float* priors,

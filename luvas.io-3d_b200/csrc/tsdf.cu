@@ -180,12 +180,31 @@ __device__ __forceinline__ void apply_q8(float& t, uint32_t& w0i, float obs, flo
     w0i = min(w0i + wi, maxq);
 }
 
-/* Voxel coordinates and storage index of the first voxel of quad q (VEC consecutive x). */
-template <int VEC>
+/* Voxel coordinates and storage index of the first voxel of quad q (VEC consecutive x).
+ * Brick pools and (BRICKS) dense grids run in brick-major order: quad q is quad q % (512 / VEC)
+ * of brick q / (512 / VEC), so the 32 threads of a warp stay inside one 8^3 brick (one mask
+ * entry, one set of views, converged branches) and touch 32-byte row segments of it; quads of a
+ * ragged grid's partial bricks that fall outside the grid are skipped.  Otherwise dense grids
+ * run in voxel-index order. */
+template <int VEC, bool BRICKS = true>
 __device__ __forceinline__ bool quad_coords(const L3dTsdfGrid& g, const int32_t* coords,
                                             long long q, int* gx, int* gy, int* gz,
                                             long long* idx, long long* brick) {
-    if (g.dense) {
+    if (g.dense && BRICKS) {
+        long long b = q / (512 / VEC);
+        if (b >= g.bricks) return false;
+        int local = (int)(q - b * (512 / VEC)) * VEC;
+        const long long bxy = (long long)g.nb[0] * g.nb[1];
+        const int bz = (int)(b / bxy);
+        const int rest = (int)(b - (long long)bz * bxy);
+        const int by = rest / g.nb[0], bx = rest - by * g.nb[0];
+        *gx = bx * 8 + (local & 7);
+        *gy = by * 8 + ((local >> 3) & 7);
+        *gz = bz * 8 + (local >> 6);
+        if (*gx >= g.dims[0] || *gy >= g.dims[1] || *gz >= g.dims[2]) return false;
+        *idx = ((long long)*gz * g.dims[1] + *gy) * g.dims[0] + *gx;
+        *brick = b;
+    } else if (g.dense) {
         long long qx = g.dims[0] / VEC;
         long long rest = q / qx;
         *gx = (int)(q - rest * qx) * VEC;
@@ -652,7 +671,7 @@ __global__ void __launch_bounds__(256) k_integrate_depth(const L3dTsdfGrid g, co
     if (q >= voxels) return;
     int gx, gy, gz;
     long long idx, brick;
-    if (!quad_coords<1>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
+    if (!quad_coords<1, false>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
     float t = tsdf_in[idx];
     float ww = 0.0f;
     uint32_t wq = 0;
@@ -692,7 +711,7 @@ __global__ void __launch_bounds__(256) k_integrate_depth_grad(
     if (q >= voxels) return;
     int gx, gy, gz;
     long long idx, brick;
-    if (!quad_coords<1>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
+    if (!quad_coords<1, false>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
     const float gt = gT[idx];
     const float gw = (!Q8 && gW) ? gW[idx] : 0.0f;
     float g_t0 = gt, g_w0 = gw;
@@ -740,9 +759,15 @@ __global__ void k_fill(float* tsdf, void* weight, long long voxels, int q8) {
 
 inline bool vec4_ok(const L3dTsdfGrid& g) { return !g.dense || (g.dims[0] % 4 == 0); }
 
+/* Threads of the integration kernels (brick-major order, see quad_coords). */
 inline long long quad_count(const L3dTsdfGrid& g, int vec) {
-    if (g.dense) return (long long)(g.dims[0] / vec) * g.dims[1] * g.dims[2];
     return g.bricks * (512 / vec);
+}
+
+/* Threads of the per-voxel kernels in voxel-index order. */
+inline long long voxel_count(const L3dTsdfGrid& g) {
+    if (g.dense) return (long long)g.dims[0] * g.dims[1] * g.dims[2];
+    return g.bricks * 512;
 }
 
 }  // namespace
@@ -839,9 +864,15 @@ cudaError_t l3d_launch_normal_table(float4* normals, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-long long l3d_tsdf_sweep_units(const L3dTsdfGrid& g, int* voxels_per_unit) {
+long long l3d_tsdf_sweep_units(const L3dTsdfGrid& g, long long* layer_units, long long* layer_voxels) {
     const int vec = vec4_ok(g) ? 4 : 1;
-    if (voxels_per_unit) *voxels_per_unit = vec;
+    if (g.dense) {
+        if (layer_units) *layer_units = (long long)g.nb[0] * g.nb[1] * (512 / vec);
+        if (layer_voxels) *layer_voxels = 8ll * g.dims[0] * g.dims[1];
+    } else {
+        if (layer_units) *layer_units = 512 / vec;
+        if (layer_voxels) *layer_voxels = 512;
+    }
     return quad_count(g, vec);
 }
 
@@ -870,7 +901,7 @@ cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_
                                  const float4* normals, float* tsdf, void* weight, int q8,
                                  cudaStream_t stream) {
     return l3d_launch_tsdf_many_range(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors,
-                                      normals, tsdf, weight, q8, 0, l3d_tsdf_sweep_units(g, nullptr),
+                                      normals, tsdf, weight, q8, 0, l3d_tsdf_sweep_units(g, nullptr, nullptr),
                                       stream);
 }
 
@@ -883,7 +914,7 @@ cudaError_t l3d_launch_tsdf_depth(const L3dTsdfGrid& g, const L3dTsdfView& v, co
                                   cudaStream_t stream) {
     if (g.bricks == 0) return cudaSuccess;
     k_visible_one<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, v, coords, mask);
-    const long long voxels = quad_count(g, 1);
+    const long long voxels = voxel_count(g);
     if (voxels == 0) return cudaSuccess;
     const unsigned blocks = (unsigned)((voxels + 255) / 256);
     if (grad_tsdf_out) {
