@@ -1410,6 +1410,7 @@ struct l3d_tsdf {
     long long prior_cap = 0;
     float4* normals = nullptr;        /* decoded normal per 12-bit normal code */
     float* tiles = nullptr;           /* depth tiles of the depth-aware brick cull, tile_cap */
+    int32_t* list = nullptr;          /* 1 + bricks: kept bricks of a one-view integration */
     long long tile_cap = 0;
     L3dTsdfView* views_host = nullptr;      /* pinned staging for views */
     const uint32_t** ptrs_host = nullptr;   /* pinned staging for depth pointers */
@@ -1468,7 +1469,8 @@ int ensure_mask(l3d_tsdf* t, int n) {
     cudaFree(t->mask);
     t->mask = nullptr;
     t->mask_views = 0;
-    L3D_CUDA(cudaMalloc(&t->mask, (size_t)t->g.bricks * n), "brick mask");
+    /* brick-major rows of n flags padded to 16 bytes (one flag per brick for one view) */
+    L3D_CUDA(cudaMalloc(&t->mask, (size_t)t->g.bricks * (size_t)((n + 15) & ~15)), "brick mask");
     t->mask_views = n;
     return L3D_OK;
 }
@@ -1476,8 +1478,8 @@ int ensure_mask(l3d_tsdf* t, int n) {
 /* Depth tiles of the depth-aware brick cull, sized in tiles. */
 int ensure_tiles(l3d_tsdf* t, long long n) {
     if (t->tile_cap >= n) return L3D_OK;
-    cudaStreamSynchronize(t->stream);
-    cudaFree(t->tiles);
+    L3D_CUDA(cudaStreamSynchronize(t->stream), "depth tiles: wait");
+    L3D_CUDA(cudaFree(t->tiles), "depth tiles: free");
     t->tiles = nullptr;
     t->tile_cap = 0;
     L3D_CUDA(cudaMalloc(&t->tiles, (size_t)n * sizeof(float)), "depth tiles");
@@ -1662,8 +1664,10 @@ static int integrate_one(l3d_tsdf* t, const l3d_stereo* src, int layer, const ui
     }
     /* visibility of this view's bricks, then the integration: two launches */
     if ((rc = ensure_tiles(t, l3d_depth_tile_count(mw, mh)))) return rc;
+    if (!t->list) L3D_CUDA(cudaMalloc(&t->list, (size_t)(t->g.bricks + 1) * sizeof(int32_t)), "brick list");
+    L3D_CUDA(cudaGetLastError(), "before the integrate launch");
     cudaError_t e = l3d_launch_tsdf_view(t->g, v, t->coords, t->mask, depth, prior, t->normals, t->tiles,
-                                         t->tsdf, t->weight, t->q8, t->stream);
+                                         t->list, t->tsdf, t->weight, t->q8, t->stream);
     t->launches += 3;
     if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
     if (src && (rc = before_stereo(t, src))) return rc;
@@ -1955,6 +1959,7 @@ void l3d_tsdf_destroy(l3d_tsdf* t) {
     cudaFree(t->priors);
     cudaFree(t->normals);
     cudaFree(t->tiles);
+    cudaFree(t->list);
     cudaFreeHost(t->views_host);
     cudaFreeHost(t->ptrs_host);
     if (t->done) cudaEventDestroy(t->done);

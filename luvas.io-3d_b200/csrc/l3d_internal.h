@@ -176,11 +176,13 @@ cudaError_t l3d_launch_tsdf_visible(const L3dTsdfGrid& g, const L3dTsdfView* vie
 /* visibility of one view (into mask) followed by its integration: two launches (three with
  * tiles).  normals: the decoded-normal table (l3d_launch_normal_table), or NULL to decode each
  * normal in place; tiles: scratch of l3d_depth_tile_count(v.W, v.H) floats for the depth-aware
- * cull, or NULL for visibleBricks alone (same results either way) */
+ * cull, or NULL for visibleBricks alone; list (with tiles and normals): scratch of 1 + bricks
+ * int32 that lists the kept bricks, so that only their quads are launched (same results in
+ * every case) */
 cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,
                                  uint8_t* mask, const uint32_t* depth, const float* prior,
-                                 const float4* normals, float* tiles, float* tsdf, void* weight, int q8,
-                                 cudaStream_t stream);
+                                 const float4* normals, float* tiles, int32_t* list, float* tsdf,
+                                 void* weight, int q8, cudaStream_t stream);
 /* Depth tiles for the depth-aware brick cull: per view, the largest depth a voxel of that view
  * can be updated from over every L3D_DEPTH_TILE x L3D_DEPTH_TILE pixel tile (decoded f16 depth,
  * or the prior where the map has none), views[i].tile_off elements into `tiles`. */

@@ -141,7 +141,7 @@ extern "C" int l3d_tsdf_integrate_noalloc(const l3d_tsdf_desc* d, const int32_t*
     int rc = flags_address(&flags);
     if (rc) return noalloc_fail(rc, "could not look up the brick-flag array on this device");
     cudaError_t e = l3d_launch_tsdf_view(g, v, d->dense ? nullptr : coords_dev, (uint8_t*)flags,
-                                         depth_dev, prior_dev, nullptr, nullptr, tsdf_dev, weight_dev,
+                                         depth_dev, prior_dev, nullptr, nullptr, nullptr, tsdf_dev, weight_dev,
                                          d->weight_type == L3D_WEIGHT_Q8, (cudaStream_t)stream);
     if (e != cudaSuccess) {
         char msg[256];

@@ -31,6 +31,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include <cuda_fp16.h>
 
 #include "l3d_fmath.h"
@@ -258,13 +260,19 @@ __device__ __forceinline__ uint8_t brick_visible(const L3dTsdfGrid& g, const L3d
     return 1;
 }
 
+/* The many-view brick mask is brick-major: brick b's flags for views 0..n-1 are the bytes
+ * mask[b * mask_stride(n) + v], the row padded with zeros to a multiple of 16 bytes, so a thread
+ * reads a brick's views with 128-bit loads. */
+__host__ __device__ __forceinline__ int mask_stride(int n_views) { return (n_views + 15) & ~15; }
+
 __global__ void k_visible(const L3dTsdfGrid g, const L3dTsdfView* __restrict__ views, int n_views,
                           const int32_t* __restrict__ coords, uint8_t* __restrict__ mask) {
+    const int stride = mask_stride(n_views);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= g.bricks * n_views) return;
-    int vi = (int)(t / g.bricks);
-    long long b = t - (long long)vi * g.bricks;
-    mask[t] = brick_visible(g, views[vi], coords, b);
+    if (t >= g.bricks * stride) return;
+    long long b = t / stride;
+    int vi = (int)(t - b * stride);
+    mask[t] = vi < n_views ? brick_visible(g, views[vi], coords, b) : 0;
 }
 
 /* The depth-aware half of the brick cull.  A voxel of view v is updated only from the depth d
@@ -361,10 +369,15 @@ __global__ void k_depth_tiles_one(const L3dTsdfView v, const uint32_t* __restric
 __global__ void k_visible_depth(const L3dTsdfGrid g, const L3dTsdfView* __restrict__ views, int n_views,
                                 const int32_t* __restrict__ coords, const float* __restrict__ tiles,
                                 uint8_t* __restrict__ mask) {
+    const int stride = mask_stride(n_views);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= g.bricks * n_views) return;
-    int vi = (int)(t / g.bricks);
-    long long b = t - (long long)vi * g.bricks;
+    if (t >= g.bricks * stride) return;
+    long long b = t / stride;
+    int vi = (int)(t - b * stride);
+    if (vi >= n_views) {
+        mask[t] = 0;
+        return;
+    }
     uint8_t m = brick_visible(g, views[vi], coords, b);
     if (m && tiles && brick_behind_depths(g, views[vi], coords, tiles, b)) m = 0;
     mask[t] = m;
@@ -380,6 +393,19 @@ __global__ void k_visible_one_depth(const L3dTsdfGrid g, const L3dTsdfView v,
     mask[b] = m;
 }
 
+/* k_visible_one_depth that also lists the kept bricks: list[0] counts them (zeroed before the
+ * launch), list[1..] receives their indices in any order. */
+__global__ void k_visible_one_list(const L3dTsdfGrid g, const L3dTsdfView v,
+                                   const int32_t* __restrict__ coords, const float* __restrict__ tiles,
+                                   uint8_t* __restrict__ mask, int32_t* __restrict__ list) {
+    long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= g.bricks) return;
+    uint8_t m = brick_visible(g, v, coords, b);
+    if (m && brick_behind_depths(g, v, coords, tiles, b)) m = 0;
+    mask[b] = m;
+    if (m) list[1 + atomicAdd(list, 1)] = (int32_t)b;
+}
+
 __global__ void k_visible_one(const L3dTsdfGrid g, const L3dTsdfView v,
                               const int32_t* __restrict__ coords, uint8_t* __restrict__ mask) {
     long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -391,20 +417,18 @@ __global__ void k_visible_one(const L3dTsdfGrid g, const L3dTsdfView v,
  * table and a quad's four depth loads are issued together (lut_pixel / lut_observe, the sweep's
  * path, equal to observe() bit for bit); otherwise observe() decodes each normal. */
 template <int VEC, bool Q8, bool LUT>
-__global__ void __launch_bounds__(256) k_integrate(const L3dTsdfGrid g, const L3dTsdfView v,
-                                                   const int32_t* __restrict__ coords,
-                                                   const uint8_t* __restrict__ mask,
-                                                   const uint32_t* __restrict__ depth,
-                                                   const float* __restrict__ prior,
-                                                   const float4* __restrict__ normals,
-                                                   float* __restrict__ tsdf, void* __restrict__ weight,
-                                                   long long quads) {
-    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= quads) return;
+__device__ __forceinline__ void integrate_quad(const L3dTsdfGrid& g, const L3dTsdfView& v,
+                                               const int32_t* __restrict__ coords,
+                                               const uint8_t* __restrict__ mask,
+                                               const uint32_t* __restrict__ depth,
+                                               const float* __restrict__ prior,
+                                               const float4* __restrict__ normals,
+                                               float* __restrict__ tsdf, void* __restrict__ weight,
+                                               long long q) {
     int gx, gy, gz;
     long long idx, brick;
     if (!quad_coords<VEC>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
-    if (!mask[brick]) return;
+    if (mask && !mask[brick]) return;
     float obs[VEC], w[VEC];
     bool ok[VEC];
     bool any = false;
@@ -468,6 +492,42 @@ __global__ void __launch_bounds__(256) k_integrate(const L3dTsdfGrid g, const L3
     }
 }
 
+template <int VEC, bool Q8, bool LUT>
+__global__ void __launch_bounds__(256) k_integrate(const L3dTsdfGrid g, const L3dTsdfView v,
+                                                   const int32_t* __restrict__ coords,
+                                                   const uint8_t* __restrict__ mask,
+                                                   const uint32_t* __restrict__ depth,
+                                                   const float* __restrict__ prior,
+                                                   const float4* __restrict__ normals,
+                                                   float* __restrict__ tsdf, void* __restrict__ weight,
+                                                   long long quads) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= quads) return;
+    integrate_quad<VEC, Q8, LUT>(g, v, coords, mask, depth, prior, normals, tsdf, weight, q);
+}
+
+/* One view over its kept bricks only: list[0] bricks listed at list[1..] (by
+ * k_visible_one_list, in any order; each brick's voxels are updated independently), a
+ * grid-stride loop over their quads. */
+template <int VEC, bool Q8>
+__global__ void __launch_bounds__(256) k_integrate_list(const L3dTsdfGrid g, const L3dTsdfView v,
+                                                        const int32_t* __restrict__ coords,
+                                                        const int32_t* __restrict__ list,
+                                                        const uint32_t* __restrict__ depth,
+                                                        const float* __restrict__ prior,
+                                                        const float4* __restrict__ normals,
+                                                        float* __restrict__ tsdf,
+                                                        void* __restrict__ weight) {
+    constexpr int PER = 512 / VEC;
+    const long long n = (long long)__ldg(list) * PER;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long b = __ldg(list + 1 + i / PER);
+        integrate_quad<VEC, Q8, true>(g, v, coords, nullptr, depth, prior, normals, tsdf, weight,
+                                      b * PER + i % PER);
+    }
+}
+
 template <int VEC, bool Q8>
 __global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
                                                         const L3dTsdfView* __restrict__ views,
@@ -485,6 +545,16 @@ __global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
     int gx, gy, gz;
     long long idx, brick;
     if (!quad_coords<VEC>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
+    /* the brick's row of the mask, 16 views per 128-bit load; a brick no view keeps is left
+     * without touching the volume */
+    const int stride = mask_stride(n_views);
+    const uint4* mrow = (const uint4*)(mask + brick * stride);
+    uint32_t any = 0u;
+    for (int k = 0; k < stride / 16; k++) {
+        const uint4 m = __ldg(mrow + k);
+        any |= m.x | m.y | m.z | m.w;
+    }
+    if (!any) return;
     float t[VEC];
     float wf[VEC];
     uint32_t wq[VEC];
@@ -493,22 +563,31 @@ __global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
     for (int j = 0; j < VEC; j++) wx[j] = fmaf((float)(gx + j) + 0.5f, g.voxel, g.origin[0]);
     const float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
     const float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
-    /* the quad's volume values are loaded up front, so their latency overlaps the first view's
-     * projection; they are written back only when a view updated them */
-#pragma unroll
-    for (int k = 0; k < VEC; k++) {
-        t[k] = tsdf[idx + k];
-        if (Q8) wq[k] = ((const uint16_t*)weight)[idx + k];
-        else wf[k] = ((const float*)weight)[idx + k];
+    /* the quad's volume values are loaded up front (one 128-bit tsdf load, one 64-bit Q8.8 or
+     * 128-bit f32 weight load), so their latency overlaps the first view's projection; they are
+     * written back only when a view updated them */
+    if (VEC == 4) {
+        const float4 t4 = *(const float4*)(tsdf + idx);
+        t[0] = t4.x; t[1] = t4.y; t[2] = t4.z; t[3] = t4.w;
+        if (Q8) {
+            const ushort4 w4 = *(const ushort4*)((const uint16_t*)weight + idx);
+            wq[0] = w4.x; wq[1] = w4.y; wq[2] = w4.z; wq[3] = w4.w;
+        } else {
+            const float4 w4 = *(const float4*)((const float*)weight + idx);
+            wf[0] = w4.x; wf[1] = w4.y; wf[2] = w4.z; wf[3] = w4.w;
+        }
+    } else {
+        t[0] = tsdf[idx];
+        if (Q8) wq[0] = ((const uint16_t*)weight)[idx];
+        else wf[0] = ((const float*)weight)[idx];
     }
     bool loaded = false;
-    /* the brick's visibility in 32 views at a time: 32 independent mask loads, then only the
-     * views that see the brick, in view order */
-    for (int w0 = 0; w0 < n_views; w0 += 32) {
-      uint32_t seen = 0u;
-#pragma unroll
-      for (int k = 0; k < 32; k++)
-          if (w0 + k < n_views && mask[(long long)(w0 + k) * g.bricks + brick]) seen |= 1u << k;
+    /* the views that keep the brick, 16 at a time, in view order: a mask byte is 0 or 1, so
+     * (word * 0x10204080) >> 28 gathers a 32-bit word's four flags into four bits */
+    for (int w0 = 0; w0 < n_views; w0 += 16) {
+      const uint4 m = __ldg(mrow + w0 / 16);
+      uint32_t seen = ((m.x * 0x10204080u) >> 28) | (((m.y * 0x10204080u) >> 28) << 4) |
+                      (((m.z * 0x10204080u) >> 28) << 8) | (((m.w * 0x10204080u) >> 28) << 12);
       while (seen) {
         const int vi = w0 + __ffs(seen) - 1;
         seen &= seen - 1u;
@@ -569,7 +648,7 @@ __global__ void __launch_bounds__(256) k_count_updates(const L3dTsdfGrid g,
         const float wy = fmaf((float)gy + 0.5f, g.voxel, g.origin[1]);
         const float wz = fmaf((float)gz + 0.5f, g.voxel, g.origin[2]);
         for (int vi = 0; vi < n_views; vi++) {
-            if (!mask[(long long)vi * g.bricks + brick]) continue;
+            if (!mask[brick * mask_stride(n_views) + vi]) continue;
             vis += VEC;
             const L3dTsdfView& v = views[vi];
             const float* prior = v.has_prior ? priors + v.prior_off : nullptr;
@@ -774,8 +853,8 @@ inline long long voxel_count(const L3dTsdfGrid& g) {
 
 cudaError_t l3d_launch_tsdf_visible(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
                                     const int32_t* coords, uint8_t* mask, cudaStream_t stream) {
-    long long n = g.bricks * n_views;
-    if (n == 0) return cudaSuccess;
+    long long n = g.bricks * mask_stride(n_views);
+    if (n == 0 || n_views == 0) return cudaSuccess;
     k_visible<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(g, views_dev, n_views, coords, mask);
     return cudaGetLastError();
 }
@@ -796,17 +875,38 @@ cudaError_t l3d_launch_depth_tiles(const L3dTsdfView* views_dev, int n_views,
 cudaError_t l3d_launch_tsdf_visible_depth(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
                                           const int32_t* coords, const float* tiles, uint8_t* mask,
                                           cudaStream_t stream) {
-    long long n = g.bricks * n_views;
-    if (n == 0) return cudaSuccess;
+    long long n = g.bricks * mask_stride(n_views);
+    if (n == 0 || n_views == 0) return cudaSuccess;
     k_visible_depth<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(g, views_dev, n_views, coords, tiles, mask);
     return cudaGetLastError();
 }
 
 cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, const int32_t* coords,
                                  uint8_t* mask, const uint32_t* depth, const float* prior,
-                                 const float4* normals, float* tiles, float* tsdf, void* weight, int q8,
-                                 cudaStream_t stream) {
+                                 const float4* normals, float* tiles, int32_t* list, float* tsdf,
+                                 void* weight, int q8, cudaStream_t stream) {
     if (g.bricks == 0) return cudaSuccess;
+    if (tiles && list && normals) {
+        /* kept bricks only: tiles, the listing cull, a grid-stride sweep of the listed bricks */
+        const long long nt = l3d_depth_tile_count(v.W, v.H);
+        L3dTsdfView vt = v;
+        vt.tile_off = 0;
+        cudaError_t e = cudaMemsetAsync(list, 0, sizeof(int32_t), stream);
+        if (e != cudaSuccess) return e;
+        k_depth_tiles_one<<<(unsigned)((nt + 127) / 128), 128, 0, stream>>>(vt, depth, prior, tiles);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        k_visible_one_list<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, vt, coords, tiles, mask, list);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        const unsigned blocks = (unsigned)std::min<long long>(148 * 8, (g.bricks * 128 + 255) / 256);
+        if (vec4_ok(g)) {
+            if (q8) k_integrate_list<4, true><<<blocks, 256, 0, stream>>>(g, v, coords, list, depth, prior, normals, tsdf, weight);
+            else k_integrate_list<4, false><<<blocks, 256, 0, stream>>>(g, v, coords, list, depth, prior, normals, tsdf, weight);
+        } else {
+            if (q8) k_integrate_list<1, true><<<blocks, 256, 0, stream>>>(g, v, coords, list, depth, prior, normals, tsdf, weight);
+            else k_integrate_list<1, false><<<blocks, 256, 0, stream>>>(g, v, coords, list, depth, prior, normals, tsdf, weight);
+        }
+        return cudaGetLastError();
+    }
     if (tiles) {
         const long long nt = l3d_depth_tile_count(v.W, v.H);
         L3dTsdfView vt = v;
