@@ -278,13 +278,15 @@ __global__ void k_visible(const L3dTsdfGrid g, const L3dTsdfView* __restrict__ v
 /* The depth-aware half of the brick cull.  A voxel of view v is updated only from the depth d
  * of the pixel it rounds to (the packed map's, or the prior where the map has none), and only
  * if d - z >= -mu for its camera depth z.  The voxel centres of brick b span a box; its eight
- * corners, projected in FP64, bound every centre's camera depth from below (z is affine) and its
- * pixel to the corners' bounding rectangle widened by a pixel (the FP32 projection is rounded
- * to the nearest pixel and differs from FP64 by far less than that).  If the smallest corner
- * depth exceeds the largest depth over the depth tiles covering that rectangle by more than mu
- * plus a margin far above the FP32 rounding of the voxel's camera depth, no voxel of the brick
- * updates: the cull changes which voxels are visited, never a result.  Bricks with a corner at
- * z <= 0.02 or a footprint wider than 32 x 32 tiles are kept. */
+ * corners bound every centre's camera depth from below (z is affine) and its pixel to the
+ * corners' bounding rectangle widened by a pixel (pixels are rounded to the nearest).  If the
+ * smallest corner depth exceeds the largest depth over the depth tiles covering that rectangle
+ * by more than mu plus a margin, no voxel of the brick updates: the cull changes which voxels
+ * are visited, never a result.  The bound is computed in FP32; the margin (0.2 mm plus 1e-6 of
+ * the sum of the magnitudes entering the camera depth, about 17 ulp of it) covers the rounding
+ * of this computation and of the kernels' own FP32 camera depth and sdf, and the one-pixel
+ * widening covers that of the projections.  Bricks with a corner at z <= 0.02 or a footprint
+ * wider than 32 x 32 tiles are kept. */
 __device__ __forceinline__ bool brick_behind_depths(const L3dTsdfGrid& g, const L3dTsdfView& v,
                                                     const int32_t* __restrict__ coords,
                                                     const float* __restrict__ tiles, long long b) {
@@ -298,30 +300,35 @@ __device__ __forceinline__ bool brick_behind_depths(const L3dTsdfGrid& g, const 
         by = coords[b * 4 + 1];
         bz = coords[b * 4 + 2];
     }
-    const double lo[3] = {g.origin_d[0] + (bx * 8 + 0.5) * g.voxel_d, g.origin_d[1] + (by * 8 + 0.5) * g.voxel_d,
-                          g.origin_d[2] + (bz * 8 + 0.5) * g.voxel_d};
-    const double span = 7.0 * g.voxel_d;
-    double zmin = 1e300, umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+    const float* R = v.R;
+    const float lx = fmaf((float)(bx * 8) + 0.5f, g.voxel, g.origin[0]);
+    const float ly = fmaf((float)(by * 8) + 0.5f, g.voxel, g.origin[1]);
+    const float lz = fmaf((float)(bz * 8) + 0.5f, g.voxel, g.origin[2]);
+    const float span = 7.0f * g.voxel;
+    const float3 p0 = make_float3(fmaf(R[2], lz, fmaf(R[1], ly, fmaf(R[0], lx, v.t[0]))),
+                                  fmaf(R[5], lz, fmaf(R[4], ly, fmaf(R[3], lx, v.t[1]))),
+                                  fmaf(R[8], lz, fmaf(R[7], ly, fmaf(R[6], lx, v.t[2]))));
+    const float mag = fabsf(lx) + fabsf(ly) + fabsf(lz) + 3.0f * span + fabsf(v.t[0]) +
+                      fabsf(v.t[1]) + fabsf(v.t[2]);
+    float zmin = 3e38f, umin = 3e38f, umax = -3e38f, vmin = 3e38f, vmax = -3e38f;
+#pragma unroll
     for (int c = 0; c < 8; c++) {
-        const double x = lo[0] + ((c & 1) ? span : 0.0);
-        const double y = lo[1] + ((c & 2) ? span : 0.0);
-        const double z = lo[2] + ((c & 4) ? span : 0.0);
-        const double* R = v.Rd;
-        const double p0 = R[0] * x + R[1] * y + R[2] * z + v.td[0];
-        const double p1 = R[3] * x + R[4] * y + R[5] * z + v.td[1];
-        const double p2 = R[6] * x + R[7] * y + R[8] * z + v.td[2];
-        if (!(p2 > 0.02)) return false;
-        const double u = v.kd[0] * p0 / p2 + v.kd[2], w = v.kd[1] * p1 / p2 + v.kd[3];
-        zmin = fmin(zmin, p2);
-        umin = fmin(umin, u);
-        umax = fmax(umax, u);
-        vmin = fmin(vmin, w);
-        vmax = fmax(vmax, w);
+        const float sx = (c & 1) ? span : 0.0f, sy = (c & 2) ? span : 0.0f, sz = (c & 4) ? span : 0.0f;
+        const float px = fmaf(R[2], sz, fmaf(R[1], sy, fmaf(R[0], sx, p0.x)));
+        const float py = fmaf(R[5], sz, fmaf(R[4], sy, fmaf(R[3], sx, p0.y)));
+        const float pz = fmaf(R[8], sz, fmaf(R[7], sy, fmaf(R[6], sx, p0.z)));
+        if (!(pz > 0.02f)) return false;
+        const float iz = 1.0f / pz;
+        const float u = fmaf(v.k[0] * px, iz, v.k[2]), w = fmaf(v.k[1] * py, iz, v.k[3]);
+        zmin = fminf(zmin, pz);
+        umin = fminf(umin, u);
+        umax = fmaxf(umax, u);
+        vmin = fminf(vmin, w);
+        vmax = fmaxf(vmax, w);
     }
-    const double x0 = fmax(floor(umin) - 1.0, 0.0), x1 = fmin(ceil(umax) + 1.0, (double)(v.W - 1));
-    const double y0 = fmax(floor(vmin) - 1.0, 0.0), y1 = fmin(ceil(vmax) + 1.0, (double)(v.H - 1));
-    const double mu = fmax((double)g.mu, g.trunc_d) + 2e-4;
-    if (x1 < x0 || y1 < y0) return true;  /* no voxel projects into the image */
+    const float x0 = fmaxf(floorf(umin) - 1.0f, 0.0f), x1 = fminf(ceilf(umax) + 1.0f, (float)(v.W - 1));
+    const float y0 = fmaxf(floorf(vmin) - 1.0f, 0.0f), y1 = fminf(ceilf(vmax) + 1.0f, (float)(v.H - 1));
+    if (!(x1 >= x0) || !(y1 >= y0)) return !(isnan(x1) || isnan(y1));  /* nothing projects inside */
     const int tx0 = (int)x0 / L3D_DEPTH_TILE, tx1 = (int)x1 / L3D_DEPTH_TILE;
     const int ty0 = (int)y0 / L3D_DEPTH_TILE, ty1 = (int)y1 / L3D_DEPTH_TILE;
     if (tx1 - tx0 >= 32 || ty1 - ty0 >= 32) return false;
@@ -330,33 +337,41 @@ __device__ __forceinline__ bool brick_behind_depths(const L3dTsdfGrid& g, const 
     float dmax = 0.0f;
     for (int ty = ty0; ty <= ty1; ty++)
         for (int tx = tx0; tx <= tx1; tx++) dmax = fmaxf(dmax, __ldg(vt + (long long)ty * tw + tx));
-    return zmin - (double)dmax > mu;
+    return zmin - dmax > g.mu + 2e-4f + 1e-6f * (mag + dmax);
 }
 
-/* Depth tile t of view v (see l3d_launch_depth_tiles). */
+/* Depth tiles of view v (see l3d_launch_depth_tiles): thread t takes row t % 8 of tile t / 8
+ * (eight pixels), and the eight threads of a tile, consecutive lanes of one warp, combine their
+ * maxima with shuffles; lane 0 of the group writes the tile. */
 __device__ __forceinline__ void depth_tile(const L3dTsdfView& v, const uint32_t* __restrict__ depth,
                                            const float* __restrict__ prior, float* __restrict__ tiles,
                                            long long t) {
+    static_assert(L3D_DEPTH_TILE == 8, "eight rows per tile, eight lanes per tile");
     const int tw = (v.W + L3D_DEPTH_TILE - 1) / L3D_DEPTH_TILE, th = (v.H + L3D_DEPTH_TILE - 1) / L3D_DEPTH_TILE;
-    if (t >= (long long)tw * th) return;
-    const int tx = (int)(t % tw), ty = (int)(t / tw);
+    const long long tile = t >> 3;
+    const int row = (int)(t & 7);
     float m = 0.0f;
-    for (int y = ty * L3D_DEPTH_TILE; y < min(v.H, (ty + 1) * L3D_DEPTH_TILE); y++)
-        for (int x = tx * L3D_DEPTH_TILE; x < min(v.W, (tx + 1) * L3D_DEPTH_TILE); x++) {
-            const long long i = (long long)y * v.W + x;
-            float d = __half2float(__ushort_as_half((unsigned short)(__ldg(depth + i) & 0xffffu)));
-            if (!(d > 0.0f)) d = prior ? __ldg(prior + i) : 0.0f;
-            if (d > m) m = d;  /* NaN never raises the maximum: such a pixel never updates */
-        }
-    tiles[v.tile_off + t] = m;
+    if (tile < (long long)tw * th) {
+        const int tx = (int)(tile % tw), ty = (int)(tile / tw);
+        const int y = ty * L3D_DEPTH_TILE + row;
+        if (y < v.H)
+            for (int x = tx * L3D_DEPTH_TILE; x < min(v.W, (tx + 1) * L3D_DEPTH_TILE); x++) {
+                const long long i = (long long)y * v.W + x;
+                float d = __half2float(__ushort_as_half((unsigned short)(__ldg(depth + i) & 0xffffu)));
+                if (!(d > 0.0f)) d = prior ? __ldg(prior + i) : 0.0f;
+                if (d > m) m = d;  /* NaN never raises the maximum: such a pixel never updates */
+            }
+    }
+    /* the tile's eight lanes are aligned groups of a warp (blocks are whole warps) */
+    for (int o = 4; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (row == 0 && tile < (long long)tw * th) tiles[v.tile_off + tile] = m;
 }
 
 __global__ void k_depth_tiles(const L3dTsdfView* __restrict__ views, int n_views,
                               const uint32_t* const* __restrict__ depths, const float* __restrict__ priors,
                               float* __restrict__ tiles, long long max_tiles) {
     const int vi = blockIdx.y;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= max_tiles) return;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;  /* every lane takes part */
     const L3dTsdfView& v = views[vi];
     depth_tile(v, depths[vi], v.has_prior ? priors + v.prior_off : nullptr, tiles, t);
 }
@@ -378,9 +393,9 @@ __global__ void k_visible_depth(const L3dTsdfGrid g, const L3dTsdfView* __restri
         mask[t] = 0;
         return;
     }
-    uint8_t m = brick_visible(g, views[vi], coords, b);
-    if (m && tiles && brick_behind_depths(g, views[vi], coords, tiles, b)) m = 0;
-    mask[t] = m;
+    /* a brick behind the depths needs no frustum test: it is dropped either way */
+    mask[t] = (tiles && brick_behind_depths(g, views[vi], coords, tiles, b))
+                  ? 0 : brick_visible(g, views[vi], coords, b);
 }
 
 __global__ void k_visible_one_depth(const L3dTsdfGrid g, const L3dTsdfView v,
@@ -388,9 +403,7 @@ __global__ void k_visible_one_depth(const L3dTsdfGrid g, const L3dTsdfView v,
                                     uint8_t* __restrict__ mask) {
     long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= g.bricks) return;
-    uint8_t m = brick_visible(g, v, coords, b);
-    if (m && brick_behind_depths(g, v, coords, tiles, b)) m = 0;
-    mask[b] = m;
+    mask[b] = brick_behind_depths(g, v, coords, tiles, b) ? 0 : brick_visible(g, v, coords, b);
 }
 
 /* k_visible_one_depth that also lists the kept bricks: list[0] counts them (zeroed before the
@@ -400,8 +413,7 @@ __global__ void k_visible_one_list(const L3dTsdfGrid g, const L3dTsdfView v,
                                    uint8_t* __restrict__ mask, int32_t* __restrict__ list) {
     long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= g.bricks) return;
-    uint8_t m = brick_visible(g, v, coords, b);
-    if (m && brick_behind_depths(g, v, coords, tiles, b)) m = 0;
+    const uint8_t m = brick_behind_depths(g, v, coords, tiles, b) ? 0 : brick_visible(g, v, coords, b);
     mask[b] = m;
     if (m) list[1 + atomicAdd(list, 1)] = (int32_t)b;
 }
@@ -867,7 +879,7 @@ cudaError_t l3d_launch_depth_tiles(const L3dTsdfView* views_dev, int n_views,
                                    const uint32_t* const* depth_ptrs_dev, const float* priors,
                                    float* tiles, long long max_tiles, cudaStream_t stream) {
     if (n_views <= 0 || max_tiles <= 0) return cudaSuccess;
-    dim3 grid((unsigned)((max_tiles + 127) / 128), (unsigned)n_views);
+    dim3 grid((unsigned)((max_tiles * 8 + 127) / 128), (unsigned)n_views);
     k_depth_tiles<<<grid, 128, 0, stream>>>(views_dev, n_views, depth_ptrs_dev, priors, tiles, max_tiles);
     return cudaGetLastError();
 }
@@ -893,7 +905,7 @@ cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, con
         vt.tile_off = 0;
         cudaError_t e = cudaMemsetAsync(list, 0, sizeof(int32_t), stream);
         if (e != cudaSuccess) return e;
-        k_depth_tiles_one<<<(unsigned)((nt + 127) / 128), 128, 0, stream>>>(vt, depth, prior, tiles);
+        k_depth_tiles_one<<<(unsigned)((nt * 8 + 127) / 128), 128, 0, stream>>>(vt, depth, prior, tiles);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         k_visible_one_list<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, vt, coords, tiles, mask, list);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -911,7 +923,7 @@ cudaError_t l3d_launch_tsdf_view(const L3dTsdfGrid& g, const L3dTsdfView& v, con
         const long long nt = l3d_depth_tile_count(v.W, v.H);
         L3dTsdfView vt = v;
         vt.tile_off = 0;
-        k_depth_tiles_one<<<(unsigned)((nt + 127) / 128), 128, 0, stream>>>(vt, depth, prior, tiles);
+        k_depth_tiles_one<<<(unsigned)((nt * 8 + 127) / 128), 128, 0, stream>>>(vt, depth, prior, tiles);
         k_visible_one_depth<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, vt, coords, tiles, mask);
     } else {
         k_visible_one<<<(unsigned)((g.bricks + 255) / 256), 256, 0, stream>>>(g, v, coords, mask);
