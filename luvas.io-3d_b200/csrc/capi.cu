@@ -120,6 +120,75 @@ cudaError_t dalloc(T** p, size_t count) {
 
 }  // namespace
 
+/* ---- TSDF descriptor and view conversions shared by the handle API and the allocation-free
+ * entry point (noalloc.cu), so both integrate with the same grid and view constants ---- */
+
+bool l3d_tsdf_grid_of(const l3d_tsdf_desc* d, bool pool_coords_given, L3dTsdfGrid* out, char* why,
+                      size_t why_size) {
+    auto bad = [&](const char* msg) {
+        std::snprintf(why, why_size, "%s", msg);
+        return false;
+    };
+    if (!(d->voxel > 0.0) || !(d->truncation > 0.0) || !(d->max_weight > 0.0))
+        return bad("voxel, truncation and max_weight must be positive");
+    if (d->width <= 0 || d->height <= 0) return bad("depth map size must be positive");
+    if (d->weight_type != L3D_WEIGHT_F32 && d->weight_type != L3D_WEIGHT_Q8)
+        return bad("unknown weight type");
+    if (d->weight_type == L3D_WEIGHT_Q8 && !(d->max_weight * 256.0 <= 65535.0))
+        return bad("Q8.8 weights need max_weight <= 255.99");
+    L3dTsdfGrid g;
+    std::memset(&g, 0, sizeof(g));
+    if (d->dense) {
+        for (int i = 0; i < 3; i++) {
+            if (d->dims[i] <= 0) return bad("dense dims must be positive");
+            g.dims[i] = d->dims[i];
+            g.nb[i] = (d->dims[i] + 7) / 8;
+        }
+        g.bricks = (long long)g.nb[0] * g.nb[1] * g.nb[2];
+    } else {
+        if (d->count <= 0 || !pool_coords_given) return bad("brick pool needs coords and count > 0");
+        g.bricks = d->count;
+    }
+    for (int i = 0; i < 3; i++) {
+        g.origin[i] = (float)d->origin[i];
+        g.origin_d[i] = d->origin[i];
+    }
+    g.voxel = (float)d->voxel;
+    g.mu = (float)d->truncation;
+    g.prior_weight = (float)d->prior_weight;
+    g.max_weight = (float)d->max_weight;
+    g.max_q = (unsigned)rintf(g.max_weight * 256.0f);
+    g.voxel_d = d->voxel;
+    g.trunc_d = d->truncation;
+    g.dense = d->dense ? 1 : 0;
+    g.W = d->width;
+    g.H = d->height;
+    *out = g;
+    return true;
+}
+
+L3dTsdfView l3d_tsdf_view_of(const l3d_integration_view& v) {
+    L3dTsdfView o;
+    std::memset(&o, 0, sizeof(o));
+    const double k[4] = {v.intrinsics.fx, v.intrinsics.fy, v.intrinsics.cx, v.intrinsics.cy};
+    for (int i = 0; i < 4; i++) {
+        o.k[i] = (float)k[i];
+        o.kd[i] = k[i];
+    }
+    for (int i = 0; i < 9; i++) {
+        o.R[i] = (float)v.pose.R[i];
+        o.Rd[i] = v.pose.R[i];
+    }
+    for (int i = 0; i < 3; i++) {
+        o.t[i] = (float)v.pose.t[i];
+        o.td[i] = v.pose.t[i];
+    }
+    o.conf = (float)v.confidence;
+    o.has_prior = v.prior != nullptr;
+    o.max_depth = v.max_depth;
+    return o;
+}
+
 /* ------------------------------------------------------------------ stereo handle ---------- */
 
 struct l3d_stereo {
@@ -1421,27 +1490,7 @@ struct l3d_tsdf {
 
 namespace {
 
-L3dTsdfView make_view(const l3d_integration_view& v) {
-    L3dTsdfView o;
-    std::memset(&o, 0, sizeof(o));
-    const double k[4] = {v.intrinsics.fx, v.intrinsics.fy, v.intrinsics.cx, v.intrinsics.cy};
-    for (int i = 0; i < 4; i++) {
-        o.k[i] = (float)k[i];
-        o.kd[i] = k[i];
-    }
-    for (int i = 0; i < 9; i++) {
-        o.R[i] = (float)v.pose.R[i];
-        o.Rd[i] = v.pose.R[i];
-    }
-    for (int i = 0; i < 3; i++) {
-        o.t[i] = (float)v.pose.t[i];
-        o.td[i] = v.pose.t[i];
-    }
-    o.conf = (float)v.confidence;
-    o.has_prior = v.prior != nullptr;
-    o.max_depth = v.max_depth;
-    return o;
-}
+L3dTsdfView make_view(const l3d_integration_view& v) { return l3d_tsdf_view_of(v); }
 
 int ensure_views(l3d_tsdf* t, int n) {
     if (t->view_cap >= n) return L3D_OK;
@@ -1538,40 +1587,9 @@ int l3d_tsdf_create(const l3d_tsdf_desc* d, l3d_tsdf** out) {
     if (!out) return fail(L3D_EINVAL, "out is NULL");
     *out = nullptr;
     if (!d) return fail(L3D_EINVAL, "descriptor is NULL");
-    if (!(d->voxel > 0.0) || !(d->truncation > 0.0) || !(d->max_weight > 0.0))
-        return fail(L3D_EINVAL, "voxel, truncation and max_weight must be positive");
-    if (d->width <= 0 || d->height <= 0) return fail(L3D_EINVAL, "depth map size must be positive");
-    if (d->weight_type != L3D_WEIGHT_F32 && d->weight_type != L3D_WEIGHT_Q8)
-        return fail(L3D_EINVAL, "unknown weight type %d", d->weight_type);
-    if (d->weight_type == L3D_WEIGHT_Q8 && !(d->max_weight * 256.0 <= 65535.0))
-        return fail(L3D_EINVAL, "Q8.8 weights need max_weight <= 255.99");
     L3dTsdfGrid g;
-    std::memset(&g, 0, sizeof(g));
-    if (d->dense) {
-        for (int i = 0; i < 3; i++) {
-            if (d->dims[i] <= 0) return fail(L3D_EINVAL, "dense dims must be positive");
-            g.dims[i] = d->dims[i];
-            g.nb[i] = (d->dims[i] + 7) / 8;
-        }
-        g.bricks = (long long)g.nb[0] * g.nb[1] * g.nb[2];
-    } else {
-        if (d->count <= 0 || !d->coords) return fail(L3D_EINVAL, "brick pool needs coords and count > 0");
-        g.bricks = d->count;
-    }
-    for (int i = 0; i < 3; i++) {
-        g.origin[i] = (float)d->origin[i];
-        g.origin_d[i] = d->origin[i];
-    }
-    g.voxel = (float)d->voxel;
-    g.mu = (float)d->truncation;
-    g.prior_weight = (float)d->prior_weight;
-    g.max_weight = (float)d->max_weight;
-    g.max_q = (unsigned)rintf(g.max_weight * 256.0f);
-    g.voxel_d = d->voxel;
-    g.trunc_d = d->truncation;
-    g.dense = d->dense ? 1 : 0;
-    g.W = d->width;
-    g.H = d->height;
+    char why[256];
+    if (!l3d_tsdf_grid_of(d, d->coords != nullptr, &g, why, sizeof(why))) return fail(L3D_EINVAL, "%s", why);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "no CUDA device");

@@ -4,8 +4,11 @@
 #ifndef L3D_INTERNAL_H
 #define L3D_INTERNAL_H
 
+#include <stddef.h>
 #include <stdint.h>
 #include <cuda_runtime.h>
+
+#include "../../include/luvas3d.h"
 
 #define L3D_MAX_SOURCES 8      /* MAX_SOURCES, mvs/dense-stereo.ts:44 */
 #define L3D_FILTER_COST 7u     /* FILTER_COST, mvs/patchmatch.wgsl.ts:43 */
@@ -73,6 +76,14 @@ struct L3dTsdfGrid {
     long long bricks;          /* dense: nb product; pool: count */
     int W, H;                  /* depth map size */
 };
+
+/* The grid constants of a TSDF descriptor (validated: false with the reason in why) and the
+ * constants of an integration view (the pose in f32 for the kernels and FP64 for brick
+ * culling), shared by l3d_tsdf_create / l3d_tsdf_integrate and the allocation-free entry point.
+ * pool_coords_given: a brick pool's coordinates are supplied (host or device). */
+bool l3d_tsdf_grid_of(const l3d_tsdf_desc* d, bool pool_coords_given, L3dTsdfGrid* out, char* why,
+                      size_t why_size);
+L3dTsdfView l3d_tsdf_view_of(const l3d_integration_view& v);
 
 /* ---- launchers (stereo.cu / stereo_fast.cu / tsdf.cu); each returns cudaGetLastError() ---- */
 

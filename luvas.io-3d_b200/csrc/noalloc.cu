@@ -15,7 +15,9 @@
  *
  * Every call shares the array.  Each call rewrites the flags of all bricks of its volume before
  * the integration reads them, so nothing needs clearing; but two calls whose kernels overlap on
- * the GPU (different streams, no ordering between them) race on the flags.
+ * the GPU (different streams, no ordering between them) race on the flags.  The cached address
+ * belongs to the device's context: after cudaDeviceReset the process must not call this entry
+ * point again on that device (the address would be stale).
  */
 #include <cuda_runtime.h>
 
@@ -66,32 +68,14 @@ extern "C" int l3d_tsdf_integrate_noalloc(const l3d_tsdf_desc* d, const int32_t*
                                           void* weight_dev, void* stream) {
     if (!d || !view || !depth_dev || !tsdf_dev || !weight_dev)
         return noalloc_fail(L3D_EINVAL, "NULL descriptor, view, depth map or volume buffer");
-    if (!(d->voxel > 0.0) || !(d->truncation > 0.0) || !(d->max_weight > 0.0))
-        return noalloc_fail(L3D_EINVAL, "voxel, truncation and max_weight must be positive");
-    if (d->width <= 0 || d->height <= 0)
-        return noalloc_fail(L3D_EINVAL, "depth map size must be positive");
-    if (d->weight_type != L3D_WEIGHT_F32 && d->weight_type != L3D_WEIGHT_Q8)
-        return noalloc_fail(L3D_EINVAL, "unknown weight type");
-    if (d->weight_type == L3D_WEIGHT_Q8 && !(d->max_weight * 256.0 <= 65535.0))
-        return noalloc_fail(L3D_EINVAL, "Q8.8 weights need max_weight <= 255.99");
     if (!(view->intrinsics.fx != 0.0) || !(view->intrinsics.fy != 0.0))
         return noalloc_fail(L3D_EINVAL, "zero focal length");
     if (((uintptr_t)tsdf_dev & 15u) || ((uintptr_t)weight_dev & 15u))
         return noalloc_fail(L3D_EINVAL, "tsdf and weight buffers must be 16-byte aligned");
+    /* the grid and view constants of the handle API (l3d_tsdf_create / l3d_tsdf_integrate) */
     L3dTsdfGrid g;
-    std::memset(&g, 0, sizeof(g));
-    if (d->dense) {
-        for (int i = 0; i < 3; i++) {
-            if (d->dims[i] <= 0) return noalloc_fail(L3D_EINVAL, "dense dims must be positive");
-            g.dims[i] = d->dims[i];
-            g.nb[i] = (d->dims[i] + 7) / 8;
-        }
-        g.bricks = (long long)g.nb[0] * g.nb[1] * g.nb[2];
-    } else {
-        if (d->count <= 0 || !coords_dev)
-            return noalloc_fail(L3D_EINVAL, "a brick pool needs device coords and count > 0");
-        g.bricks = d->count;
-    }
+    char why[256];
+    if (!l3d_tsdf_grid_of(d, coords_dev != nullptr, &g, why, sizeof(why))) return noalloc_fail(L3D_EINVAL, why);
     if (g.bricks > L3D_NOALLOC_MAX_BRICKS) {
         char msg[256];
         std::snprintf(msg, sizeof(msg),
@@ -100,42 +84,10 @@ extern "C" int l3d_tsdf_integrate_noalloc(const l3d_tsdf_desc* d, const int32_t*
                       g.bricks, (int)L3D_NOALLOC_MAX_BRICKS);
         return noalloc_fail(L3D_EINVAL, msg);
     }
-    for (int i = 0; i < 3; i++) {
-        g.origin[i] = (float)d->origin[i];
-        g.origin_d[i] = d->origin[i];
-    }
-    g.voxel = (float)d->voxel;
-    g.mu = (float)d->truncation;
-    g.prior_weight = (float)d->prior_weight;
-    g.max_weight = (float)d->max_weight;
-    g.max_q = (unsigned)rintf(g.max_weight * 256.0f);
-    g.voxel_d = d->voxel;
-    g.trunc_d = d->truncation;
-    g.dense = d->dense ? 1 : 0;
-    g.W = d->width;
-    g.H = d->height;
-
-    L3dTsdfView v;
-    std::memset(&v, 0, sizeof(v));
-    const double k[4] = {view->intrinsics.fx, view->intrinsics.fy, view->intrinsics.cx,
-                         view->intrinsics.cy};
-    for (int i = 0; i < 4; i++) {
-        v.k[i] = (float)k[i];
-        v.kd[i] = k[i];
-    }
-    for (int i = 0; i < 9; i++) {
-        v.R[i] = (float)view->pose.R[i];
-        v.Rd[i] = view->pose.R[i];
-    }
-    for (int i = 0; i < 3; i++) {
-        v.t[i] = (float)view->pose.t[i];
-        v.td[i] = view->pose.t[i];
-    }
-    v.conf = (float)view->confidence;
-    v.has_prior = prior_dev != nullptr;
+    L3dTsdfView v = l3d_tsdf_view_of(*view);
+    v.has_prior = prior_dev != nullptr;  /* the prior is the caller's device map, not view->prior */
     v.W = d->width;
     v.H = d->height;
-    v.max_depth = view->max_depth;
 
     void* flags = nullptr;
     int rc = flags_address(&flags);
