@@ -246,15 +246,18 @@ int64_t l3d_stereo_launches(const l3d_stereo* s);
 /* Batched-form kernel variant (no reference counterpart; the reference has one WGSL kernel):
  * window rows sampled by the texture unit (6, 4, 3 or 2; the others use software bilinear
  * on the LSU path) + 8 for the 2x2 quad lane mapping + 16 (fast form, 6 rows) for texture
- * gathers weighted with exact FP32 bilinear weights instead of the hardware filter.  All
- * variants compute the same algorithm; fast-form results differ only by the texture unit's 8-bit
- * filter weights on the rows it filters.  The exact form and compensated sums take 6 or 14 (the
- * exact form always gathers). */
+ * gathers weighted with exact FP32 bilinear weights instead of the hardware filter + 32 (fast
+ * form, 6 rows) for the reference window kept in shared memory instead of registers (more
+ * resident warps; results unchanged).  All variants compute the same algorithm; fast-form
+ * results differ only by the texture unit's 8-bit filter weights on the rows it filters.  The
+ * exact form and compensated sums take 6 or 14 (the exact form always gathers and always keeps
+ * its window in shared memory). */
 int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant);
 int32_t l3d_stereo_variant(const l3d_stereo* s);
 
 /* Times every variant of the handle's form on up to three iterations of the given batch (it
- * overwrites that batch's hypotheses) and keeps the fastest; the gather bit (16) stays as set.
+ * overwrites that batch's hypotheses) and keeps the fastest, the shared-memory window (32)
+ * included; the gather bit (16) stays as set.
  * best_variant / best_ms (either may be NULL) report it.
  * No reference counterpart. */
 int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,

@@ -25,7 +25,8 @@
 #include "l3d_internal.h"
 
 /* Fast-form kernel variant: window rows through the texture unit (0..6; the others use software
- * bilinear on the pair image) + 8 for the 2x2 quad lane mapping. */
+ * bilinear on the pair image) + 8 for the 2x2 quad lane mapping (+16 gathers, +32 shared-memory
+ * window: see l3d_stereo_set_variant). */
 #define L3D_FAST_DEFAULT_VARIANT 14
 
 /* Voxel ranges the sweep of l3d_tsdf_integrate_many_read is split into, each read back as soon
@@ -1330,17 +1331,22 @@ int l3d_stereo_view_size(const l3d_stereo* s, int32_t layer, int32_t* width, int
 int l3d_stereo_set_variant(l3d_stereo* s, int32_t variant) {
     if (!s) return fail(L3D_EINVAL, "NULL handle");
     if (!batched(s)) return fail(L3D_ESTATE, "variants select fast- and exact-form kernels");
-    const int rows = variant & 7, rest = variant & ~31;
-    const bool gather = (variant & 16) != 0;
+    const int rows = variant & 7, rest = variant & ~63;
+    const bool gather = (variant & 16) != 0, shared_window = (variant & 32) != 0;
     if (rest || !(rows == 6 || rows == 4 || rows == 3 || rows == 2))
         return fail(L3D_EINVAL, "variant %d: texture rows must be 6, 4, 3 or 2 (+8 for quads, +16 "
-                                "for gathers)", variant);
-    if (rows != 6 && (s->opts.form == L3D_FORM_EXACT || s->opts.compensated || gather))
-        return fail(L3D_EINVAL, "variant %d: the exact form, compensated sums and gathers sample all "
-                                "six rows through the texture unit", variant);
+                                "for gathers, +32 for a shared-memory window)", variant);
+    if (rows != 6 && (s->opts.form == L3D_FORM_EXACT || s->opts.compensated || gather || shared_window))
+        return fail(L3D_EINVAL, "variant %d: the exact form, compensated sums, gathers and the "
+                                "shared-memory window sample all six rows through the texture unit",
+                    variant);
     if (gather && (s->opts.form != L3D_FORM_FAST || s->opts.storage == L3D_DTYPE_BF16))
         return fail(L3D_EINVAL, "variant %d: gathers with exact weights are a fast-form option for "
                                 "texture storage (U8, F16, F32); the exact form always gathers", variant);
+    if (shared_window && (s->opts.form != L3D_FORM_FAST || s->opts.storage == L3D_DTYPE_BF16))
+        return fail(L3D_EINVAL, "variant %d: the shared-memory window is a fast-form option for "
+                                "texture storage (U8, F16, F32); the exact form always keeps its "
+                                "window in shared memory", variant);
     s->variant = variant;
     return L3D_OK;
 }
@@ -1369,7 +1375,13 @@ int l3d_stereo_autotune(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
     }
     const bool six_only = s->opts.form == L3D_FORM_EXACT || s->opts.compensated || !s->pairs ||
                           (s->variant & 16);
-    const std::vector<int> candidates = six_only ? std::vector<int>{6, 14} : std::vector<int>{6, 14, 4, 12};
+    /* +32 (the window in shared memory) is a fast-form option; BF16 returned above */
+    const bool shwin = s->opts.form == L3D_FORM_FAST;
+    std::vector<int> candidates = six_only ? std::vector<int>{6, 14} : std::vector<int>{6, 14, 4, 12};
+    if (shwin) {
+        candidates.push_back(6 | 32);
+        candidates.push_back(14 | 32);
+    }
     /* up to three iterations: the first propagates random planes, the later ones the converging
      * planes whose neighbouring pixels agree, and the variants rank differently on the two */
     std::vector<l3d_solve_opts> one(opts, opts + n_refs);

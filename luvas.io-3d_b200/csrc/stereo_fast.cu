@@ -36,6 +36,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include <cuda_fp16.h>
 
 #include "l3d_fmath.h"
@@ -48,6 +50,15 @@ constexpr int TY = 8;    /* rows per tile */
 constexpr int S = 36;    /* 6 x 6 window, offsets -5, -3, ..., 5 */
 #ifndef L3D_EXACT_MIN_BLOCKS
 #define L3D_EXACT_MIN_BLOCKS 5 /* resident blocks per SM of the exact propagate kernel (5: 81 M px-iters/s on the scan, 4: 72 M) */
+#endif
+/* Resident blocks per SM of the fast propagate kernel with the window in shared memory, with
+ * gathers (4: 168.9 M px-iters/s on the scan with FP32 texels, 5: 166.8 M) and with filtered
+ * samples (5: 249.7 M with FP16 texels, 4: 248.0 M). */
+#ifndef L3D_SHWIN_GATHER_MIN_BLOCKS
+#define L3D_SHWIN_GATHER_MIN_BLOCKS 4
+#endif
+#ifndef L3D_SHWIN_MIN_BLOCKS
+#define L3D_SHWIN_MIN_BLOCKS 5
 #endif
 
 __device__ __forceinline__ float rcp_fast(float x) {
@@ -332,6 +343,16 @@ __device__ __forceinline__ float hyp_cost(const E& e, const L3dFastView& v, cons
     return total / (float)kk;
 }
 
+/* This thread's window column in shared memory: element i (sample i's pair of window values)
+ * at [i * XBLOCK]; consecutive threads read consecutive float2, so a warp's access is
+ * conflict-free.  The exact evaluator keeps (w, r) there, the fast evaluator with a shared
+ * window (w, w (r - c)). */
+constexpr int XBLOCK = 128;
+__device__ __forceinline__ float2* exact_window() {
+    __shared__ float2 win[S * XBLOCK];
+    return win + threadIdx.x;
+}
+
 /* Per-pixel state: the reference window as w and w (r - c), c = centre pixel. */
 struct FPix {
     float rw[S], rwr[S];
@@ -341,14 +362,26 @@ struct FPix {
     float3 ray;
 };
 
+/* The same without the window, which lives in shared memory (exact_window). */
+struct FPixS {
+    float center, inv_sum, mean_r, var_r;
+    uint32_t rng;
+    float px, py;
+    float3 ray;
+};
+
 /* TEX: texture-unit sampling of F16/F32 arrays (false: BF16 linear memory).  TEXROWS: window
  * rows (of 6) sampled by the texture unit; the other rows use pair_sample (TEX only).  COMP:
  * compensated window sums.  GATHER: the texture rows are texture gathers weighted with exact
- * FP32 bilinear weights instead of hardware-filtered fetches (8-bit weights). */
-template <bool TEX, int TEXROWS = 6, bool COMP = false, bool GATHER = false>
+ * FP32 bilinear weights instead of hardware-filtered fetches (8-bit weights).  SHWIN: the
+ * reference window lives in shared memory instead of 72 registers, so that more warps are
+ * resident to cover the texture latency; the arithmetic, and so every result, is unchanged. */
+template <bool TEX, int TEXROWS = 6, bool COMP = false, bool GATHER = false, bool SHWIN = false>
 struct Fast {
-    using Pix = FPix;
-    static constexpr int kMinBlocks = 3;  /* resident blocks per SM the propagate kernel targets */
+    using Pix = typename std::conditional<SHWIN, FPixS, FPix>::type;
+    /* resident blocks per SM the propagate kernel targets */
+    static constexpr int kMinBlocks =
+        SHWIN ? (GATHER ? L3D_SHWIN_GATHER_MIN_BLOCKS : L3D_SHWIN_MIN_BLOCKS) : 3;
     const L3dFastView& v;
     const L3dFastDev& d;
     __device__ Fast(const L3dFastView& view, const L3dFastDev& dev) : v(view), d(dev) {}
@@ -364,10 +397,10 @@ struct Fast {
         return make_float3((x - v.k[2]) / v.k[0], (y - v.k[3]) / v.k[1], 1.0f);
     }
 
-    __device__ float random(FPix& s) const { return l3d_random(&s.rng); }
+    __device__ float random(Pix& s) const { return l3d_random(&s.rng); }
 
     /* prepare_window (patchmatch.wgsl.ts:90-110), shifted by the centre pixel */
-    __device__ void prepare(FPix& s, int x, int y) const {
+    __device__ void prepare(Pix& s, int x, int y) const {
         const uint16_t* ri = img(v.ref_img_off);
         const float center = Img<TEX>::texel(v.ref_tex, ri, v.W, v.H, x, y);
         const float ic1 = 1.0f / (2.0f * 0.06f * 0.06f);
@@ -379,8 +412,12 @@ struct Fast {
             float val = Img<TEX>::texel(v.ref_tex, ri, v.W, v.H, x + ox, y + oy);
             float dc = val - center;
             float w = __expf(-(dc * dc) * ic1 - spatial);
-            s.rw[i] = w;
-            s.rwr[i] = w * dc;
+            if constexpr (SHWIN) {
+                exact_window()[i * XBLOCK] = make_float2(w, w * dc);
+            } else {
+                s.rw[i] = w;
+                s.rwr[i] = w * dc;
+            }
             sw.add(w);
             sr.fma_add(w, dc);
             srr.fma_add(w * dc, dc);
@@ -391,8 +428,18 @@ struct Fast {
         s.var_r = fmaxf(fmaf(-s.mean_r, s.mean_r, srr.value() * s.inv_sum), 0.0f);
     }
 
+    /* one sample's terms of the window sums: w s', s' and (w r') s' (s' = s - c, r' = r - c) */
+    static __device__ __forceinline__ void window_term(WinSums<COMP>& ws, const Pix& s, int i, float sv) {
+        if constexpr (SHWIN) {
+            const float2 w = exact_window()[i * XBLOCK];
+            ws.term(w.x * sv, sv, w.y);
+        } else {
+            ws.term(s.rw[i] * sv, sv, s.rwr[i]);
+        }
+    }
+
     /* view_cost (patchmatch.wgsl.ts:130-159) with H = Bt + ktt u^T. */
-    __device__ float view_cost(const FPix& s, const L3dFastSrc& src, const float* u) const {
+    __device__ float view_cost(const Pix& s, const L3dFastSrc& src, const float* u) const {
         float h[9];
 #pragma unroll
         for (int r = 0; r < 3; r++)
@@ -435,7 +482,7 @@ struct Fast {
                 float val = GATHER ? bilinear_gather(src.tex, fmaf(qx, iz, -0.5f), fmaf(qy, iz, -0.5f))
                                    : Img<TEX>::sample(src.tex, si, src.W, src.H, qx * iz, qy * iz);
                 float sv = val - s.center;  /* s' = s - c; r' = r - c lives in rwr / rw */
-                ws.term(s.rw[i] * sv, sv, s.rwr[i]);
+                window_term(ws, s, i, sv);
                 qx += dxx;
                 qy += dxy;
                 qz += dxz;
@@ -456,7 +503,7 @@ struct Fast {
                     float iz = rcp_fast(qz);
                     float val = pair_sample(sp, src.W, src.H, qx * iz, qy * iz);
                     float sv = val - s.center;
-                    ws.term(s.rw[i] * sv, sv, s.rwr[i]);
+                    window_term(ws, s, i, sv);
                     qx += dxx;
                     qy += dxy;
                     qz += dxz;
@@ -476,12 +523,12 @@ struct Fast {
     }
 
     /* hypothesis_cost (patchmatch.wgsl.ts:192-233) */
-    __device__ float hypothesis_cost(const FPix& s, float3 n, float dd) const {
+    __device__ float hypothesis_cost(const Pix& s, float3 n, float dd) const {
         return hyp_cost(*this, v, d, s, n, dd);
     }
 
     /* random_normal, random_depth (patchmatch.wgsl.ts:235-249) */
-    __device__ float3 random_normal(FPix& s) const {
+    __device__ float3 random_normal(Pix& s) const {
         float z = fmaf(random(s), 2.0f, -1.0f);
         float a = random(s) * 6.2831853f;
         float r = sqrtf(fmaxf(0.0f, fmaf(-z, z, 1.0f)));
@@ -493,12 +540,12 @@ struct Fast {
         return normalize_fast(make_float3(fmaf(view.x, -0.5f, n.x), fmaf(view.y, -0.5f, n.y),
                                           fmaf(view.z, -0.5f, n.z)));
     }
-    __device__ float random_depth(FPix& s) const {
+    __device__ float random_depth(Pix& s) const {
         float t = random(s);
         return 1.0f / fmaf(v.range[0], t, v.range[1] * (1.0f - t));
     }
 
-    __device__ void begin(FPix& s, int x, int y, int iteration, int phase) const {
+    __device__ void begin(Pix& s, int x, int y, int iteration, int phase) const {
         s.px = (float)x;
         s.py = (float)y;
         uint32_t seed = (uint32_t)(v.ref + 1) * 0x9e3779b1u + (uint32_t)iteration * 97u +
@@ -520,14 +567,6 @@ struct XPix {
     float px, py;
     float3 ray;
 };
-
-/* This thread's window column: element i (sample i's (w, v)) at [i * XBLOCK]; consecutive
- * threads read consecutive float2, so a warp's access is conflict-free. */
-constexpr int XBLOCK = 128;
-__device__ __forceinline__ float2* exact_window() {
-    __shared__ float2 win[S * XBLOCK];
-    return win + threadIdx.x;
-}
 
 /* The plain form's arithmetic in the batched kernels (see the file header).  COMP: Neumaier-
  * compensated window sums (the oracle's compensated mode). */
@@ -944,8 +983,9 @@ cudaError_t l3d_launch_make_pairs(const void* img, int storage, int W, int H, ui
     return cudaGetLastError();
 }
 
-/* variant = texture rows (6, 4, 3, 2; the exact evaluator, compensated sums and gathers take 6
- * only) + 8 x quad mapping + 16 x texture gathers with exact weights (fast evaluator, F16/F32). */
+/* variant = texture rows (6, 4, 3, 2; the exact evaluator, compensated sums, gathers and the
+ * shared window take 6 only) + 8 x quad mapping + 16 x texture gathers with exact weights (fast
+ * evaluator, F16/F32/U8) + 32 x the reference window in shared memory (fast evaluator). */
 cudaError_t l3d_launch_fast(int kernel, const L3dFastDev& d, int iteration, int phase, int variant,
                             cudaStream_t stream) {
     if (d.total_tiles <= 0) return cudaSuccess;
@@ -962,6 +1002,19 @@ cudaError_t l3d_launch_fast(int kernel, const L3dFastDev& d, int iteration, int 
     if (d.storage == 3) { /* BF16 is sampled from linear memory */
         if (d.comp) return launch_eval<Fast<false, 6, true>, false>(kernel, d, iteration, phase, stream);
         return launch_eval<Fast<false, 6, false>, false>(kernel, d, iteration, phase, stream);
+    }
+    if (variant & 32) { /* the reference window in shared memory (six texture rows) */
+        if (rows != 6) return cudaErrorInvalidValue;
+        switch ((d.comp ? 1 : 0) + ((variant & 16) ? 2 : 0) + (quad ? 4 : 0)) {
+            case 0: return launch_eval<Fast<true, 6, false, false, true>, false>(kernel, d, iteration, phase, stream);
+            case 1: return launch_eval<Fast<true, 6, true, false, true>, false>(kernel, d, iteration, phase, stream);
+            case 2: return launch_eval<Fast<true, 6, false, true, true>, false>(kernel, d, iteration, phase, stream);
+            case 3: return launch_eval<Fast<true, 6, true, true, true>, false>(kernel, d, iteration, phase, stream);
+            case 4: return launch_eval<Fast<true, 6, false, false, true>, true>(kernel, d, iteration, phase, stream);
+            case 5: return launch_eval<Fast<true, 6, true, false, true>, true>(kernel, d, iteration, phase, stream);
+            case 6: return launch_eval<Fast<true, 6, false, true, true>, true>(kernel, d, iteration, phase, stream);
+            default: return launch_eval<Fast<true, 6, true, true, true>, true>(kernel, d, iteration, phase, stream);
+        }
     }
     if (variant & 16) { /* texture gathers with exact weights */
         if (rows != 6) return cudaErrorInvalidValue;

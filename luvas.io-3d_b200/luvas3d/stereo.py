@@ -280,7 +280,8 @@ class DenseStereo:
 
     @property
     def variant(self) -> int:
-        """Fast-form kernel variant: texture-sampled window rows + 8 x quad lane mapping."""
+        """Batched-form kernel variant: texture-sampled window rows + 8 x quad lane mapping
+        + 16 x texture gathers with exact weights + 32 x the window in shared memory."""
         return int(self._lib.l3d_stereo_variant(self._h()))
 
     @variant.setter
@@ -288,7 +289,7 @@ class DenseStereo:
         _lib.check(self._lib.l3d_stereo_set_variant(self._h(), int(v)))
 
     def autotune(self, refs: Sequence[int], options: Sequence[SolveOptions]) -> tuple[int, float]:
-        """Times each fast-form variant on one iteration of this batch; keeps the fastest."""
+        """Times each variant on up to three iterations of this batch; keeps the fastest."""
         args = [_SolveArgs(o, int(np.prod(self.shape(r)))) for r, o in zip(refs, options)]
         arr = (_lib.SolveOpts * len(args))(*[a.c for a in args])
         crefs = (C.c_int32 * len(refs))(*[int(r) for r in refs])

@@ -106,12 +106,37 @@ def test_every_variant_keeps_accuracy(arc, variant):
     assert np.percentile(np.abs(got[valid] - want[valid]), 99) < 5e-3
 
 
+@pytest.mark.parametrize("storage,compensated,variant", [
+    (DTYPE_F16, False, 14), (DTYPE_F16, False, 6), (DTYPE_F32, False, 30), (DTYPE_F32, True, 30),
+    (DTYPE_F16, True, 14), (DTYPE_U8, False, 14)])
+def test_shared_window_equals_register_window(arc, storage, compensated, variant):
+    """+32 keeps the reference window in shared memory instead of registers; the arithmetic is the
+    same, so a solve (init and every propagate colour) equals the register variant bit for bit."""
+    views, imgs, truth, srcs = arc
+    W, H = 256, 192
+    out = []
+    for v in (variant, variant | 32):
+        s = DenseStereo(W, H, views, StereoOptions(form=FORM_FAST, storage=storage,
+                                                   compensated=compensated))
+        for i, im in enumerate(imgs):
+            s.set_image(i, np.asarray(im, dtype=np.float32))
+        s.variant = v
+        assert s.variant == v
+        s.solve_all([1, 2, 3], [SolveOptions(srcs[r], 0.5, 5.0, iterations=3) for r in (1, 2, 3)])
+        out.append([a for r in (1, 2, 3) for a in s.read_hypotheses_layer(r)])
+    for i, (a, b) in enumerate(zip(*out)):
+        assert_bit_equal(b, a, f"view {i // 2 + 1} {'cost' if i % 2 else 'hypotheses'}")
+
+
 def test_variant_validation(arc):
     views, imgs, truth, srcs = arc
     fast = make(views, imgs, 256, 192)
-    for bad in (5, 1, 7, 16, -1):
+    for bad in (5, 1, 7, 16, -1, 36, 44, 64, 128):
         with pytest.raises(L3dError):
             fast.variant = bad
+    bf16 = make(views, imgs, 256, 192, storage=DTYPE_BF16)
+    with pytest.raises(L3dError):
+        bf16.variant = 46
     plain = make(views, imgs, 256, 192, form=FORM_PLAIN, storage=DTYPE_F32)
     with pytest.raises(L3dError):
         plain.variant = 6
