@@ -32,6 +32,9 @@
 extern "C" {
 #endif
 
+/* Version of the structures and calls below.  2: l3d_stereo_opts gained `compensated` (its size
+ * changed, so a host built against version 1 must be rebuilt), L3D_FORM_EXACT, variant bits 16
+ * and 32, l3d_tsdf_integrate_layer, l3d_tsdf_count_updates and l3d_measure_fetch_rate. */
 #define L3D_ABI_VERSION 2
 
 /* Status codes. */
@@ -95,7 +98,7 @@ typedef struct {
                                  solves; it must outlive this handle.  NULL = none */
     int32_t depth_maps;       /* 1: a packed depth map per view (default); 0: one map */
     int32_t storage;          /* device image storage: F32 (plain form); U8, F16, BF16 or F32 (fast) */
-    int32_t form;             /* L3D_FORM_PLAIN or L3D_FORM_FAST */
+    int32_t form;             /* L3D_FORM_PLAIN, L3D_FORM_FAST or L3D_FORM_EXACT */
     int32_t window;           /* samples per window side: 6 (reference, offsets +-1,3,5) or 11 */
     int32_t dilation;         /* spacing of window samples: 2 (reference) or 1 */
     void* stream;             /* cudaStream_t to run on, or NULL to create one */

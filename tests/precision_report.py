@@ -40,6 +40,7 @@ def _forms():
         ("fast f32 comp", FORM_FAST, DTYPE_F32, True, 14),
         ("fast f32 gather", FORM_FAST, DTYPE_F32, False, 30),
         ("fast f32 gather comp", FORM_FAST, DTYPE_F32, True, 30),
+        ("fast f32 gather shared", FORM_FAST, DTYPE_F32, False, 62),
         ("fast f16", FORM_FAST, DTYPE_F16, False, 14),
         ("fast f16 comp", FORM_FAST, DTYPE_F16, True, 14),
         ("fast f16 gather", FORM_FAST, DTYPE_F16, False, 30),

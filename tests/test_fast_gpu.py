@@ -78,10 +78,11 @@ def test_fast_depth_accuracy_matches_plain(arc, storage):
     assert abs(vp - vf) < 0.05
 
 
-@pytest.mark.parametrize("variant", [6, 14, 4, 12, 3, 11, 2, 10])
+@pytest.mark.parametrize("variant", [6, 14, 4, 12, 3, 11, 2, 10, 38, 46])
 def test_every_variant_keeps_accuracy(arc, variant):
     """Kernel variants split the window rows between the texture unit and software bilinear on
-    the LSU path, and map hardware quads to rows or 2x2 blocks; accuracy must not change."""
+    the LSU path, map hardware quads to rows or 2x2 blocks and keep the window in shared memory
+    (+32); accuracy must not change."""
     views, imgs, truth, srcs = arc
     W, H = 256, 192
     plain = make(views, imgs, W, H, form=FORM_PLAIN, storage=DTYPE_F32)
@@ -131,7 +132,7 @@ def test_shared_window_equals_register_window(arc, storage, compensated, variant
 def test_variant_validation(arc):
     views, imgs, truth, srcs = arc
     fast = make(views, imgs, 256, 192)
-    for bad in (5, 1, 7, 16, -1, 36, 44, 64, 128):
+    for bad in (5, 1, 7, 16, -1, 36, 44, 64, 110, 128):
         with pytest.raises(L3dError):
             fast.variant = bad
     bf16 = make(views, imgs, 256, 192, storage=DTYPE_BF16)
@@ -222,4 +223,4 @@ def test_autotune_picks_a_valid_variant(arc):
     s = make(views, imgs, 256, 192)
     opts = [SolveOptions(srcs[r], 0.5, 5.0, iterations=3) for r in range(5)]
     best, ms = s.autotune(list(range(5)), opts)
-    assert best in (6, 14, 4, 12) and s.variant == best and ms > 0
+    assert best in (6, 14, 4, 12, 38, 46) and s.variant == best and ms > 0

@@ -26,6 +26,7 @@ FLOORS = {
     "exact f32 comp": {"small": (0.998, 1e-4), "scan4": (0.995, 1e-4)},
     "fast f32 gather": {"small": (0.998, 1e-4), "scan4": (0.995, 1e-4)},
     "fast f32 gather comp": {"small": (0.998, 1e-4), "scan4": (0.995, 1e-4)},
+    "fast f32 gather shared": {"small": (0.998, 1e-4), "scan4": (0.995, 1e-4)},
     "fast f32": {"small": (0.98, 5e-4), "scan4": (0.97, 5e-4)},
     "fast f16": {"small": (0.94, 3e-3), "scan4": (0.92, 3e-3)},
     "fast f16 comp": {"small": (0.94, 3e-3), "scan4": (0.92, 3e-3)},
@@ -46,6 +47,14 @@ def test_form_against_fp64_oracle(rep, form):
     depth_floor, cost_p99 = FLOORS[form][workload]
     assert r["depth_rel_vs_fp64_solve"]["within_0.001"] >= depth_floor, r["depth_rel_vs_fp64_solve"]
     assert r["plane_cost_abs_vs_fp64"]["p99"] <= cost_p99, r["plane_cost_abs_vs_fp64"]
+
+
+def test_shared_window_equals_register_window(rep):
+    """+32 moves the window to shared memory without changing any arithmetic."""
+    workload, r = rep
+    a, b = dict(r["forms"]["fast f32 gather shared"]), dict(r["forms"]["fast f32 gather"])
+    a.pop("variant"), b.pop("variant")
+    assert a == b
 
 
 def test_exact_form_equals_plain_form(rep):
