@@ -871,7 +871,7 @@ def run_scan(args) -> None:
     # ---- TSDF: the sweep of the step, and the reference's one-view-per-launch form ---------
     stereo.solve_all(refs, opts)
     stereo.filter_all(refs, w.sources, w.needed)
-    visible, updates = tsdf.count_updates(iviews, stereo=stereo, layers=refs)
+    visible, updates, kept = tsdf.count_updates(iviews, stereo=stereo, layers=refs)
     pv = []
     for i in range(4):
         tsdf.reset()
@@ -891,19 +891,25 @@ def run_scan(args) -> None:
                  "peak_source": peak_kind, "bytes_per_launch": vox * 12,
                  "bytes_model": "12 B per voxel per sweep (f32 tsdf and Q8.8 weight, read and written)",
                  "voxel_updates": updates, "visible_voxel_views": visible,
-                 "launch_ms": sweep_ms,
+                 "depth_kept_voxel_views": kept, "launch_ms": sweep_ms,
                  # the one-view-per-pass form moves 12 B per voxel-update it applies; the sweep's
                  # time against those bytes is its HBM-equivalent rate
                  "per_view_form_equivalent_frac": updates * 12 / (sweep_ms / 1e3) / 1e9 / hbm}
     roof_tsdf["frac"] = roof_tsdf["achieved"] / hbm
-    roof_tsdf_view = {"kernel": f"k_integrate ({V} launches, one view each)", "bound": "hbm",
+    roof_tsdf_view = {"kernel": f"k_integrate_list ({V} launches, one view each)", "bound": "hbm",
                       "achieved": updates * 12 / (per_view_ms / 1e3) / 1e9, "peak": hbm,
                       "unit": "GB/s", "peak_source": peak_kind, "traffic": None,
                       "bytes_model": "12 B per voxel-update applied (f32 tsdf and Q8.8 weight, "
                                      "read and written), counted by l3d_tsdf_count_updates",
                       "bytes_per_step": updates * 12, "voxel_updates": updates,
-                      "visible_voxel_views": visible, "ms_per_step": per_view_ms,
-                      "voxel_updates_per_s": vox * V / (per_view_ms / 1e3)}
+                      "visible_voxel_views": visible, "depth_kept_voxel_views": kept,
+                      "ms_per_step": per_view_ms,
+                      "voxel_updates_per_s": vox * V / (per_view_ms / 1e3),
+                      # 12 B per voxel of every brick a launch visits (the bricks visibleBricks
+                      # and the depth-aware cull keep): the bytes a form that streams whole kept
+                      # bricks would move
+                      "kept_brick_bytes_per_step": kept * 12,
+                      "kept_brick_frac": kept * 12 / (per_view_ms / 1e3) / 1e9 / hbm}
     roof_tsdf_view["frac"] = roof_tsdf_view["achieved"] / hbm
 
     # ---- end to end through the C ABI with pinned host buffers ------------------------------

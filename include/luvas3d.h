@@ -292,12 +292,14 @@ int l3d_tsdf_integrate_layer(l3d_tsdf* t, const l3d_stereo* src, int32_t layer,
 
 /* The work of integrating n depth maps (arguments as for l3d_tsdf_integrate_many) without doing
  * it: *visible receives the voxel-views that visibleBricks keeps, *updates the voxel-updates the
- * integration applies (the voxels a view's depth sample updates).  12 bytes per update (f32 tsdf
- * and Q8.8 weight read and written) are the algorithmic bytes of the one-view-per-pass form.
- * Synchronises.  No reference counterpart. */
+ * integration applies (the voxels a view's depth sample updates), and *kept (may be NULL) the
+ * voxel-views of the bricks the depth-aware cull keeps as well (a brick entirely behind the
+ * truncation band of its view's depths is dropped; the call fails if that cull would drop an
+ * update).  12 bytes per update (f32 tsdf and Q8.8 weight read and written) are the algorithmic
+ * bytes of the one-view-per-pass form.  Synchronises.  No reference counterpart. */
 int l3d_tsdf_count_updates(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
                            const uint32_t* packed, int32_t n, const l3d_integration_view* views,
-                           int64_t* visible, int64_t* updates);
+                           int64_t* visible, int64_t* updates, int64_t* kept);
 
 /* Integrates n depth maps in one sweep over the volume (each voxel read and written once);
  * equal, bit for bit, to n integrate() calls in order.  Maps come from src's filtered_all

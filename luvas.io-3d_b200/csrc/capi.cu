@@ -1492,6 +1492,8 @@ struct l3d_tsdf {
     float4* normals = nullptr;        /* decoded normal per 12-bit normal code */
     float* tiles = nullptr;           /* depth tiles of the depth-aware brick cull, tile_cap */
     int32_t* list = nullptr;          /* 1 + bricks: kept bricks of a one-view integration */
+    uint32_t* sweep = nullptr;        /* the sweep's brick list: flags, prefix (bricks + 1 each),
+                                         list (bricks), scan scratch */
     long long tile_cap = 0;
     L3dTsdfView* views_host = nullptr;      /* pinned staging for views */
     const uint32_t** ptrs_host = nullptr;   /* pinned staging for depth pointers */
@@ -1547,6 +1549,20 @@ int ensure_tiles(l3d_tsdf* t, long long n) {
     t->tile_cap = n;
     return L3D_OK;
 }
+
+/* The sweep's list of the bricks some view keeps (allocated once: its size is the grid's). */
+long long sweep_words(const l3d_tsdf* t) {
+    return 3 * (t->g.bricks + 1) + (long long)((l3d_scan_scratch(t->g.bricks + 1) + 3) / 4);
+}
+int ensure_sweep(l3d_tsdf* t) {
+    if (t->sweep || t->g.bricks == 0) return L3D_OK;
+    L3D_CUDA(cudaMalloc(&t->sweep, (size_t)sweep_words(t) * 4), "sweep brick list");
+    return L3D_OK;
+}
+uint32_t* sweep_flags(l3d_tsdf* t) { return t->sweep; }
+uint32_t* sweep_prefix(l3d_tsdf* t) { return t->sweep + (t->g.bricks + 1); }
+int32_t* sweep_list(l3d_tsdf* t) { return (int32_t*)(t->sweep + 2 * (t->g.bricks + 1)); }
+uint32_t* sweep_scratch(l3d_tsdf* t) { return t->sweep + 3 * (t->g.bricks + 1); }
 
 /* Upload buffers, sized in elements (u32 maps / f32 priors). */
 int ensure_maps(l3d_tsdf* t, long long elems) {
@@ -1763,8 +1779,8 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
                 L3D_CUDA(cudaMemcpyAsync(t->priors + poff[i], views[i].prior, (size_t)mw[i] * mh[i] * 4,
                                          cudaMemcpyHostToDevice, t->stream), "prior upload");
     }
-    /* depth tiles per view for the depth-aware brick cull (integration only: the update count
-     * reports what visibleBricks alone keeps) */
+    /* depth tiles per view for the depth-aware brick cull (the update count reports what
+     * visibleBricks alone keeps, and what the depth-aware cull keeps of it) */
     std::vector<long long> toff(n);
     long long ttotal = 0, tmax = 0;
     for (int i = 0; i < n; i++) {
@@ -1773,7 +1789,7 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
         ttotal += nt;
         tmax = std::max(tmax, nt);
     }
-    if (!counts_out && (rc = ensure_tiles(t, ttotal))) return rc;
+    if ((rc = ensure_tiles(t, ttotal)) || (!counts_out && (rc = ensure_sweep(t)))) return rc;
     /* the pinned staging tables are reused: wait until the previous call's copies have run */
     L3D_CUDA(cudaEventSynchronize(t->staged), "staging wait");
     for (int i = 0; i < n; i++) {
@@ -1789,32 +1805,51 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
     L3D_CUDA(cudaEventRecord(t->staged, t->stream), "event record");
     cudaError_t e;
     if (counts_out) {
-        e = l3d_launch_tsdf_visible(t->g, t->views, n, t->coords, t->mask, t->stream);
-        t->launches++;
-    } else {
-        e = l3d_launch_depth_tiles(t->views, n, t->depth_ptrs, t->priors, t->tiles, tmax, t->stream);
+        /* visibleBricks alone: visible voxel-views and updates; then the depth-aware mask: the
+         * voxel-views it keeps (the updates are the same, which the count checks) */
+        unsigned long long* counts = nullptr;
+        unsigned long long host[4] = {0, 0, 0, 0};
+        L3D_CUDA(pool_alloc((void**)&counts, 4 * sizeof(unsigned long long), t->stream), "count buffer");
+        e = cudaMemsetAsync(counts, 0, 4 * sizeof(unsigned long long), t->stream);
+        if (e == cudaSuccess) e = l3d_launch_tsdf_visible(t->g, t->views, n, t->coords, t->mask, t->stream);
+        if (e == cudaSuccess)
+            e = l3d_launch_tsdf_count(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
+                                      t->normals, counts, t->stream);
+        if (e == cudaSuccess)
+            e = l3d_launch_depth_tiles(t->views, n, t->depth_ptrs, t->priors, t->tiles, tmax, t->stream);
         if (e == cudaSuccess)
             e = l3d_launch_tsdf_visible_depth(t->g, t->views, n, t->coords, t->tiles, t->mask, t->stream);
-        t->launches += 2;
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "visibility launch");
-    if (counts_out) {
-        unsigned long long* counts = nullptr;
-        unsigned long long host[2] = {0, 0};
-        L3D_CUDA(pool_alloc((void**)&counts, 2 * sizeof(unsigned long long), t->stream), "count buffer");
-        if ((e = cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), t->stream)) == cudaSuccess &&
-            (e = l3d_launch_tsdf_count(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
-                                       t->normals, counts, t->stream)) == cudaSuccess &&
-            (e = cudaMemcpyAsync(host, counts, sizeof(host), cudaMemcpyDeviceToHost, t->stream)) == cudaSuccess)
-            e = cudaStreamSynchronize(t->stream);
-        t->launches++;
+        if (e == cudaSuccess)
+            e = l3d_launch_tsdf_count(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
+                                      t->normals, counts + 2, t->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host, counts, sizeof(host), cudaMemcpyDeviceToHost, t->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+        t->launches += 5;
         cudaFreeAsync(counts, t->stream);
         if (e != cudaSuccess) return cuda_fail(e, "update count");
+        if (host[3] != host[1])
+            return fail(L3D_ECUDA, "update count: the depth-aware cull dropped %llu updates",
+                        (unsigned long long)(host[1] - host[3]));
         counts_out[0] = (int64_t)host[0];
         counts_out[1] = (int64_t)host[1];
-    } else if (!tsdf_out && !weight_out) {
-        e = l3d_launch_tsdf_many(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
-                                 t->normals, t->tsdf, t->weight, t->q8, t->stream);
+        counts_out[2] = (int64_t)host[2];
+        if (src && (rc = before_stereo(t, src))) return rc;
+        return L3D_OK;
+    }
+    e = l3d_launch_depth_tiles(t->views, n, t->depth_ptrs, t->priors, t->tiles, tmax, t->stream);
+    if (e == cudaSuccess)
+        e = l3d_launch_tsdf_visible_depth(t->g, t->views, n, t->coords, t->tiles, t->mask, t->stream);
+    /* the sweep visits only the bricks some view keeps */
+    if (e == cudaSuccess)
+        e = l3d_launch_tsdf_brick_list(t->g, n, t->mask, sweep_flags(t), sweep_prefix(t), sweep_list(t),
+                                       sweep_scratch(t), t->stream);
+    t->launches += 4 + l3d_scan_launches(t->g.bricks + 1, false);
+    if (e != cudaSuccess) return cuda_fail(e, "visibility launch");
+    if (!tsdf_out && !weight_out) {
+        e = l3d_launch_tsdf_many_list(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
+                                      t->normals, t->tsdf, t->weight, t->q8, sweep_prefix(t),
+                                      sweep_list(t), 0, l3d_tsdf_sweep_units(t->g, nullptr, nullptr),
+                                      t->stream);
         t->launches++;
         if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
     } else {
@@ -1833,9 +1868,9 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
         for (int i = 0; i < L3D_TSDF_READ_SLABS; i++) {
             const long long q0 = std::min(layers, i * per) * lu;
             const long long q1 = std::min(layers, i * per + per) * lu;
-            e = l3d_launch_tsdf_many_range(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs,
-                                           t->priors, t->normals, t->tsdf, t->weight, t->q8, q0, q1,
-                                           t->stream);
+            e = l3d_launch_tsdf_many_list(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs,
+                                          t->priors, t->normals, t->tsdf, t->weight, t->q8,
+                                          sweep_prefix(t), sweep_list(t), q0, q1, t->stream);
             t->launches += q1 > q0 ? 1 : 0;
             if (e != cudaSuccess) return cuda_fail(e, "integrate launch");
             L3D_CUDA(cudaEventRecord(t->slab_done[i], t->stream), "event record");
@@ -1862,12 +1897,13 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
 
 int l3d_tsdf_count_updates(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
                            const uint32_t* packed, int32_t n, const l3d_integration_view* views,
-                           int64_t* visible, int64_t* updates) {
+                           int64_t* visible, int64_t* updates, int64_t* kept) {
     if (!visible || !updates) return fail(L3D_EINVAL, "visible and updates must not be NULL");
-    int64_t c[2] = {0, 0};
+    int64_t c[3] = {0, 0, 0};
     int rc = integrate_many(t, src, layers, packed, n, views, nullptr, nullptr, c);
     *visible = c[0];
     *updates = c[1];
+    if (kept) *kept = c[2];
     return rc;
 }
 
@@ -1990,6 +2026,7 @@ void l3d_tsdf_destroy(l3d_tsdf* t) {
     cudaFree(t->normals);
     cudaFree(t->tiles);
     cudaFree(t->list);
+    cudaFree(t->sweep);
     cudaFreeHost(t->views_host);
     cudaFreeHost(t->ptrs_host);
     if (t->done) cudaEventDestroy(t->done);

@@ -216,6 +216,19 @@ cudaError_t l3d_launch_tsdf_count(const L3dTsdfGrid& g, const L3dTsdfView* views
                                   cudaStream_t stream);
 /* normals[code] = unpack_normal(code << 16) for the 4096 normal codes */
 cudaError_t l3d_launch_normal_table(float4* normals, cudaStream_t stream);
+/* The bricks some view keeps (a non-zero mask row), in ascending order: flags (bricks + 1),
+ * prefix (bricks + 1: prefix[b] = kept bricks below b, prefix[bricks] = their number), list
+ * (bricks), scratch of l3d_scan_scratch(bricks + 1) bytes. */
+cudaError_t l3d_launch_tsdf_brick_list(const L3dTsdfGrid& g, int n_views, const uint8_t* mask,
+                                      uint32_t* flags, uint32_t* prefix, int32_t* list,
+                                      uint32_t* scratch, cudaStream_t stream);
+/* The many-view sweep of quads [q_begin, q_end) (whole bricks) over the listed bricks only. */
+cudaError_t l3d_launch_tsdf_many_list(const L3dTsdfGrid& g, const L3dTsdfView* views_dev,
+                                      int n_views, const int32_t* coords, const uint8_t* mask,
+                                      const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                      const float4* normals, float* tsdf, void* weight, int q8,
+                                      const uint32_t* prefix, const int32_t* list,
+                                      long long q_begin, long long q_end, cudaStream_t stream);
 cudaError_t l3d_launch_tsdf_many(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
                                  const int32_t* coords, const uint8_t* mask,
                                  const uint32_t* const* depth_ptrs_dev, const float* priors,
@@ -336,6 +349,8 @@ cudaError_t l3d_launch_cloud_emit_sorted(const L3dCloudTable& t, unsigned total,
 
 /* Bytes of scratch l3d_scan_exclusive needs for n elements. */
 size_t l3d_scan_scratch(long long n);
+/* Kernel launches l3d_scan_exclusive makes for n elements (with or without `total`). */
+int l3d_scan_launches(long long n, bool total);
 /* out[i] = in[0] + ... + in[i-1] (in == out allowed); *total (device, may be NULL) = the sum. */
 cudaError_t l3d_scan_exclusive(const uint32_t* in, uint32_t* out, long long n, uint32_t* scratch,
                                uint32_t* total, cudaStream_t stream);

@@ -81,6 +81,13 @@ size_t l3d_scan_scratch(long long n) {
     return (words + 1) * sizeof(uint32_t);
 }
 
+int l3d_scan_launches(long long n, bool total) {
+    if (n <= 0) return 0;
+    int depth = 0;
+    for (long long m = n; blocks_of(m) > 1; m = blocks_of(m)) depth++;
+    return 1 + (depth + 1) + depth + (total ? 1 : 0);  /* last, block scans, add-backs, total */
+}
+
 cudaError_t l3d_scan_exclusive(const uint32_t* in, uint32_t* out, long long n, uint32_t* scratch,
                                uint32_t* total, cudaStream_t stream) {
     if (n <= 0) {

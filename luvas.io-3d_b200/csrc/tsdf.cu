@@ -540,20 +540,17 @@ __global__ void __launch_bounds__(256) k_integrate_list(const L3dTsdfGrid g, con
     }
 }
 
+/* One quad of the many-view sweep: its voxels stay in registers while every view that keeps
+ * its brick is applied in view order; written back once. */
 template <int VEC, bool Q8>
-__global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
-                                                        const L3dTsdfView* __restrict__ views,
-                                                        int n_views,
-                                                        const int32_t* __restrict__ coords,
-                                                        const uint8_t* __restrict__ mask,
-                                                        const uint32_t* const* __restrict__ depths,
-                                                        const float* __restrict__ priors,
-                                                        const float4* __restrict__ normals,
-                                                        float* __restrict__ tsdf,
-                                                        void* __restrict__ weight,
-                                                        long long q_begin, long long q_end) {
-    long long q = q_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= q_end) return;
+__device__ __forceinline__ void sweep_quad(const L3dTsdfGrid& g, const L3dTsdfView* __restrict__ views,
+                                           int n_views, const int32_t* __restrict__ coords,
+                                           const uint8_t* __restrict__ mask,
+                                           const uint32_t* const* __restrict__ depths,
+                                           const float* __restrict__ priors,
+                                           const float4* __restrict__ normals,
+                                           float* __restrict__ tsdf, void* __restrict__ weight,
+                                           long long q) {
     int gx, gy, gz;
     long long idx, brick;
     if (!quad_coords<VEC>(g, coords, q, &gx, &gy, &gz, &idx, &brick)) return;
@@ -637,6 +634,75 @@ __global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
         if (Q8) ((uint16_t*)weight)[idx] = (uint16_t)wq[0];
         else ((float*)weight)[idx] = wf[0];
     }
+}
+
+template <int VEC, bool Q8>
+__global__ void __launch_bounds__(256, 4) k_integrate_many(const L3dTsdfGrid g,
+                                                        const L3dTsdfView* __restrict__ views,
+                                                        int n_views,
+                                                        const int32_t* __restrict__ coords,
+                                                        const uint8_t* __restrict__ mask,
+                                                        const uint32_t* const* __restrict__ depths,
+                                                        const float* __restrict__ priors,
+                                                        const float4* __restrict__ normals,
+                                                        float* __restrict__ tsdf,
+                                                        void* __restrict__ weight,
+                                                        long long q_begin, long long q_end) {
+    const long long q = q_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= q_end) return;
+    sweep_quad<VEC, Q8>(g, views, n_views, coords, mask, depths, priors, normals, tsdf, weight, q);
+}
+
+/* The sweep over the bricks some view keeps: list holds them in ascending order
+ * (l3d_launch_tsdf_brick_list), prefix[b] is the number of kept bricks below brick b, so the
+ * kept bricks of [b_begin, b_end) are list[prefix[b_begin] .. prefix[b_end]).  A grid-stride
+ * loop over their quads; each quad is still one thread's, so results equal k_integrate_many's. */
+template <int VEC, bool Q8>
+__global__ void __launch_bounds__(256, 4) k_integrate_many_list(const L3dTsdfGrid g,
+                                                             const L3dTsdfView* __restrict__ views,
+                                                             int n_views,
+                                                             const int32_t* __restrict__ coords,
+                                                             const uint8_t* __restrict__ mask,
+                                                             const uint32_t* const* __restrict__ depths,
+                                                             const float* __restrict__ priors,
+                                                             const float4* __restrict__ normals,
+                                                             float* __restrict__ tsdf,
+                                                             void* __restrict__ weight,
+                                                             const uint32_t* __restrict__ prefix,
+                                                             const int32_t* __restrict__ list,
+                                                             long long b_begin, long long b_end) {
+    constexpr int PER = 512 / VEC;
+    const long long first = __ldg(prefix + b_begin);
+    const long long n = ((long long)__ldg(prefix + b_end) - first) * PER;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long b = __ldg(list + first + i / PER);
+        sweep_quad<VEC, Q8>(g, views, n_views, coords, mask, depths, priors, normals, tsdf, weight,
+                            b * PER + i % PER);
+    }
+}
+
+/* flags[b] = 1 if some view keeps brick b (its mask row is not all zero), for b < bricks;
+ * flags[bricks] = 0, so that an exclusive scan of bricks + 1 flags ends with the total. */
+__global__ void k_brick_any(const uint8_t* __restrict__ mask, int stride, long long bricks,
+                            uint32_t* __restrict__ flags) {
+    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > bricks) return;
+    uint32_t any = 0u;
+    if (b < bricks) {
+        const uint4* row = (const uint4*)(mask + b * stride);
+        for (int k = 0; k < stride / 16; k++) {
+            const uint4 m = __ldg(row + k);
+            any |= m.x | m.y | m.z | m.w;
+        }
+    }
+    flags[b] = any ? 1u : 0u;
+}
+
+__global__ void k_brick_list_fill(const uint32_t* __restrict__ flags, const uint32_t* __restrict__ prefix,
+                                  long long bricks, int32_t* __restrict__ list) {
+    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < bricks && flags[b]) list[prefix[b]] = (int32_t)b;
 }
 
 /* The work of a many-view integration without its writes: per voxel, the views whose brick
@@ -1003,6 +1069,45 @@ cudaError_t l3d_launch_tsdf_many_range(const L3dTsdfGrid& g, const L3dTsdfView* 
     } else {
         if (q8) k_integrate_many<1, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, q_begin, q_end);
         else k_integrate_many<1, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, q_begin, q_end);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_tsdf_brick_list(const L3dTsdfGrid& g, int n_views, const uint8_t* mask,
+                                      uint32_t* flags, uint32_t* prefix, int32_t* list,
+                                      uint32_t* scratch, cudaStream_t stream) {
+    if (g.bricks == 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((g.bricks + 1 + 255) / 256);
+    k_brick_any<<<blocks, 256, 0, stream>>>(mask, mask_stride(n_views), g.bricks, flags);
+    cudaError_t e = l3d_scan_exclusive(flags, prefix, g.bricks + 1, scratch, nullptr, stream);
+    if (e != cudaSuccess) return e;
+    k_brick_list_fill<<<blocks, 256, 0, stream>>>(flags, prefix, g.bricks, list);
+    return cudaGetLastError();
+}
+
+cudaError_t l3d_launch_tsdf_many_list(const L3dTsdfGrid& g, const L3dTsdfView* views_dev,
+                                      int n_views, const int32_t* coords, const uint8_t* mask,
+                                      const uint32_t* const* depth_ptrs_dev, const float* priors,
+                                      const float4* normals, float* tsdf, void* weight, int q8,
+                                      const uint32_t* prefix, const int32_t* list,
+                                      long long q_begin, long long q_end, cudaStream_t stream) {
+    const int vec = vec4_ok(g) ? 4 : 1;
+    const long long per = 512 / vec;
+    q_end = q_end < quad_count(g, vec) ? q_end : quad_count(g, vec);
+    if (q_end <= q_begin || n_views == 0) return cudaSuccess;
+    const long long b0 = q_begin / per, b1 = (q_end + per - 1) / per;
+    /* a grid-stride loop: four resident blocks per SM */
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        sms = 148;
+    const unsigned blocks = (unsigned)(4 * sms);
+    if (vec == 4) {
+        if (q8) k_integrate_many_list<4, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
+        else k_integrate_many_list<4, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
+    } else {
+        if (q8) k_integrate_many_list<1, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
+        else k_integrate_many_list<1, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
     }
     return cudaGetLastError();
 }

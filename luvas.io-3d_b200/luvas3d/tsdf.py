@@ -189,21 +189,22 @@ class TsdfVolume:
             self.synchronize()
 
     def count_updates(self, views: Sequence[IntegrationView], depths=None, stereo=None,
-                      layers: Sequence[int] | None = None) -> tuple[int, int]:
-        """(visible voxel-views, voxel-updates) that integrating these maps would apply."""
+                      layers: Sequence[int] | None = None) -> tuple[int, int, int]:
+        """(visible voxel-views, voxel-updates, voxel-views the depth-aware cull keeps) of
+        integrating these maps, without integrating them."""
         keep: list = []
         arr = (_lib.IntegrationView * len(views))(*[_c_view(v, keep) for v in views])
-        vis, upd = C.c_int64(), C.c_int64()
+        vis, upd, kept = C.c_int64(), C.c_int64(), C.c_int64()
         if stereo is not None:
             lay = np.asarray(layers if layers is not None else range(len(views)), dtype=np.int32)
             _lib.check(self._lib.l3d_tsdf_count_updates(
                 self._h(), stereo._h(), lay.ctypes.data_as(C.POINTER(C.c_int32)), None,
-                len(views), arr, C.byref(vis), C.byref(upd)))
+                len(views), arr, C.byref(vis), C.byref(upd), C.byref(kept)))
         else:
             p = np.ascontiguousarray(depths, dtype=np.uint32)
             _lib.check(self._lib.l3d_tsdf_count_updates(self._h(), None, None, _lib.ptr(p), len(views),
-                                                        arr, C.byref(vis), C.byref(upd)))
-        return int(vis.value), int(upd.value)
+                                                        arr, C.byref(vis), C.byref(upd), C.byref(kept)))
+        return int(vis.value), int(upd.value), int(kept.value)
 
     def integrate_many(self, views: Sequence[IntegrationView], depths=None, stereo=None,
                        layers: Sequence[int] | None = None) -> None:
