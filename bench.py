@@ -922,36 +922,50 @@ def run_scan(args) -> None:
         pinned = [torch.from_numpy(np.ascontiguousarray(im)).pin_memory() for im in w.images]
         out_f = torch.empty(w.pixels, dtype=torch.int32).pin_memory()
         f_off = np.concatenate([[0], np.cumsum([a * b for a, b in sizes])])
-        out_t = torch.empty(vox, dtype=torch.float32).pin_memory()
-        out_w = torch.empty(vox, dtype=torch.int16).pin_memory()
+        # two volumes and two pinned outputs: scan k's volume is read back while scan k + 1 runs
+        vols = [tsdf, TsdfVolume(max(s[0] for s in sizes), max(s[1] for s in sizes), w.tsdf_voxel,
+                                 w.tsdf_origin, dense=w.tsdf_dims, truncation=w.tsdf_truncation,
+                                 weight_q8=True, stream=sptr)]
+        outs = [(torch.empty(vox, dtype=torch.float32).pin_memory(),
+                 torch.empty(vox, dtype=torch.int16).pin_memory()) for _ in range(2)]
 
-        def e2e_step():
+        def e2e_step(k):
+            vol = vols[k % 2]
             for i, im in enumerate(pinned):
                 stereo.set_image_device(i, im.data_ptr(), DTYPE_F32)
             stereo.solve_all(refs, opts)
             stereo.filter_all(refs, w.sources, w.needed)
-            tsdf.reset()
+            vol.reset()  # queued after this volume's previous read-back (on the device)
             for r in refs:
                 _lib.check(lib.l3d_stereo_read_filtered_layer(
                     stereo._h(), r, C.c_void_p(out_f[int(f_off[r]):].data_ptr())))
-            # the sweep with the volume's read-back overlapped (l3d_tsdf_integrate_many_read)
-            tsdf.integrate_many_read(iviews, stereo=stereo, layers=refs, out=(out_t, out_w))
+            # the sweep, its read-back queued behind it on the volume's copy stream
+            # (l3d_tsdf_integrate_many_read_async); the host goes on to the next scan
+            vol.integrate_many_read(iviews, stereo=stereo, layers=refs, out=outs[k % 2], wait=False)
 
-        e2e_step()
+        for k in range(2):
+            e2e_step(k)
+        for v in vols:
+            v.wait_read()
         torch.cuda.synchronize()
         g = Stage(stream, ["e2e"])
         g.mark()
-        for _ in range(args.steps):
-            e2e_step()
+        for k in range(args.steps):
+            e2e_step(k)
+        for v in vols:
+            v.wait_read()  # every scan's volume is in host memory before the end mark
         g.mark()
         torch.cuda.synchronize()
         e2e_s = g.ms()["e2e"] / 1e3
         e2e = {"value": px_iters_step * args.steps / e2e_s, "unit": "px-iters/s",
                "h2d_bytes_per_step": w.pixels * 4, "d2h_bytes_per_step": w.pixels * 4 + vox * 6,
                "ms_per_step": e2e_s * 1e3 / args.steps,
-               "includes": "image upload from pinned host memory, PatchMatch, filter, read-back of "
-                           "the filtered maps, TSDF sweep with the volume's read-back overlapped "
-                           "(l3d_tsdf_integrate_many_read)"}
+               "includes": "every scan: image upload from pinned host memory, PatchMatch, filter, "
+                           "read-back of the filtered maps, TSDF sweep, and the volume's read-back "
+                           "(l3d_tsdf_integrate_many_read_async into one of two pinned buffers, "
+                           "overlapping the next scan's PatchMatch); the timed region ends after "
+                           "the last scan's volume is in host memory"}
+        vols[1].destroy()
     stereo.destroy()
     tsdf.destroy()
 

@@ -318,6 +318,18 @@ int l3d_tsdf_integrate_many_read(l3d_tsdf* t, const l3d_stereo* src, const int32
 
 /* TsdfVolume.read() (tsdf-volume.ts:270-277).  weight is float* (F32) or uint16_t* (Q8).
  * Either pointer may be NULL. */
+/* l3d_tsdf_integrate_many_read without waiting for the read-back: it returns once the sweep and
+ * the copies are queued (the copies run on a second stream as each part of the sweep is done).
+ * The host buffers must stay valid and untouched until l3d_tsdf_wait_read (or
+ * l3d_tsdf_synchronize / l3d_tsdf_read / l3d_tsdf_destroy) returns; work queued later on the
+ * handle that writes the volume waits for the copies on the device, so the next scan's
+ * reset and sweep can be queued at once and the read-back overlaps other work (a stereo
+ * solve on another handle).  No reference counterpart. */
+int l3d_tsdf_integrate_many_read_async(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                                       const uint32_t* packed, int32_t n,
+                                       const l3d_integration_view* views, float* tsdf, void* weight);
+/* Blocks until the handle's asynchronous read-back (if any) is in host memory. */
+int l3d_tsdf_wait_read(l3d_tsdf* t);
 int l3d_tsdf_read(l3d_tsdf* t, float* tsdf, void* weight);
 /* Back to the initial state (tsdf 1, weight 0). */
 int l3d_tsdf_reset(l3d_tsdf* t);

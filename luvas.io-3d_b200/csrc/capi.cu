@@ -1494,6 +1494,10 @@ struct l3d_tsdf {
     int32_t* list = nullptr;          /* 1 + bricks: kept bricks of a one-view integration */
     uint32_t* sweep = nullptr;        /* the sweep's brick list: flags, prefix (bricks + 1 each),
                                          list (bricks), scan scratch */
+    uint8_t* super = nullptr;         /* super-brick flags of the visibility pass, super_cap */
+    long long super_cap = 0;
+    cudaEvent_t read_done = nullptr;  /* after the copies of an asynchronous read-back */
+    bool read_pending = false;
     long long tile_cap = 0;
     L3dTsdfView* views_host = nullptr;      /* pinned staging for views */
     const uint32_t** ptrs_host = nullptr;   /* pinned staging for depth pointers */
@@ -1563,6 +1567,24 @@ uint32_t* sweep_flags(l3d_tsdf* t) { return t->sweep; }
 uint32_t* sweep_prefix(l3d_tsdf* t) { return t->sweep + (t->g.bricks + 1); }
 int32_t* sweep_list(l3d_tsdf* t) { return (int32_t*)(t->sweep + 2 * (t->g.bricks + 1)); }
 uint32_t* sweep_scratch(l3d_tsdf* t) { return t->sweep + 3 * (t->g.bricks + 1); }
+
+/* Work that writes the volume waits (on the device) for an asynchronous read-back of it. */
+int after_read(l3d_tsdf* t) {
+    if (t->read_pending) L3D_CUDA(cudaStreamWaitEvent(t->stream, t->read_done, 0), "stream wait");
+    return L3D_OK;
+}
+
+int ensure_super(l3d_tsdf* t, int n_views) {
+    const long long n = l3d_tsdf_super_flags(t->g, n_views);
+    if (t->super_cap >= n) return L3D_OK;
+    L3D_CUDA(cudaStreamSynchronize(t->stream), "super-brick flags: wait");
+    L3D_CUDA(cudaFree(t->super), "super-brick flags: free");
+    t->super = nullptr;
+    t->super_cap = 0;
+    L3D_CUDA(cudaMalloc(&t->super, (size_t)n), "super-brick flags");
+    t->super_cap = n;
+    return L3D_OK;
+}
 
 /* Upload buffers, sized in elements (u32 maps / f32 priors). */
 int ensure_maps(l3d_tsdf* t, long long elems) {
@@ -1665,6 +1687,8 @@ int l3d_tsdf_create(const l3d_tsdf_desc* d, l3d_tsdf** out) {
 
 int l3d_tsdf_reset(l3d_tsdf* t) {
     if (!t) return fail(L3D_EINVAL, "NULL handle");
+    int rc = after_read(t);
+    if (rc) return rc;
     cudaError_t e = l3d_launch_tsdf_fill(t->tsdf, t->weight, t->voxels, t->q8, t->stream);
     t->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "volume fill");
@@ -1689,7 +1713,7 @@ static int integrate_one(l3d_tsdf* t, const l3d_stereo* src, int layer, const ui
     const int mw = src ? src->Wv[ml] : t->g.W;
     const int mh = src ? src->Hv[ml] : t->g.H;
     const long long P = (long long)mw * mh;
-    if ((rc = ensure_mask(t, 1))) return rc;
+    if ((rc = ensure_mask(t, 1)) || (rc = after_read(t))) return rc;
     L3dTsdfView v = make_view(*view);
     v.W = mw;
     v.H = mh;
@@ -1737,8 +1761,13 @@ int l3d_tsdf_integrate_layer(l3d_tsdf* t, const l3d_stereo* src, int32_t layer,
  * copied out on the copy stream as soon as its launch is done. */
 static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
                           const uint32_t* packed, int32_t n, const l3d_integration_view* views,
-                          float* tsdf_out, void* weight_out, int64_t* counts_out = nullptr) {
+                          float* tsdf_out, void* weight_out, int64_t* counts_out = nullptr,
+                          bool wait = true) {
     if (!t) return fail(L3D_EINVAL, "NULL handle");
+    if (!counts_out) {
+        int rc0 = after_read(t);
+        if (rc0) return rc0;
+    }
     if (n < 0 || (n > 0 && !views)) return fail(L3D_EINVAL, "bad view list");
     if (n == 0) return L3D_OK;
     if ((src == nullptr) == (packed == nullptr))
@@ -1789,7 +1818,9 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
         ttotal += nt;
         tmax = std::max(tmax, nt);
     }
-    if ((rc = ensure_tiles(t, ttotal)) || (!counts_out && (rc = ensure_sweep(t)))) return rc;
+    if ((rc = ensure_tiles(t, ttotal)) || (rc = ensure_super(t, n)) ||
+        (!counts_out && (rc = ensure_sweep(t))))
+        return rc;
     /* the pinned staging tables are reused: wait until the previous call's copies have run */
     L3D_CUDA(cudaEventSynchronize(t->staged), "staging wait");
     for (int i = 0; i < n; i++) {
@@ -1818,13 +1849,13 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
         if (e == cudaSuccess)
             e = l3d_launch_depth_tiles(t->views, n, t->depth_ptrs, t->priors, t->tiles, tmax, t->stream);
         if (e == cudaSuccess)
-            e = l3d_launch_tsdf_visible_depth(t->g, t->views, n, t->coords, t->tiles, t->mask, t->stream);
+            e = l3d_launch_tsdf_visible_depth(t->g, t->views, n, t->coords, t->tiles, t->super, t->mask, t->stream);
         if (e == cudaSuccess)
             e = l3d_launch_tsdf_count(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
                                       t->normals, counts + 2, t->stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(host, counts, sizeof(host), cudaMemcpyDeviceToHost, t->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
-        t->launches += 5;
+        t->launches += 5 + (l3d_tsdf_super_flags(t->g, n) > 0 ? 1 : 0);
         cudaFreeAsync(counts, t->stream);
         if (e != cudaSuccess) return cuda_fail(e, "update count");
         if (host[3] != host[1])
@@ -1838,12 +1869,12 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
     }
     e = l3d_launch_depth_tiles(t->views, n, t->depth_ptrs, t->priors, t->tiles, tmax, t->stream);
     if (e == cudaSuccess)
-        e = l3d_launch_tsdf_visible_depth(t->g, t->views, n, t->coords, t->tiles, t->mask, t->stream);
+        e = l3d_launch_tsdf_visible_depth(t->g, t->views, n, t->coords, t->tiles, t->super, t->mask, t->stream);
     /* the sweep visits only the bricks some view keeps */
     if (e == cudaSuccess)
         e = l3d_launch_tsdf_brick_list(t->g, n, t->mask, sweep_flags(t), sweep_prefix(t), sweep_list(t),
                                        sweep_scratch(t), t->stream);
-    t->launches += 4 + l3d_scan_launches(t->g.bricks + 1, false);
+    t->launches += 4 + (l3d_tsdf_super_flags(t->g, n) > 0 ? 1 : 0) + l3d_scan_launches(t->g.bricks + 1, false);
     if (e != cudaSuccess) return cuda_fail(e, "visibility launch");
     if (!tsdf_out && !weight_out) {
         e = l3d_launch_tsdf_many_list(t->g, t->views, n, t->coords, t->mask, t->depth_ptrs, t->priors,
@@ -1889,7 +1920,15 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
                                          (size_t)(v1 - v0) * wsize, cudaMemcpyDeviceToHost, t->copy),
                          "read weight");
         }
-        L3D_CUDA(cudaStreamSynchronize(t->copy), "read");
+        if (wait) {
+            L3D_CUDA(cudaStreamSynchronize(t->copy), "read");
+            t->read_pending = false;
+        } else {
+            if (!t->read_done)
+                L3D_CUDA(cudaEventCreateWithFlags(&t->read_done, cudaEventDisableTiming), "event creation");
+            L3D_CUDA(cudaEventRecord(t->read_done, t->copy), "event record");
+            t->read_pending = true;
+        }
     }
     if (src && (rc = before_stereo(t, src))) return rc;
     return L3D_OK;
@@ -1917,6 +1956,13 @@ int l3d_tsdf_integrate_many_read(l3d_tsdf* t, const l3d_stereo* src, const int32
                                  const l3d_integration_view* views, float* tsdf, void* weight) {
     if (!tsdf && !weight) return fail(L3D_EINVAL, "no output buffer");
     return integrate_many(t, src, layers, packed, n, views, tsdf, weight);
+}
+
+int l3d_tsdf_integrate_many_read_async(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
+                                       const uint32_t* packed, int32_t n,
+                                       const l3d_integration_view* views, float* tsdf, void* weight) {
+    if (!tsdf && !weight) return fail(L3D_EINVAL, "no output buffer");
+    return integrate_many(t, src, layers, packed, n, views, tsdf, weight, nullptr, false);
 }
 
 /* Shared body of l3d_tsdf_forward_depth / l3d_tsdf_backward. */
@@ -1982,6 +2028,8 @@ int l3d_tsdf_backward(l3d_tsdf* t, const l3d_integration_view* view, int32_t wid
 
 int l3d_tsdf_read(l3d_tsdf* t, float* tsdf, void* weight) {
     if (!t) return fail(L3D_EINVAL, "NULL handle");
+    int rc = l3d_tsdf_wait_read(t);
+    if (rc) return rc;
     if (tsdf) L3D_CUDA(cudaMemcpyAsync(tsdf, t->tsdf, (size_t)t->voxels * 4, cudaMemcpyDeviceToHost, t->stream), "read tsdf");
     if (weight)
         L3D_CUDA(cudaMemcpyAsync(weight, t->weight, (size_t)t->voxels * (t->q8 ? 2 : 4), cudaMemcpyDeviceToHost, t->stream), "read weight");
@@ -2004,10 +2052,19 @@ int l3d_tsdf_stream(const l3d_tsdf* t, void** stream) {
     return L3D_OK;
 }
 
+int l3d_tsdf_wait_read(l3d_tsdf* t) {
+    if (!t) return fail(L3D_EINVAL, "NULL handle");
+    if (t->read_pending) {
+        L3D_CUDA(cudaEventSynchronize(t->read_done), "read");
+        t->read_pending = false;
+    }
+    return L3D_OK;
+}
+
 int l3d_tsdf_synchronize(l3d_tsdf* t) {
     if (!t) return fail(L3D_EINVAL, "NULL handle");
     L3D_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
-    return L3D_OK;
+    return l3d_tsdf_wait_read(t);
 }
 
 int64_t l3d_tsdf_launches(const l3d_tsdf* t) { return t ? t->launches : -1; }
@@ -2027,11 +2084,13 @@ void l3d_tsdf_destroy(l3d_tsdf* t) {
     cudaFree(t->tiles);
     cudaFree(t->list);
     cudaFree(t->sweep);
+    cudaFree(t->super);
     cudaFreeHost(t->views_host);
     cudaFreeHost(t->ptrs_host);
     if (t->done) cudaEventDestroy(t->done);
     if (t->staged) cudaEventDestroy(t->staged);
     if (t->copy) cudaStreamSynchronize(t->copy);
+    if (t->read_done) cudaEventDestroy(t->read_done);
     for (cudaEvent_t ev : t->slab_done)
         if (ev) cudaEventDestroy(ev);
     if (t->copy) cudaStreamDestroy(t->copy);

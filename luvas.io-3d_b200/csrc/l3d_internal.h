@@ -206,8 +206,13 @@ cudaError_t l3d_launch_depth_tiles(const L3dTsdfView* views_dev, int n_views,
  * (l3d_launch_depth_tiles first), not provably behind every depth of its footprint by more than
  * the truncation band (such a brick has no voxel that updates) */
 cudaError_t l3d_launch_tsdf_visible_depth(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
-                                          const int32_t* coords, const float* tiles, uint8_t* mask,
-                                          cudaStream_t stream);
+                                          const int32_t* coords, const float* tiles, uint8_t* super,
+                                          uint8_t* mask, cudaStream_t stream);
+/* Bytes of the super-brick flags l3d_launch_tsdf_visible_depth uses on a dense grid (0 for a
+ * brick pool, which gets no super-brick pass; `super` may then be NULL).  With `super` and
+ * `tiles` it first tests blocks of 4^3 bricks per view and skips the bricks of those behind the
+ * depths (one launch more). */
+long long l3d_tsdf_super_flags(const L3dTsdfGrid& g, int n_views);
 /* counts[0] += visible voxel-views, counts[1] += voxel-updates of a many-view integration */
 cudaError_t l3d_launch_tsdf_count(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
                                   const int32_t* coords, const uint8_t* mask,

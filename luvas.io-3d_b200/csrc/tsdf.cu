@@ -14,12 +14,17 @@
  *   k_count_updates
  *                  the visible voxel-views and voxel-updates of a many-view integration, without
  *                  its writes (the algorithmic bytes of the one-view-per-launch form).
- *   k_depth_tiles, k_visible_depth
- *                  the depth-aware half of the brick cull (see brick_behind_depths).
- *   k_integrate_many
+ *   k_depth_tiles, k_super_behind, k_visible_depth
+ *                  the depth-aware half of the brick cull (see brick_behind_depths), first for
+ *                  blocks of 4^3 bricks, then for the bricks of the blocks not dropped.
+ *   k_integrate_many, k_integrate_many_list
  *                  many views per sweep: the same thread keeps its four voxels in registers,
  *                  applies every view in order and writes back once; per-voxel results equal the
- *                  per-view launches bit for bit (the per-voxel update order is unchanged).
+ *                  per-view launches bit for bit (the per-voxel update order is unchanged).  The
+ *                  list form visits only the bricks some view keeps (k_brick_any, a prefix sum,
+ *                  k_brick_list_fill).
+ *   k_integrate_list
+ *                  one view over the bricks it keeps (k_visible_one_list), grid-stride.
  *
  * Per-voxel arithmetic (tsdf-volume.ts:111-153), fixed order shared with the FP32 restatement:
  *   world = fma(i + 0.5, voxel, origin); cam = R world + t (fma chain); pixel =
@@ -287,6 +292,10 @@ __global__ void k_visible(const L3dTsdfGrid g, const L3dTsdfView* __restrict__ v
  * of this computation and of the kernels' own FP32 camera depth and sdf, and the one-pixel
  * widening covers that of the projections.  Bricks with a corner at z <= 0.02 or a footprint
  * wider than 32 x 32 tiles are kept. */
+__device__ __forceinline__ bool box_behind_depths(const L3dTsdfGrid& g, const L3dTsdfView& v,
+                                                  const float* __restrict__ tiles, float lx, float ly,
+                                                  float lz, float span);
+
 __device__ __forceinline__ bool brick_behind_depths(const L3dTsdfGrid& g, const L3dTsdfView& v,
                                                     const int32_t* __restrict__ coords,
                                                     const float* __restrict__ tiles, long long b) {
@@ -300,11 +309,17 @@ __device__ __forceinline__ bool brick_behind_depths(const L3dTsdfGrid& g, const 
         by = coords[b * 4 + 1];
         bz = coords[b * 4 + 2];
     }
+    return box_behind_depths(g, v, tiles, fmaf((float)(bx * 8) + 0.5f, g.voxel, g.origin[0]),
+                             fmaf((float)(by * 8) + 0.5f, g.voxel, g.origin[1]),
+                             fmaf((float)(bz * 8) + 0.5f, g.voxel, g.origin[2]), 7.0f * g.voxel);
+}
+
+/* brick_behind_depths for the axis-aligned box of voxel centres from (lx, ly, lz) to
+ * (lx, ly, lz) + span on each axis. */
+__device__ __forceinline__ bool box_behind_depths(const L3dTsdfGrid& g, const L3dTsdfView& v,
+                                                  const float* __restrict__ tiles, float lx, float ly,
+                                                  float lz, float span) {
     const float* R = v.R;
-    const float lx = fmaf((float)(bx * 8) + 0.5f, g.voxel, g.origin[0]);
-    const float ly = fmaf((float)(by * 8) + 0.5f, g.voxel, g.origin[1]);
-    const float lz = fmaf((float)(bz * 8) + 0.5f, g.voxel, g.origin[2]);
-    const float span = 7.0f * g.voxel;
     const float3 p0 = make_float3(fmaf(R[2], lz, fmaf(R[1], ly, fmaf(R[0], lx, v.t[0]))),
                                   fmaf(R[5], lz, fmaf(R[4], ly, fmaf(R[3], lx, v.t[1]))),
                                   fmaf(R[8], lz, fmaf(R[7], ly, fmaf(R[6], lx, v.t[2]))));
@@ -381,9 +396,39 @@ __global__ void k_depth_tiles_one(const L3dTsdfView v, const uint32_t* __restric
     depth_tile(v, depth, v.has_prior ? prior : nullptr, tiles, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+/* Super-bricks of a dense grid: blocks of L3D_SUPER^3 bricks.  super[s * n_views + v] = 1 if
+ * the voxel centres of super-brick s (the grid's edge cut off) are behind view v's depths by the
+ * test of brick_behind_depths: then so is every brick inside it, and k_visible_depth drops those
+ * bricks without their own tests. */
+constexpr int L3D_SUPER = 4;
+__host__ __device__ __forceinline__ int super_count(const L3dTsdfGrid& g, int axis) {
+    return (g.nb[axis] + L3D_SUPER - 1) / L3D_SUPER;
+}
+
+__global__ void k_super_behind(const L3dTsdfGrid g, const L3dTsdfView* __restrict__ views, int n_views,
+                               const float* __restrict__ tiles, uint8_t* __restrict__ super) {
+    const long long n = (long long)super_count(g, 0) * super_count(g, 1) * super_count(g, 2);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * n_views) return;
+    const long long sb = t / n_views;
+    const int vi = (int)(t - sb * n_views);
+    const int sx = (int)(sb % super_count(g, 0));
+    const int sy = (int)((sb / super_count(g, 0)) % super_count(g, 1));
+    const int sz = (int)(sb / ((long long)super_count(g, 0) * super_count(g, 1)));
+    constexpr int V = 8 * L3D_SUPER;
+    /* the box's far corner: the last voxel of the super-brick inside the grid on each axis */
+    const int ex = min(V, g.dims[0] - sx * V) - 1, ey = min(V, g.dims[1] - sy * V) - 1;
+    const int ez = min(V, g.dims[2] - sz * V) - 1;
+    const int e = max(ex, max(ey, ez));
+    super[t] = box_behind_depths(g, views[vi], tiles, fmaf((float)(sx * V) + 0.5f, g.voxel, g.origin[0]),
+                                 fmaf((float)(sy * V) + 0.5f, g.voxel, g.origin[1]),
+                                 fmaf((float)(sz * V) + 0.5f, g.voxel, g.origin[2]), (float)e * g.voxel)
+                   ? 1 : 0;
+}
+
 __global__ void k_visible_depth(const L3dTsdfGrid g, const L3dTsdfView* __restrict__ views, int n_views,
                                 const int32_t* __restrict__ coords, const float* __restrict__ tiles,
-                                uint8_t* __restrict__ mask) {
+                                const uint8_t* __restrict__ super, uint8_t* __restrict__ mask) {
     const int stride = mask_stride(n_views);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= g.bricks * stride) return;
@@ -392,6 +437,16 @@ __global__ void k_visible_depth(const L3dTsdfGrid g, const L3dTsdfView* __restri
     if (vi >= n_views) {
         mask[t] = 0;
         return;
+    }
+    if (super) {
+        const int bx = (int)(b % g.nb[0]), by = (int)((b / g.nb[0]) % g.nb[1]);
+        const int bz = (int)(b / ((long long)g.nb[0] * g.nb[1]));
+        const long long sb = ((long long)(bz / L3D_SUPER) * super_count(g, 1) + by / L3D_SUPER) *
+                                 super_count(g, 0) + bx / L3D_SUPER;
+        if (__ldg(super + sb * n_views + vi)) {
+            mask[t] = 0;
+            return;
+        }
     }
     /* a brick behind the depths needs no frustum test: it is dropped either way */
     mask[t] = (tiles && brick_behind_depths(g, views[vi], coords, tiles, b))
@@ -950,12 +1005,25 @@ cudaError_t l3d_launch_depth_tiles(const L3dTsdfView* views_dev, int n_views,
     return cudaGetLastError();
 }
 
+long long l3d_tsdf_super_flags(const L3dTsdfGrid& g, int n_views) {
+    if (!g.dense) return 0;
+    return (long long)super_count(g, 0) * super_count(g, 1) * super_count(g, 2) * n_views;
+}
+
 cudaError_t l3d_launch_tsdf_visible_depth(const L3dTsdfGrid& g, const L3dTsdfView* views_dev, int n_views,
-                                          const int32_t* coords, const float* tiles, uint8_t* mask,
-                                          cudaStream_t stream) {
+                                          const int32_t* coords, const float* tiles, uint8_t* super,
+                                          uint8_t* mask, cudaStream_t stream) {
     long long n = g.bricks * mask_stride(n_views);
     if (n == 0 || n_views == 0) return cudaSuccess;
-    k_visible_depth<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(g, views_dev, n_views, coords, tiles, mask);
+    const long long ns = l3d_tsdf_super_flags(g, n_views);
+    const bool use_super = super && tiles && ns > 0;
+    if (use_super) {
+        k_super_behind<<<(unsigned)((ns + 255) / 256), 256, 0, stream>>>(g, views_dev, n_views, tiles, super);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    k_visible_depth<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(g, views_dev, n_views, coords, tiles,
+                                                                   use_super ? super : nullptr, mask);
     return cudaGetLastError();
 }
 

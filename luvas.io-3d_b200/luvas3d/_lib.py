@@ -163,6 +163,8 @@ SIGNATURES = [
     ("l3d_tsdf_count_updates", C.c_int, [_P, _P, C.POINTER(C.c_int32), _P, _I, C.POINTER(IntegrationView),
                                          C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("l3d_tsdf_integrate_many_read", C.c_int, [_P, _P, C.POINTER(C.c_int32), _P, _I, C.POINTER(IntegrationView), _P, _P]),
+    ("l3d_tsdf_integrate_many_read_async", C.c_int, [_P, _P, C.POINTER(C.c_int32), _P, _I, C.POINTER(IntegrationView), _P, _P]),
+    ("l3d_tsdf_wait_read", C.c_int, [_P]),
     ("l3d_tsdf_read", C.c_int, [_P, _P, _P]),
     ("l3d_tsdf_reset", C.c_int, [_P]),
     ("l3d_tsdf_voxels", C.c_int64, [_P]),

@@ -225,26 +225,33 @@ class TsdfVolume:
             self.synchronize()
 
     def integrate_many_read(self, views: Sequence[IntegrationView], depths=None, stereo=None,
-                            layers: Sequence[int] | None = None, out=None):
+                            layers: Sequence[int] | None = None, out=None, wait: bool = True):
         """integrate_many() then read(), with the read-back overlapped with the sweep.  `out`:
         optional (tsdf, weight) host buffers of voxels elements each (pinned memory, e.g.
-        torch's pin_memory(), overlaps fully); returns them shaped like read()'s."""
+        torch's pin_memory(), overlaps fully); returns them shaped like read()'s.  With
+        wait=False (`out` required) the call returns once the work is queued
+        (l3d_tsdf_integrate_many_read_async): the buffers hold the volume after wait_read()."""
+        if not wait and out is None:
+            raise ValueError("an asynchronous read-back needs the caller's `out` buffers")
         keep: list = []
         arr = (_lib.IntegrationView * len(views))(*[_c_view(v, keep) for v in views])
         tsdf, weight = out if out is not None else self._host_volume()
         tp = _host_ptr(tsdf, self.voxels, 4)
         wp = _host_ptr(weight, self.voxels, 2 if self.weight_q8 else 4)
+        fn = self._lib.l3d_tsdf_integrate_many_read if wait else self._lib.l3d_tsdf_integrate_many_read_async
         if stereo is not None:
             lay = np.asarray(layers if layers is not None else range(len(views)), dtype=np.int32)
-            _lib.check(self._lib.l3d_tsdf_integrate_many_read(
-                self._h(), stereo._h(), lay.ctypes.data_as(C.POINTER(C.c_int32)), None,
-                len(views), arr, tp, wp))
+            _lib.check(fn(self._h(), stereo._h(), lay.ctypes.data_as(C.POINTER(C.c_int32)), None,
+                          len(views), arr, tp, wp))
         else:
             p = np.ascontiguousarray(depths, dtype=np.uint32)
-            _lib.check(self._lib.l3d_tsdf_integrate_many_read(self._h(), None, None, _lib.ptr(p),
-                                                              len(views), arr, tp, wp))
+            _lib.check(fn(self._h(), None, None, _lib.ptr(p), len(views), arr, tp, wp))
             keep.append(p)
         return self._shaped(tsdf, weight)
+
+    def wait_read(self) -> None:
+        """Blocks until an asynchronous read-back (integrate_many_read(wait=False)) is done."""
+        _lib.check(self._lib.l3d_tsdf_wait_read(self._h()))
 
     def _host_volume(self) -> tuple[np.ndarray, np.ndarray]:
         n = self.voxels

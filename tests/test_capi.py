@@ -101,6 +101,9 @@ def test_bad_arguments_are_rejected_with_a_message():
     assert "no output" in _lib.last_error()
     assert lib.l3d_tsdf_integrate_many_read(None, None, None, None, 1, None, buf, None) == _lib.L3D_EINVAL
     assert "NULL handle" in _lib.last_error()
+    assert lib.l3d_tsdf_integrate_many_read_async(None, None, None, None, 1, None, None, None) == _lib.L3D_EINVAL
+    assert "no output" in _lib.last_error()
+    assert lib.l3d_tsdf_wait_read(None) == _lib.L3D_EINVAL
     rate = C.c_double(-1.0)
     assert lib.l3d_measure_texture_rate(_lib.DTYPE_BF16, 1, C.byref(rate)) == _lib.L3D_EINVAL
     assert "dtype" in _lib.last_error()

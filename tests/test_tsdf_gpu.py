@@ -140,6 +140,41 @@ def test_integrate_many_read_equals_sweep_then_read(scene, layout, q8):
         b.integrate_many_read(iv, depths=np.stack(maps), out=(np.empty(3, np.float32), None))
 
 
+@pytest.mark.parametrize("q8", [False, True])
+def test_asynchronous_read_back_is_ordered_before_later_writes(scene, q8):
+    """l3d_tsdf_integrate_many_read_async returns before the volume is in host memory; a reset
+    and another sweep queued on the same handle right after it wait for its copies on the
+    device, so the buffers receive the first scan's volume, and wait_read returns it."""
+    import torch
+    views, maps = scene
+    W, H = 120, 90
+    iv = [gpu_view(v, confidence=1.5) for v in views]
+
+    def make():
+        return TsdfVolume(W, H, 0.04, (-1.28, -1.1, -1.1), dense=(64, 48, 56), truncation=0.12,
+                          weight_q8=q8)
+    a, b = make(), make()
+    a.integrate_many(iv, depths=np.stack(maps))
+    ta, wa = a.read()
+    a.reset()
+    a.integrate_many(iv[::-1], depths=np.stack(maps[::-1]))  # a different second scan
+    tr, wr = a.read()
+    n = b.voxels
+    outs = [(torch.empty(n, dtype=torch.float32).pin_memory(),
+             torch.empty(n, dtype=torch.int16 if q8 else torch.float32).pin_memory()) for _ in range(2)]
+    b.integrate_many_read(iv, depths=np.stack(maps), out=outs[0], wait=False)
+    b.reset()
+    b.integrate_many_read(iv[::-1], depths=np.stack(maps[::-1]), out=outs[1], wait=False)
+    b.wait_read()
+    for (pt, pw), (t, w), what in zip(outs, ((ta, wa), (tr, wr)), ("first scan", "second scan")):
+        assert_bit_equal(pt.numpy().reshape(t.shape), t, f"tsdf ({what})")
+        assert_bit_equal(pw.numpy().view(w.dtype).reshape(w.shape), w, f"weight ({what})")
+    tb, wb = b.read()
+    assert_bit_equal(tb, tr, "tsdf after the reads")
+    with pytest.raises(ValueError):
+        b.integrate_many_read(iv, depths=np.stack(maps), wait=False)
+
+
 def test_brick_pool_and_prior_bit_exact(scene):
     views, maps = scene
     W, H = 120, 90
