@@ -915,13 +915,8 @@ def run_scan(args) -> None:
     # ---- end to end through the C ABI with pinned host buffers ------------------------------
     e2e = None
     if not args.no_e2e:
-        import ctypes as C
-
-        from luvas3d import _lib
-        lib = _lib.load()
         pinned = [torch.from_numpy(np.ascontiguousarray(im)).pin_memory() for im in w.images]
         out_f = torch.empty(w.pixels, dtype=torch.int32).pin_memory()
-        f_off = np.concatenate([[0], np.cumsum([a * b for a, b in sizes])])
         # two volumes and two pinned outputs: scan k's volume is read back while scan k + 1 runs
         vols = [tsdf, TsdfVolume(max(s[0] for s in sizes), max(s[1] for s in sizes), w.tsdf_voxel,
                                  w.tsdf_origin, dense=w.tsdf_dims, truncation=w.tsdf_truncation,
@@ -936,9 +931,7 @@ def run_scan(args) -> None:
             stereo.solve_all(refs, opts)
             stereo.filter_all(refs, w.sources, w.needed)
             vol.reset()  # queued after this volume's previous read-back (on the device)
-            for r in refs:
-                _lib.check(lib.l3d_stereo_read_filtered_layer(
-                    stereo._h(), r, C.c_void_p(out_f[int(f_off[r]):].data_ptr())))
+            stereo.read_filtered_all_async(out_f)  # every filtered map, one copy on the stream
             # the sweep, its read-back queued behind it on the volume's copy stream
             # (l3d_tsdf_integrate_many_read_async); the host goes on to the next scan
             vol.integrate_many_read(iviews, stereo=stereo, layers=refs, out=outs[k % 2], wait=False)
@@ -954,6 +947,7 @@ def run_scan(args) -> None:
             e2e_step(k)
         for v in vols:
             v.wait_read()  # every scan's volume is in host memory before the end mark
+        stereo.synchronize()  # and the last scan's filtered maps
         g.mark()
         torch.cuda.synchronize()
         e2e_s = g.ms()["e2e"] / 1e3
@@ -961,7 +955,8 @@ def run_scan(args) -> None:
                "h2d_bytes_per_step": w.pixels * 4, "d2h_bytes_per_step": w.pixels * 4 + vox * 6,
                "ms_per_step": e2e_s * 1e3 / args.steps,
                "includes": "every scan: image upload from pinned host memory, PatchMatch, filter, "
-                           "read-back of the filtered maps, TSDF sweep, and the volume's read-back "
+                           "read-back of the filtered maps (l3d_stereo_read_filtered_all_async), "
+                           "TSDF sweep, and the volume's read-back "
                            "(l3d_tsdf_integrate_many_read_async into one of two pinned buffers, "
                            "overlapping the next scan's PatchMatch); the timed region ends after "
                            "the last scan's volume is in host memory"}

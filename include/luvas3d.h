@@ -220,6 +220,11 @@ int l3d_stereo_filter_all(l3d_stereo* s, int32_t n_refs, const int32_t* refs,
 int l3d_stereo_read_filtered(l3d_stereo* s, uint32_t* out);
 /* filtered_all[layer]. */
 int l3d_stereo_read_filtered_layer(l3d_stereo* s, int32_t layer, uint32_t* out);
+/* Every view's filter_all map in one copy queued on the handle's stream, without waiting: the
+ * maps concatenated in layer order (each of its view's width * height), the same values as
+ * l3d_stereo_read_filtered_layer per layer.  `out` (pinned memory overlaps with other work) holds
+ * them after l3d_stereo_synchronize; later work on the handle is ordered after the copy. */
+int l3d_stereo_read_filtered_all_async(l3d_stereo* s, uint32_t* out);
 /* DenseStereo.depthMap(ref) (dense-stereo.ts:309-312). */
 int l3d_stereo_read_depth(l3d_stereo* s, int32_t ref, uint32_t* out);
 /* DenseStereo.hypotheses (dense-stereo.ts:242-244) and the cost buffer; hyp4 is

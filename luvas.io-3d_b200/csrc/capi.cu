@@ -1114,6 +1114,14 @@ int l3d_stereo_read_filtered_layer(l3d_stereo* s, int32_t layer, uint32_t* out) 
                     "read filtered layer");
 }
 
+int l3d_stereo_read_filtered_all_async(l3d_stereo* s, uint32_t* out) {
+    if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
+    if (!s->filtered_all) return fail(L3D_ESTATE, "no filter_all has run");
+    L3D_CUDA(cudaMemcpyAsync(out, s->filtered_all, (size_t)s->Ptot * 4, cudaMemcpyDeviceToHost, s->stream),
+             "read filtered maps");
+    return L3D_OK;
+}
+
 int l3d_stereo_read_depth(l3d_stereo* s, int32_t ref, uint32_t* out) {
     if (!s || !out) return fail(L3D_EINVAL, "NULL argument");
     if (ref < 0 || ref >= s->n_maps) return fail(L3D_EINVAL, "depth map %d out of range", ref);

@@ -727,15 +727,26 @@ __global__ void __launch_bounds__(256, 4) k_integrate_many_list(const L3dTsdfGri
                                                              const int32_t* __restrict__ list,
                                                              long long b_begin, long long b_end) {
     constexpr int PER = 512 / VEC;
+    /* the view table in shared memory, copied once per block (the blocks loop over the list) */
+    extern __shared__ __align__(16) unsigned char sweep_smem[];
+    L3dTsdfView* sv = reinterpret_cast<L3dTsdfView*>(sweep_smem);
+    {
+        const int words = n_views * (int)(sizeof(L3dTsdfView) / 8);
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(views);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(sweep_smem);
+        for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = __ldg(src + k);
+        __syncthreads();
+    }
     const long long first = __ldg(prefix + b_begin);
     const long long n = ((long long)__ldg(prefix + b_end) - first) * PER;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         const long long b = __ldg(list + first + i / PER);
-        sweep_quad<VEC, Q8>(g, views, n_views, coords, mask, depths, priors, normals, tsdf, weight,
+        sweep_quad<VEC, Q8>(g, sv, n_views, coords, mask, depths, priors, normals, tsdf, weight,
                             b * PER + i % PER);
     }
 }
+static_assert(sizeof(L3dTsdfView) % 8 == 0, "the view table is copied in 8-byte words");
 
 /* flags[b] = 1 if some view keeps brick b (its mask row is not all zero), for b < bricks;
  * flags[bricks] = 0, so that an exclusive scan of bricks + 1 flags ends with the total. */
@@ -1170,12 +1181,16 @@ cudaError_t l3d_launch_tsdf_many_list(const L3dTsdfGrid& g, const L3dTsdfView* v
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
         sms = 148;
     const unsigned blocks = (unsigned)(4 * sms);
+    const size_t smem = (size_t)n_views * sizeof(L3dTsdfView);
+    if (smem > 48 * 1024)  /* more than ~200 views: the sweep of every quad, views from global memory */
+        return l3d_launch_tsdf_many_range(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors,
+                                          normals, tsdf, weight, q8, q_begin, q_end, stream);
     if (vec == 4) {
-        if (q8) k_integrate_many_list<4, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
-        else k_integrate_many_list<4, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
+        if (q8) k_integrate_many_list<4, true><<<blocks, 256, smem, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
+        else k_integrate_many_list<4, false><<<blocks, 256, smem, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
     } else {
-        if (q8) k_integrate_many_list<1, true><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
-        else k_integrate_many_list<1, false><<<blocks, 256, 0, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
+        if (q8) k_integrate_many_list<1, true><<<blocks, 256, smem, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
+        else k_integrate_many_list<1, false><<<blocks, 256, smem, stream>>>(g, views_dev, n_views, coords, mask, depth_ptrs_dev, priors, normals, tsdf, weight, prefix, list, b0, b1);
     }
     return cudaGetLastError();
 }

@@ -140,6 +140,7 @@ SIGNATURES = [
     ("l3d_stereo_filter_all", C.c_int, [_P, _I, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("l3d_stereo_read_filtered", C.c_int, [_P, _P]),
     ("l3d_stereo_read_filtered_layer", C.c_int, [_P, _I, _P]),
+    ("l3d_stereo_read_filtered_all_async", C.c_int, [_P, _P]),
     ("l3d_stereo_read_depth", C.c_int, [_P, _I, _P]),
     ("l3d_stereo_read_hyp", C.c_int, [_P, _P, _P]),
     ("l3d_stereo_read_hyp_layer", C.c_int, [_P, _I, _P, _P]),

@@ -245,6 +245,20 @@ class DenseStereo:
         _lib.check(self._lib.l3d_stereo_read_filtered_layer(self._h(), int(layer), _lib.ptr(out)))
         return out
 
+    def read_filtered_all_async(self, out) -> None:
+        """Queues the copy of every view's filter_all map (concatenated in layer order) into the
+        host buffer `out` (u32 or i32, at least the views' total pixels; pinned memory, e.g. a
+        pinned torch tensor, overlaps with other work); `out` holds them after synchronize()."""
+        total = int(sum(w * h for w, h in self.sizes))
+        if isinstance(out, np.ndarray):
+            ok, addr = out.flags.c_contiguous and out.size >= total and out.itemsize == 4, out.ctypes.data
+        else:
+            ok = (not out.is_cuda) and out.is_contiguous() and out.numel() >= total and out.element_size() == 4
+            addr = out.data_ptr()
+        if not ok:
+            raise ValueError(f"host buffer must be contiguous with >= {total} 4-byte elements")
+        _lib.check(self._lib.l3d_stereo_read_filtered_all_async(self._h(), C.c_void_p(addr)))
+
     def depth_map(self, ref: int) -> np.ndarray:
         """depthMap (dense-stereo.ts:309-312): raw packed map of one view, (H, W) u32."""
         out = np.empty(self.shape(ref), dtype=np.uint32)

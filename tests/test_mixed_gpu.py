@@ -92,6 +92,18 @@ def test_tsdf_sweep_over_mixed_sizes(mixed):
     assert_bit_equal(t_s.reshape(-1), want_t, "tsdf")
     assert_bit_equal(w_s.reshape(-1), want_w, "weight")
     assert (want_w > 0).sum() > 1000
+    # every view's filtered map in one asynchronous copy equals the per-layer reads
+    import torch
+    out = torch.empty(sum(w * h for w, h in SIZES), dtype=torch.int32).pin_memory()
+    s.read_filtered_all_async(out)
+    s.synchronize()
+    off = 0
+    for r, (W, H) in enumerate(SIZES):
+        assert np.array_equal(out.numpy()[off:off + W * H].view(np.uint32).reshape(H, W),
+                              s.read_filtered_layer(r)), f"view {r}"
+        off += W * H
+    with pytest.raises(ValueError):
+        s.read_filtered_all_async(np.empty(3, np.uint32))
 
 
 def test_view_sizes_are_reported(mixed):

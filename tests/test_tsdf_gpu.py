@@ -175,6 +175,29 @@ def test_asynchronous_read_back_is_ordered_before_later_writes(scene, q8):
         b.integrate_many_read(iv, depths=np.stack(maps), wait=False)
 
 
+def test_sweep_of_more_views_than_the_shared_view_table_holds(scene):
+    """More than ~200 views in one sweep take the sweep of every quad with the view table in
+    global memory; the result still equals the views integrated one at a time."""
+    views, maps = scene
+    W, H = 120, 90
+    reps = 220 // len(views) + 1
+    iv = [gpu_view(v, confidence=1.5) for v in views] * reps
+    ms = np.stack(list(maps) * reps)
+    assert len(iv) > 215
+
+    def make():
+        return TsdfVolume(W, H, 0.04, (-1.28, -1.1, -1.1), dense=(64, 48, 56), truncation=0.12,
+                          weight_q8=True)
+    a, b = make(), make()
+    a.integrate_many(iv, depths=ms)
+    for v, m in zip(iv, ms):
+        b.integrate(v, m)
+    ta, wa = a.read()
+    tb, wb = b.read()
+    assert_bit_equal(ta, tb, "tsdf")
+    assert_bit_equal(wa, wb, "weight")
+
+
 def test_brick_pool_and_prior_bit_exact(scene):
     views, maps = scene
     W, H = 120, 90
