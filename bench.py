@@ -916,51 +916,64 @@ def run_scan(args) -> None:
     e2e = None
     if not args.no_e2e:
         pinned = [torch.from_numpy(np.ascontiguousarray(im)).pin_memory() for im in w.images]
-        out_f = torch.empty(w.pixels, dtype=torch.int32).pin_memory()
-        # two volumes and two pinned outputs: scan k's volume is read back while scan k + 1 runs
+        # two scans in flight: two stereo handles and two volumes on two streams, used in turn,
+        # so that scan k + 1's image upload and PatchMatch start while scan k's filter, sweep
+        # and read-backs finish, and scan k's 805 MB volume read-back overlaps scan k + 1
+        stream2 = torch.cuda.Stream()
+        sptr2 = stream2.cuda_stream
+        stereo2, _ = make_stereo(w, chosen, chosen_storage, sptr2, refs, opts,
+                                 variant=R["tuned"]["variant"])
+        sts = [stereo, stereo2]
         vols = [tsdf, TsdfVolume(max(s[0] for s in sizes), max(s[1] for s in sizes), w.tsdf_voxel,
                                  w.tsdf_origin, dense=w.tsdf_dims, truncation=w.tsdf_truncation,
-                                 weight_q8=True, stream=sptr)]
+                                 weight_q8=True, stream=sptr2)]
         outs = [(torch.empty(vox, dtype=torch.float32).pin_memory(),
                  torch.empty(vox, dtype=torch.int16).pin_memory()) for _ in range(2)]
+        out_f = [torch.empty(w.pixels, dtype=torch.int32).pin_memory() for _ in range(2)]
 
         def e2e_step(k):
-            vol = vols[k % 2]
+            st, vol = sts[k % 2], vols[k % 2]
             for i, im in enumerate(pinned):
-                stereo.set_image_device(i, im.data_ptr(), DTYPE_F32)
-            stereo.solve_all(refs, opts)
-            stereo.filter_all(refs, w.sources, w.needed)
+                st.set_image_device(i, im.data_ptr(), DTYPE_F32)
+            st.solve_all(refs, opts)
+            st.filter_all(refs, w.sources, w.needed)
             vol.reset()  # queued after this volume's previous read-back (on the device)
-            stereo.read_filtered_all_async(out_f)  # every filtered map, one copy on the stream
+            st.read_filtered_all_async(out_f[k % 2])  # every filtered map, one copy on the stream
             # the sweep, its read-back queued behind it on the volume's copy stream
             # (l3d_tsdf_integrate_many_read_async); the host goes on to the next scan
-            vol.integrate_many_read(iviews, stereo=stereo, layers=refs, out=outs[k % 2], wait=False)
+            vol.integrate_many_read(iviews, stereo=st, layers=refs, out=outs[k % 2], wait=False)
+
+        def drain():
+            for v in vols:
+                v.wait_read()
+            for st in sts:
+                st.synchronize()
 
         for k in range(2):
             e2e_step(k)
-        for v in vols:
-            v.wait_read()
+        drain()
         torch.cuda.synchronize()
-        g = Stage(stream, ["e2e"])
-        g.mark()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        stream2.wait_event(t0)
         for k in range(args.steps):
             e2e_step(k)
-        for v in vols:
-            v.wait_read()  # every scan's volume is in host memory before the end mark
-        stereo.synchronize()  # and the last scan's filtered maps
-        g.mark()
+        drain()  # every scan's filtered maps and volume are in host memory
+        t1.record(stream)
         torch.cuda.synchronize()
-        e2e_s = g.ms()["e2e"] / 1e3
+        g = {"e2e": t0.elapsed_time(t1)}
+        e2e_s = g["e2e"] / 1e3
         e2e = {"value": px_iters_step * args.steps / e2e_s, "unit": "px-iters/s",
                "h2d_bytes_per_step": w.pixels * 4, "d2h_bytes_per_step": w.pixels * 4 + vox * 6,
                "ms_per_step": e2e_s * 1e3 / args.steps,
                "includes": "every scan: image upload from pinned host memory, PatchMatch, filter, "
                            "read-back of the filtered maps (l3d_stereo_read_filtered_all_async), "
                            "TSDF sweep, and the volume's read-back "
-                           "(l3d_tsdf_integrate_many_read_async into one of two pinned buffers, "
-                           "overlapping the next scan's PatchMatch); the timed region ends after "
-                           "the last scan's volume is in host memory"}
+                           "(l3d_tsdf_integrate_many_read_async); two scans in flight (two stereo "
+                           "handles, volumes, pinned buffers and streams, used in turn); the timed "
+                           "region ends after the last scan's maps and volume are in host memory"}
         vols[1].destroy()
+        stereo2.destroy()
     stereo.destroy()
     tsdf.destroy()
 
