@@ -1915,6 +1915,8 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
             L3D_CUDA(cudaEventRecord(t->slab_done[i], t->stream), "event record");
         }
         const size_t wsize = t->q8 ? 2 : 4;
+        if (!wait && !t->read_done)
+            L3D_CUDA(cudaEventCreateWithFlags(&t->read_done, cudaEventDisableTiming), "event creation");
         for (int i = 0; i < L3D_TSDF_READ_SLABS; i++) {
             const long long v0 = std::min(t->voxels, std::min(layers, i * per) * lv);
             const long long v1 = std::min(t->voxels, std::min(layers, i * per + per) * lv);
@@ -1932,8 +1934,6 @@ static int integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* lay
             L3D_CUDA(cudaStreamSynchronize(t->copy), "read");
             t->read_pending = false;
         } else {
-            if (!t->read_done)
-                L3D_CUDA(cudaEventCreateWithFlags(&t->read_done, cudaEventDisableTiming), "event creation");
             L3D_CUDA(cudaEventRecord(t->read_done, t->copy), "event record");
             t->read_pending = true;
         }
@@ -1997,6 +1997,8 @@ static int tsdf_depth_run(l3d_tsdf* t, const l3d_integration_view* view, int32_t
         L3D_CUDA(cudaEventRecord(t->done, t->stream), "event record");
         L3D_CUDA(cudaStreamWaitEvent(st, t->done, 0), "stream wait");
     }
+    /* the caller's buffers may be the handle's own volume: after its pending read-back */
+    if (t->read_pending) L3D_CUDA(cudaStreamWaitEvent(st, t->read_done, 0), "stream wait");
     cudaError_t e = l3d_launch_tsdf_depth(t->g, v, t->coords, t->mask, packed, depth, prior, tsdf_in,
                                           weight_in, tsdf_out, weight_out, grad_tsdf_out,
                                           grad_weight_out, grad_depth, grad_tsdf_in, grad_weight_in,
