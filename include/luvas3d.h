@@ -310,8 +310,8 @@ int l3d_tsdf_count_updates(l3d_tsdf* t, const l3d_stereo* src, const int32_t* la
  * equal, bit for bit, to n integrate() calls in order.  Maps come from src's filtered_all
  * (src != NULL, layers[i]) or from packed (host, n * width * height).  The sweep visits only the
  * bricks that some view keeps (visibleBricks and a depth-aware cull that drops bricks entirely
- * behind a view's truncation band, which cannot be updated), and only the volume of bricks that
- * a view updates is written. */
+ * behind a view's truncation band, which cannot be updated), and writes back only the voxels of
+ * the four-voxel groups that some view updated. */
 int l3d_tsdf_integrate_many(l3d_tsdf* t, const l3d_stereo* src, const int32_t* layers,
                             const uint32_t* packed, int32_t n, const l3d_integration_view* views);
 
