@@ -34,7 +34,9 @@ extern "C" {
 
 /* Version of the structures and calls below.  2: l3d_stereo_opts gained `compensated` (its size
  * changed, so a host built against version 1 must be rebuilt), L3D_FORM_EXACT, variant bits 16
- * and 32, l3d_tsdf_integrate_layer, l3d_tsdf_count_updates and l3d_measure_fetch_rate. */
+ * and 32, l3d_tsdf_integrate_layer, l3d_tsdf_count_updates (with the kept count),
+ * l3d_measure_fetch_rate, l3d_stereo_read_filtered_all_async, l3d_tsdf_integrate_many_read_async
+ * and l3d_tsdf_wait_read. */
 #define L3D_ABI_VERSION 2
 
 /* Status codes. */
