@@ -145,3 +145,24 @@ def test_equal_accuracy_forms_at_full_size(scan, form, storage, variant):
                          f"view {r} hypotheses")
     one.destroy()
     s.destroy()
+
+
+def test_exact_form_equals_plain_form_at_full_size(scan):
+    """The exact batched form (all 48 views per launch, CUDA graphs) and the plain per-view form
+    compute the FP32 oracle's arithmetic, so at the benchmark's size too their packed depth maps
+    agree bit for bit for every view, and their planes and costs for the views checked."""
+    w, refs, opts = scan
+    exact = solved(w, refs, opts, FORM_EXACT, DTYPE_F32)
+    exact.set_graphs(True)
+    exact.solve_all(refs, opts)  # a replayed graph gives the same solve
+    plain = solved(w, refs, opts, FORM_PLAIN, DTYPE_F32)
+    for r in refs:
+        assert np.array_equal(exact.depth_map(r), plain.depth_map(r)), f"view {r} packed map"
+    for r in (0, 17, 47):
+        plain.solve(r, opts[r])
+        hp, cp = plain.read_hypotheses()
+        hx, cx = exact.read_hypotheses_layer(r)
+        assert_bit_equal(hx, hp, f"view {r} hypotheses")
+        assert_bit_equal(cx, cp, f"view {r} costs")
+    exact.destroy()
+    plain.destroy()
