@@ -2,7 +2,7 @@
 5 iterations, TSDF 512^3 at 4 mm).
 
 The oracle cannot solve this size in test time, so these check relations that hold at any size:
-the fast form's depth accuracy against the rendered ground truth equals the plain form's, a
+the exact batched form equals the plain per-view form bit for bit, the fast form's depth accuracy against the rendered ground truth equals the plain form's, a
 batched solve equals its views solved one by one, the batched consistency filter equals the
 per-view filter, the many-view TSDF sweep (with and without the overlapped read-back) and the
 one-view-per-launch integration of the batched maps equal the per-view integrations bit for bit,
