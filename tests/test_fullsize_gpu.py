@@ -2,16 +2,19 @@
 5 iterations, TSDF 512^3 at 4 mm).
 
 The oracle cannot solve this size in test time, so these check relations that hold at any size:
-the exact batched form equals the plain per-view form bit for bit, the fast form's depth accuracy against the rendered ground truth equals the plain form's, a
-batched solve equals its views solved one by one, the batched consistency filter equals the
-per-view filter, the many-view TSDF sweep (with and without the overlapped read-back) and the
-one-view-per-launch integration of the batched maps equal the per-view integrations bit for bit,
-and the equal-accuracy forms (fast form with FP32 gathers, exact form) keep the plain form's
-accuracy against the ground truth, batched or one by one.
+the exact batched form equals the plain per-view form bit for bit; the fast form's depth
+accuracy against the rendered ground truth equals the plain form's; a batched solve equals its
+views solved one by one; the batched consistency filter equals the per-view filter; the
+many-view TSDF sweep (with and without the overlapped read-back) and the one-view-per-launch
+integration of the batched maps equal the per-view integrations, and the FP32 oracle's
+integration of the same maps (which does run in test time), bit for bit; and the equal-accuracy
+forms (fast form with FP32 gathers, exact form) keep the plain form's accuracy against the
+ground truth, batched or one by one.
 """
 import numpy as np
 import pytest
 
+import oracle
 from helpers import assert_bit_equal
 from luvas3d import (DTYPE_F16, DTYPE_F32, FORM_EXACT, FORM_FAST, FORM_PLAIN, DenseStereo, IntegrationView,
                      SolveOptions, StereoOptions, TsdfVolume, scenes)
@@ -122,6 +125,15 @@ def test_tsdf_sweep_equals_per_view_integration(scan, fast):
     assert (wa > 0).mean() > 0.05
     for v in (a, b, c, d):
         v.destroy()
+    # the FP32 oracle integrating the same 48 maps into the same 512^3 volume (all host cores)
+    o = oracle.Tsdf(w.width, w.height, w.tsdf_voxel, w.tsdf_origin, w.tsdf_truncation,
+                    dense=w.tsdf_dims, weight_q8=True)
+    for i, r in enumerate(refs):
+        k = w.views[i].intrinsics
+        o.integrate(dict(k=(k.fx, k.fy, k.cx, k.cy), R=w.views[i].pose.R, t=w.views[i].pose.t,
+                         max_depth=w.ranges[i][1]), fast.read_filtered_layer(r))
+    assert_bit_equal(tb.reshape(-1), o.tsdf.reshape(-1), "tsdf against the oracle")
+    assert_bit_equal(wb.reshape(-1), o.weight.reshape(-1), "weight against the oracle")
 
 
 @pytest.mark.parametrize("form,storage,variant", [(FORM_FAST, DTYPE_F32, 30), (FORM_EXACT, DTYPE_F32, 14)])
