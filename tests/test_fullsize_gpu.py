@@ -178,3 +178,23 @@ def test_exact_form_equals_plain_form_at_full_size(scan):
         assert_bit_equal(cx, cp, f"view {r} costs")
     exact.destroy()
     plain.destroy()
+
+
+def test_plain_form_equals_the_fp32_oracle_at_full_size(scan):
+    """Two of the scan's views solved at full size (640x480, 8 sources, 5 iterations) by the
+    plain form and by the FP32 oracle (all host cores, a few seconds per view): planes, costs and
+    packed maps bit for bit."""
+    w, refs, opts = scan
+    plain = DenseStereo(w.width, w.height, w.views, StereoOptions(storage=DTYPE_F32, form=FORM_PLAIN))
+    for i, im in enumerate(w.images):
+        plain.set_image(i, im)
+    o = oracle.Stereo(w.width, w.height, w.views, w.images, 32)
+    for r in (12, 40):
+        plain.solve(r, opts[r])
+        o.solve(r, w.sources[r], min_depth=w.ranges[r][0], max_depth=w.ranges[r][1],
+                iterations=w.iterations)
+        hp, cp = plain.read_hypotheses()
+        assert_bit_equal(hp, o.hyp, f"view {r} planes")
+        assert_bit_equal(cp, o.cost, f"view {r} costs")
+        assert np.array_equal(plain.depth_map(r), o.depths[r]), f"view {r} packed map"
+    plain.destroy()
