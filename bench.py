@@ -23,8 +23,9 @@ mixed sizes, TSDF 768^3) and the differentiation configuration (polish: the NCC 
 views of 640x480), and the CPU sample of the reference algorithm.
 
 Multi-GPU (--gpus N, or N ranks under torch.distributed.run): one scan split over the GPUs, views
-dealt by pixel count, one NCCL all-gather of the packed depth maps per step, TSDF z-slabs per
-GPU ("scaling": "strong": the scan is the same at every N).
+dealt by pixel count, one NCCL all-gather of the packed depth maps and one of the filtered maps
+per step (each rank filters its own views), TSDF z-slabs per GPU ("scaling": "strong": the scan
+is the same at every N).
 """
 from __future__ import annotations
 
@@ -1123,7 +1124,7 @@ def run_split(args, rank: int, world: int, local: int) -> None:
                          weight_q8=True, stream=sptr)
     split = shard.ScanSplit(shard.DeviceScan(st, vol, opts, w.sources, w.needed, iviews), sizes,
                             rank, world, device=device)
-    names = ["patchmatch", "exchange", "filter", "tsdf"]
+    names = ["patchmatch", "exchange", "filter", "exchange_filtered", "tsdf"]
 
     def step(g):
         with torch.cuda.stream(stream):
@@ -1136,6 +1137,8 @@ def run_split(args, rank: int, world: int, local: int) -> None:
         if vol is not None:
             vol.reset()
         split.filter()
+        g.mark()
+        split.exchange_filtered()
         g.mark()
         split.integrate()
         g.mark()
@@ -1189,6 +1192,7 @@ def run_split(args, rank: int, world: int, local: int) -> None:
             if vol is not None:
                 vol.reset()
             split.filter()
+            split.exchange_filtered()
             for r in mine:
                 _lib.check(lib.l3d_stereo_read_filtered_layer(
                     st._h(), r, C.c_void_p(out_f[int(f_off[r]):].data_ptr())))
@@ -1209,9 +1213,9 @@ def run_split(args, rank: int, world: int, local: int) -> None:
                "h2d_bytes_per_step": world * w.pixels * 4, "d2h_bytes_per_step": w.pixels * 4 + vox * 6,
                "ms_per_step": e2e_s * 1e3 / args.steps,
                "includes": "every rank: every image uploaded from pinned host memory, its views' "
-                           "PatchMatch, the all-gather of packed maps, every view's filter, the "
-                           "read-back of its views' filtered maps, the sweep of its slab with the "
-                           "slab's read-back overlapped"}
+                           "PatchMatch, the all-gather of packed maps, its views' filter, the "
+                           "all-gather of filtered maps, the read-back of its views' filtered "
+                           "maps, the sweep of its slab with the slab's read-back overlapped"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": px_iters_step * args.steps / pm_s, "unit": "px-iters/s",
@@ -1223,8 +1227,9 @@ def run_split(args, rank: int, world: int, local: int) -> None:
             "config": {"workload": workload_name(w), "form": "fast", "variant": tuned["variant"],
                        "graphs": True, "l2": "flushed (256 MB write) before every step",
                        "parallelism": (f"split over {world} GPUs: reference views dealt by pixel "
-                                       "count, one NCCL all-gather of the packed depth maps per "
-                                       "step, TSDF z-slabs of bricks per GPU")},
+                                       "count, NCCL all-gathers of the packed depth maps and of "
+                                       "the filtered maps per step (each rank filters its own "
+                                       "views), TSDF z-slabs of bricks per GPU")},
             "tsdf_voxel_updates_per_s": vox * V * args.steps / ts_s,
             "stage_ms_rank0": stage,
             "views_rank0": len(mine),

@@ -137,17 +137,20 @@ def slab_pool(dims: Sequence[int], rank: int, world: int) -> np.ndarray | None:
 class ScanSplit:
     """One scan split over the ranks of a process group: the photometric solve of this rank's
     views (shard_views), one all-gather of every view's packed depth map, the consistency filter
-    of every view on every rank (cheap, and it needs every map), and the TSDF integration of
-    every view into this rank's z-slab of bricks.  Each rank's slab equals the same bricks of a
-    single-GPU volume bit for bit, and every rank's packed and filtered maps equal the single-GPU
-    maps bit for bit (the batched photometric solve of a subset of views equals its views solved
-    alone).
+    of this rank's views (it reads every view's packed map), one all-gather of every view's
+    filtered map, and the TSDF integration of every view into this rank's z-slab of bricks.
+    Each rank's slab equals the same bricks of a single-GPU volume bit for bit, and every rank's
+    packed and filtered maps equal the single-GPU maps bit for bit (the batched photometric solve
+    of a subset of views equals its views solved alone, and the filter of a view depends only on
+    the packed maps).
 
     `backend` does the device work:
       solve(views)              photometric solve of the given reference views;
       packed_maps(views)        {view: that view's packed map (H, W) or flat}, 4-byte integers;
       set_packed_maps(full)     every view's packed map, concatenated in view order (flat);
-      filter_all()              consistency filter of every view;
+      filter_views(views)       consistency filter of the given views;
+      filtered_maps(views)      {view: that view's filtered map}, 4-byte integers;
+      set_filtered_maps(full)   every view's filtered map, concatenated in view order (flat);
       integrate()               TSDF integration of every view into the rank's slab."""
 
     def __init__(self, backend, sizes: Sequence[tuple[int, int]], rank: int, world: int,
@@ -172,7 +175,16 @@ class ScanSplit:
             self.backend.set_packed_maps(full)
 
     def filter(self) -> None:
-        self.backend.filter_all()
+        if self.views:
+            self.backend.filter_views(self.views)
+
+    def exchange_filtered(self) -> None:
+        ctx = getattr(self.backend, "context", None)
+        with (ctx() if ctx else contextlib.nullcontext()):
+            local = self.backend.filtered_maps(self.views)
+            full = gather_packed_maps(local, self.sizes, self.shards, self.rank, self.group,
+                                      self.device)
+            self.backend.set_filtered_maps(full)
 
     def integrate(self) -> None:
         self.backend.integrate()
@@ -181,6 +193,7 @@ class ScanSplit:
         self.solve()
         self.exchange()
         self.filter()
+        self.exchange_filtered()
         self.integrate()
 
 
@@ -214,6 +227,7 @@ class DeviceScan:
         sizes = stereo.sizes
         self.off = _offsets(sizes)
         self.maps = device_view(stereo.buffers().depths, int(self.off[-1]))
+        self.filtered = None
 
     def solve(self, views):
         self.stereo.solve_all(views, [self.options[v] for v in views])
@@ -230,8 +244,19 @@ class DeviceScan:
     def set_packed_maps(self, full):
         self.maps.copy_(full)
 
-    def filter_all(self):
-        self.stereo.filter_all(self.refs, self.sources, self.needed)
+    def filter_views(self, views):
+        self.stereo.filter_all(views, [self.sources[v] for v in views], [self.needed[v] for v in views])
+        if self.filtered is None:  # filtered_all exists after the first filter
+            self.filtered = device_view(self.stereo.buffers().filtered_all, int(self.off[-1]))
+
+    def filtered_maps(self, views):
+        return {v: self.filtered[int(self.off[v]):int(self.off[v + 1])] for v in views}
+
+    def set_filtered_maps(self, full):
+        if self.filtered is None:  # a rank without views: allocate filtered_all by filtering none
+            self.stereo.filter_all([0], [self.sources[0]], [self.needed[0]])
+            self.filtered = device_view(self.stereo.buffers().filtered_all, int(self.off[-1]))
+        self.filtered.copy_(full)
 
     def integrate(self):
         if self.tsdf is not None:

@@ -134,8 +134,16 @@ class OracleScan:
     def set_packed_maps(self, full):
         self.o._depths[:] = full.numpy().view(np.uint32)
 
-    def filter_all(self):
-        self.filtered = {v: self.o.filter(v, self.w.sources[v], self.w.needed[v])
+    def filter_views(self, views):
+        self.filtered.update({v: self.o.filter(v, self.w.sources[v], self.w.needed[v]) for v in views})
+
+    def filtered_maps(self, views):
+        return {v: self.filtered[v] for v in views}
+
+    def set_filtered_maps(self, full):
+        flat = full.numpy().view(np.uint32)
+        n = self.w.width * self.w.height
+        self.filtered = {v: flat[v * n:(v + 1) * n].reshape(self.w.height, self.w.width).copy()
                          for v in range(len(self.w.views))}
 
     def integrate(self):
@@ -189,8 +197,9 @@ def _split_worker(rank, world, port, out_dir):
 
 
 def test_scan_split_over_two_and_three_gloo_ranks_equals_one_rank():
-    """ScanSplit end to end (solve of each rank's views, the all-gather of packed maps, every
-    view's filter on every rank, the z-slab TSDF), on 1, 2 and 3 gloo ranks: every rank's
+    """ScanSplit end to end (solve of each rank's views, the all-gather of packed maps, the filter
+    of each rank's views, the all-gather of filtered maps, the z-slab TSDF), on 1, 2 and 3 gloo
+    ranks: every rank's
     filtered maps and the slabs put together equal the one-rank result bit for bit.  Three ranks
     over a grid of three brick rows, and four views of five dealt by pixel count."""
     import torch.multiprocessing as mp
