@@ -229,6 +229,23 @@ def test_scan_split_over_two_and_three_gloo_ranks_equals_one_rank():
             np.testing.assert_array_equal(wt, want_w)
 
 
+def test_scan_split_with_a_rank_that_owns_no_view():
+    """Six gloo ranks over five views: one rank solves and filters nothing but still takes part in
+    both all-gathers, and ends with every view's filtered map, equal to one rank's."""
+    import torch.multiprocessing as mp
+
+    with tempfile.TemporaryDirectory() as d:
+        for world in (1, 6):
+            mp.start_processes(_split_worker, args=(world, _free_port(), d), nprocs=world,
+                               join=True, start_method="spawn")
+        want_f = np.load(os.path.join(d, "w1_filtered0.npy"))
+        owners = [[v for v in np.load(os.path.join(d, f"w6_views{r}.npy")) if v >= 0] for r in range(6)]
+        assert sorted(v for o in owners for v in o) == list(range(5))
+        assert any(not o for o in owners)
+        for r in range(6):
+            np.testing.assert_array_equal(np.load(os.path.join(d, f"w6_filtered{r}.npy")), want_f)
+
+
 def test_empty_slab_ranks_integrate_nothing():
     dims = (16, 16, 16)  # two brick rows along z
     assert shard.slab_pool(dims, 2, 3) is None
